@@ -1,0 +1,394 @@
+"""Benchmark of the PyCLES hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c5_dycoms]
+                    [--precision fp64|fp32] [--impl ours|reference]
+
+A step is one time step (three SSP-RK3 stages) of the hot path --
+thermodynamics, scalar and momentum advection, RK update, ghost fill and the
+pressure solve -- over the configuration's whole grid.  Metric: grid-cell
+RK-stage updates/s = interior cells x 3 / time per step.
+
+Workload (default): 512 x 512 x 256 cells, dx = dy = 35 m, dz = 5 m, gw = 4,
+WENO7 scalars, WENO5 momentum, saturation adjustment, dt = 0.25 s, a seeded
+synthetic DYCOMS-RF01-like stratocumulus state (no public data set is used).
+The state (~19 GB FP64) is larger than L2, so no L2 flush is needed.
+
+Multi-GPU: the domain is not split across GPUs here; N ranks run N
+independent replicas (weak scaling), timed as the max over ranks.
+
+``--impl reference`` times the reference's own CPU implementation of the
+path (its C kernels compiled from source into oracle/_ref, driven by the
+restated glue) on all host cores, each core stepping a bounded sub-domain
+of the same configuration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "grid-cell RK-stage updates/s"
+UNIT = "cell-stage/s"
+# algorithmic bytes and flops per interior cell per RK stage of the fused
+# advection (read every prognostic field once, read-modify-write every
+# tendency once): 24 B x nv; flops of WENO5/7 fluxes + divergence.
+ADV_BYTES_PER_CELL = {5: 120, 4: 96}
+ADV_FLOPS_PER_CELL = {("c5", 7): 3252, ("moist", 5): 2340, ("dry", 5): 1881}
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU side: reference implementation on bounded per-core samples
+# ---------------------------------------------------------------------------
+def _cpu_sample_shape(cfg):
+    """Per-core sub-domain: the configuration's nz, gw and orders, with a
+    horizontal extent sized for a few seconds of reference CPU work per step."""
+    nz = cfg["nz"]
+    nh = 64 if nz >= 128 else 48
+    return nh, nh, nz
+
+
+def _cpu_worker(args):
+    """One process: build a sub-domain sample, run `nsteps` steps of the
+    reference's C kernels + restated glue, return per-step wall times."""
+    cfg, nsteps, backend, conn_barrier = args
+    import numpy as np  # noqa: F401
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import host_case, oracle_sim
+    nx, ny, nz = _cpu_sample_shape(cfg)
+    nl, rs, f = host_case(cfg["case"], nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"], gw=cfg["gw"], dt=cfg["dt"],
+                          scalar_order=cfg.get("scalar_order", 5), momentum_order=cfg.get("momentum_order", 5))
+    sim = oracle_sim(nl, rs, f, backend=backend)
+    sim.update_all_bcs()
+    times = []
+    for _ in range(nsteps):
+        if conn_barrier is not None:
+            conn_barrier.wait()
+        t0 = time.perf_counter()
+        sim.step()
+        times.append(time.perf_counter() - t0)
+    return nx * ny * nz, times
+
+
+def cpu_reference_run(cfg, nsteps, nwarm, backend="ref", cores=None):
+    """Runs `cores` concurrent workers in lock-step; returns per-step aggregate
+    throughput (cell-stage/s) and the description of the sample."""
+    import multiprocessing as mp
+    from oracle import ref as oref
+    if backend == "ref" and not oref.available():
+        backend = "port"
+    cores = cores or len(os.sched_getaffinity(0))
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        barrier = mgr.Barrier(cores)
+        with ctx.Pool(cores) as pool:
+            res = pool.map(_cpu_worker, [(cfg, nsteps + nwarm, backend, barrier)] * cores)
+    cells = res[0][0]
+    per_step = []
+    for s in range(nwarm, nwarm + nsteps):
+        wall = max(r[1][s] for r in res)
+        per_step.append(cores * cells * 3 / wall)
+    nx, ny, nz = _cpu_sample_shape(cfg)
+    kind = "reference" if backend == "ref" else "port"
+    sample = (f"{cores} concurrent processes, each one time step of a {nx}x{ny}x{nz} sub-domain "
+              f"(gw={cfg['gw']}, WENO{cfg.get('scalar_order', 5)}/{cfg.get('momentum_order', 5)}) of the same case; "
+              f"{'reference C kernels compiled from source + restated glue' if kind == 'reference' else 'numpy port'}"
+              "; no halo exchange or pencil transposes between processes (MPI-free upper bound)")
+    return per_step, {"kind": kind, "cores": cores, "sample": sample}
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from pycles_b200 import _capi
+    from pycles_b200.simulation import CONFIGS, HotPathSimulation, namelist_for
+
+    cfg = dict(CONFIGS[args.config])
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nl = namelist_for(**cfg, precision=args.precision)
+    sim = HotPathSimulation(nl, device=dev)
+    fields = sim.initialize(seed=rank)
+    stream = torch.cuda.current_stream(dev)
+    sim.run(0)  # ghost fill + first thermodynamics update, as Simulation3d.run
+    _capi.clear_error()
+    for _ in range(args.warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    # ---- device-resident timed region ---------------------------------------
+    comp = ["thermo", "scalar_adv", "momentum_adv", "rk3+bcs", "pressure"]
+    ev = []
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    L = _capi.load()
+    n_launch0 = L.pb_launch_count()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_start.record(stream)
+    Gr, PV, DV, RS = sim.Gr, sim.PV, sim.DV, sim.RS
+    for _ in range(args.steps):
+        for rk in range(3):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+            e[0].record(stream)
+            sim.Th.update(Gr, RS, PV, DV)
+            e[1].record(stream)
+            sim.SA.update(Gr, RS, PV, DV)
+            e[2].record(stream)
+            sim.MA.update(Gr, RS, PV)
+            e[3].record(stream)
+            sim.TS.rk_step = rk
+            sim.TS.update(Gr, PV)
+            PV.Update_all_bcs(Gr)
+            e[4].record(stream)
+            sim.Pr.update(Gr, RS, DV, PV)
+            e[5].record(stream)
+            ev.append(e)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    launches = L.pb_launch_count() - n_launch0
+    clock_info = clocks.stop()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    comp_ms = {c: 0.0 for c in comp}
+    for e in ev:
+        for i, c in enumerate(comp):
+            comp_ms[c] += e[i].elapsed_time(e[i + 1])
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms = float(t.item())
+    err = _capi.get_error()
+
+    npl = Gr.dims.npl
+    ms_per_step = elapsed_ms / args.steps
+    value = world * npl * 3 * args.steps / (elapsed_ms / 1e3)
+
+    # ---- end to end through the public API with host buffers ---------------
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(PV.values.numel(), dtype=torch.float64, pin_memory=True)
+        host.copy_(PV.values)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            PV.values.copy_(host, non_blocking=True)
+            sim.step()
+            host.copy_(PV.values, non_blocking=True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        nbytes = PV.values.numel() * 8
+        e2e = {"value": world * npl * 3 * args.steps / (float(te.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+        del host
+
+    # ---- roofline of the dominant kernel group (advection) -----------------
+    peak, peak_kind = _peaks()
+    nv = PV.nv
+    adv_ms = (comp_ms["scalar_adv"] + comp_ms["momentum_adv"]) / (args.steps * 3)
+    adv_bytes = ADV_BYTES_PER_CELL.get(nv, 24 * nv) * npl
+    achieved = adv_bytes / (adv_ms / 1e3) / 1e9
+    flops_key = ("c5", 7) if cfg.get("scalar_order", 5) == 7 else (("moist", 5) if nv == 5 else ("dry", 5))
+    adv_flops = ADV_FLOPS_PER_CELL[flops_key] * npl
+    traffic = _read_traffic(args.config, args.precision)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "advection (scalar + momentum, 6 launches per stage)",
+                "algorithmic_bytes_per_cell_stage": ADV_BYTES_PER_CELL.get(nv, 24 * nv),
+                "fp64_flops_per_cell_stage": ADV_FLOPS_PER_CELL[flops_key],
+                "achieved_fp64_tflops": round(adv_flops / (adv_ms / 1e3) / 1e12, 2)}
+
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64",
+            "data": "synthetic (seeded DYCOMS-RF01-like state)" if cfg["case"] == "dycoms" else "synthetic (seeded)",
+            "config": {"workload": f"{args.config}: {cfg['nx']}x{cfg['ny']}x{cfg['nz']} cells, "
+                                   f"gw={cfg['gw']}, WENO{cfg.get('scalar_order', 5)} scalars / "
+                                   f"WENO{cfg.get('momentum_order', 5)} momentum, case={cfg['case']}, "
+                                   f"dt={cfg['dt']}", "form": args.precision,
+                       "cells": npl, "state_bytes": int(PV.values.numel() * 8 * 4),
+                       "l2": "inputs larger than L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}"},
+            "component_ms_per_step": {c: round(v / args.steps, 4) for c, v in comp_ms.items()},
+            "roofline": roofline,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clock_info,
+            "device_error_word": err,
+        }
+    del fields
+    return out, sim
+
+
+def _read_traffic(config, precision):
+    """DRAM bytes per launch of the dominant kernels, from the committed ncu
+    summary (profiles/advection_*.md: a line 'traffic_bytes_per_stage: N')."""
+    import glob
+    import re
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "advection_*.md"))):
+        try:
+            txt = open(p).read()
+        except OSError:
+            continue
+        m = re.search(rf"traffic_bytes_per_stage\[{re.escape(config)},{precision}\]:\s*([0-9.eE+]+)", txt)
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="c5_dycoms")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-cores", type=int, default=None)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from pycles_b200.simulation import CONFIGS
+    cfg = dict(CONFIGS[args.config])
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        per_step, info = cpu_reference_run(cfg, args.steps, args.warmup, backend="ref", cores=args.cpu_cores)
+        value = statistics.mean(per_step)
+        info["value"] = value
+        info["unit"] = UNIT
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"{args.config}: per-core sub-domains of the same configuration",
+                       "parallelism": f"{info['cores']} host processes"},
+            "cpu_baseline": info,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return 0
+
+    # CPU baseline first (spawned workers, before any CUDA context exists)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            per_step, info = cpu_reference_run(cfg, 1, 1, backend="ref", cores=args.cpu_cores)
+            info["value"] = per_step[0]
+            info["unit"] = UNIT
+            cpu = info
+        except Exception as e:  # reported, not fatal
+            cpu = {"error": str(e)[:200]}
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    out, _ = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        out["cpu_baseline"] = cpu
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,244 @@
+/*
+ * pycles_b200 -- C ABI of the B200 (sm_100a) PyCLES hot path.
+ *
+ * Every entry point takes plain pointers and sizes (device pointers unless
+ * stated otherwise), a CUDA stream as `void*` (NULL = legacy default
+ * stream), is stream-ordered, never synchronises the host, allocates no
+ * device memory, and returns a pb_status.  Fields use the reference layout:
+ * flat ghosted [i][j][k] arrays, k contiguous, length npg each, as held in
+ * PrognosticVariables.values / DiagnosticVariables.values
+ * (PrognosticVariables.pyx:78-79, DiagnosticVariables.pyx).
+ *
+ * Numerical failures detected on the device (pv* table range, secant
+ * iteration cap, non-finite temperatures) are OR-ed into a device error
+ * word that pb_get_error() reads; they do not make a call return non-zero.
+ */
+#ifndef PYCLES_B200_H
+#define PYCLES_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+enum pb_status {
+  PB_OK = 0,
+  PB_ERR_ARG = 1,          /* invalid shape, null pointer, bad enum      */
+  PB_ERR_CUDA = 2,         /* a CUDA runtime call or launch failed       */
+  PB_ERR_UNSUPPORTED = 3,  /* valid for the reference, not built here    */
+  PB_ERR_WORKSPACE = 4     /* workspace missing or too small             */
+};
+
+/* Arithmetic form of the advection / FFT paths. */
+enum pb_precision {
+  PB_FP64 = 0,             /* plain form: the reference method in FP64  */
+  PB_FP32 = 1              /* fluxes in FP32, divergence accumulated in FP64 */
+};
+
+/*
+ * Grid geometry.  Field for field (types and order) the reference's
+ * struct DimStruct (Csrc/grid.h:2-24), so a Cython caller can pass
+ * &Grid.dims directly.  One rank holds the whole domain: nl == n,
+ * nlg == n + 2*gw, indx_lo == 0.
+ */
+typedef struct pb_dims {
+  long dims;
+  long n[3];
+  long ng[3];
+  long nl[3];
+  long nlg[3];
+  long npd;
+  long npl;
+  long npg;
+  long gw;
+  long indx_lo[3];
+  long indx_lo_g[3];
+  long nbuffer[3];
+  long ghosted_stride[3];
+  double dx[3];
+  double dxi[3];
+} pb_dims;
+
+/*
+ * Saturation vapour pressure table on the device: the reference's
+ * LookupStruct (Csrc/lookup.h:4-13) with y in device memory.
+ * x_min = min(T), dx = T[1]-T[0], dxi = 1/dx as init_table computes them.
+ */
+typedef struct pb_table {
+  const double* y;
+  long n;
+  double x_min;
+  double dx;
+  double dxi;
+} pb_table;
+
+/*
+ * Learned saturation-adjustment seed: a 3->64->64->1 SiLU MLP with BF16
+ * weights (device pointers), inputs (p0, s, qt) mapped affinely to [-1,1]
+ * by in_lo/in_hi, output T = out_mean + out_scale * y.
+ * Weight layouts: w1 [64][3], w2 [64][64], w3 [64] (row = output unit),
+ * biases FP32.
+ */
+typedef struct pb_mlp {
+  const void* w1;   /* bf16 [64*3]  */
+  const float* b1;  /* [64]         */
+  const void* w2;   /* bf16 [64*64] */
+  const float* b2;  /* [64]         */
+  const void* w3;   /* bf16 [64]    */
+  const float* b3;  /* [1]          */
+  float in_lo[3];
+  float in_hi[3];
+  float out_mean;
+  float out_scale;
+} pb_mlp;
+
+/* ------------------------------------------------------------------------
+ * Advection
+ * --------------------------------------------------------------------- */
+
+/*
+ * ScalarAdvection.update (ScalarAdvection.pyx:69-123) without the
+ * sedimentation branch: for every scalar and every direction d, the face
+ * fluxes of compute_advective_fluxes_a (Csrc/scalar_advection.h:689-730;
+ * WENO5 :319-394, WENO7 :396-480) and their divergence
+ * scalar_flux_divergence (Csrc/flux_divergence.h:4-32), subtracted from the
+ * scalar's tendency over the interior, d = 0, 1, 2 in that order.
+ *   scalars, tendencies : HOST arrays of nscalars device pointers.
+ *   flux (nullable)     : nscalars*3*npg doubles, [scalar][d][ijk] as
+ *                         ScalarAdvection.flux (:55); written on the faces
+ *                         the divergence reads (interior cells in the other
+ *                         two directions, faces gw-1 .. nlg-gw-1 along d).
+ *   order               : 5 or 7 (needs gw >= 3 resp. gw >= 4).
+ */
+int pb_scalar_advection(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                        const double* alpha0, const double* alpha0_half, const double* u,
+                        const double* v, const double* w, int nscalars,
+                        const double* const* scalars, double* const* tendencies, double* flux,
+                        int order, int precision, void* stream);
+
+/*
+ * MomentumAdvection.update (MomentumAdvection.pyx:41-69): for advected
+ * component a and advecting direction d (a, d = 0..2 in that order),
+ * compute_advective_tendencies_m (Csrc/momentum_advection.h:13-93; WENO5
+ * Csrc/momentum_advection_weno.h:113-245, WENO7 :247-400) including its
+ * momentum_flux_divergence (Csrc/flux_divergence.h:34-60).  The reference
+ * mallocs a flux array per call; this path needs none.
+ */
+int pb_momentum_advection(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                          const double* alpha0, const double* alpha0_half, const double* u,
+                          const double* v, const double* w, double* ut, double* vt, double* wt,
+                          int order, int precision, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Thermodynamics
+ * --------------------------------------------------------------------- */
+
+/*
+ * ThermodynamicsSA.update (ThermodynamicsSA.pyx:176-213): clip_qt
+ * (Csrc/thermodynamics_sa.h:213-219) when clip_qt != 0, eos_update
+ * (:68-96, per-cell eos_c secant :17-66 and alpha_c), buoyancy_update_sa
+ * (:98-132, adds to w_tend), bvf_sa (:134-182), thetali_update (:185-211).
+ * Latent heat: latent_heat_variable, lambda = 1 (Microphysics.pxd:65-75).
+ *   mlp (nullable)        : learned seed for the secant's second point.
+ *   secant_iters (nullable): device long long[2]; receives
+ *                           {sum of secant iterations, saturated cells}.
+ *   max_iter              : secant iteration cap (the reference has none);
+ *                           reaching it sets PB_ERR_SECANT_CAP in the error word.
+ */
+int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const double* alpha0_half,
+                 const pb_table* table, const double* s, double* qt, double* T, double* qv,
+                 double* ql, double* qi, double* alpha, double* buoyancy, double* theta_rho,
+                 double* bvf, double* thetali, double* w_tend, int clip_qt, const pb_mlp* mlp,
+                 long long* secant_iters, int max_iter, void* stream);
+
+/*
+ * ThermodynamicsDry.update (ThermodynamicsDry.pyx:105-120): eos_update
+ * (Csrc/thermodynamics_dry.h:12-37), buoyancy_update (:39-73, adds to
+ * w_tend), bvf_dry (:75-110).  pd is RS.p0_half as the reference passes it.
+ */
+int pb_thermo_dry(const pb_dims* dims, const double* p0_half, const double* alpha0_half,
+                  const double* s, double* T, double* alpha, double* buoyancy, double* theta,
+                  double* bvf, double* w_tend, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Time stepping and boundary conditions
+ * --------------------------------------------------------------------- */
+
+/*
+ * TimeStepping.update_third (TimeStepping.pyx:131-151) over n values
+ * (nv*npg, ghosts included): SSP-RK3 stage rk_step (0, 1, 2), tendencies
+ * zeroed afterwards.  value_copy is TimeStepping.value_copies[0].
+ */
+int pb_rk3_update(double* values, double* tendencies, double* value_copy, long long n, double dt,
+                  int rk_step, void* stream);
+
+/*
+ * PrognosticVariables.update_all_bcs (PrognosticVariables.pyx:183-233) on
+ * one periodic-x,y rank, and DiagnosticVariables.communicate_variable
+ * (DiagnosticVariables.pyx:65-112) when nv == 1: x and y ghost planes from
+ * the opposite interior planes (build_buffer / buffer_to_values,
+ * Csrc/prognostic_variables.h:11-203), z ghosts by set_bcs (:205-270) with
+ * bc_factor 1 (sym), -1 (asym) or 2.  values holds nv fields spaced npg;
+ * bc_factor is a HOST array of nv doubles.
+ */
+int pb_update_all_bcs(const pb_dims* dims, double* values, const double* bc_factor, int nv,
+                      void* stream);
+
+/* ------------------------------------------------------------------------
+ * Pressure
+ * --------------------------------------------------------------------- */
+
+/* Bytes of device scratch pb_pressure_solve needs for this grid. */
+long long pb_pressure_workspace_bytes(const pb_dims* dims);
+
+/*
+ * PressureFFTParallel.initialize (PressureFFTParallel.pyx:27-62): fills the
+ * grid constants of the workspace -- the modified wave numbers of
+ * compute_modified_wave_numbers (:64-98), evaluated on the host with the C
+ * library cos exactly as the reference evaluates them, and the FFT twiddle
+ * factors.  Synchronous; call once per workspace before pb_pressure_solve.
+ */
+int pb_pressure_init(const pb_dims* dims, void* workspace, long long workspace_bytes);
+
+/*
+ * PressureSolver.update (PressureSolver.pyx:38-80) up to, not including,
+ * its final PV.update_all_bcs: w -= HorizontalMean(w) (ParallelMPI.pyx:
+ * 196-241, remove_mean_u3 :113-136), divergence = second_order_divergence
+ * (:138-175), PressureFFTParallel.solve (PressureFFTParallel.pyx:150-219:
+ * horizontal FFT, per-(kx,ky) tridiagonal solve with modified wave numbers
+ * :64-98 and the matrix of :100-148, mode (0,0) zeroed, inverse FFT, real
+ * part; SparseSolvers.TDMA :24-44), the sym ghost fill of the pressure
+ * (DiagnosticVariables.communicate_variable) and
+ * second_order_pressure_correction (:83-110).
+ *   workspace : >= pb_pressure_workspace_bytes(dims) bytes, 256-byte aligned,
+ *               initialised by pb_pressure_init.
+ *   n[0], n[1] : any size; powers of two take the radix-2 path.
+ */
+int pb_pressure_solve(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                      const double* alpha0, const double* alpha0_half, double* u, double* v,
+                      double* w, double* divergence, double* dynamic_pressure, void* workspace,
+                      long long workspace_bytes, int precision, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Errors
+ * --------------------------------------------------------------------- */
+
+/* Reads (synchronously) and returns the device error word of the current device. */
+int pb_get_error(unsigned int* word);
+/* Clears the device error word of the current device (stream-ordered). */
+int pb_clear_error(void* stream);
+/* Human-readable status text. */
+const char* pb_status_string(int status);
+
+/*
+ * Number of kernels this library has launched in this process (host-side
+ * counter, incremented at every launch).  Instrumentation with no
+ * counterpart in the reference.
+ */
+long long pb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYCLES_B200_H */

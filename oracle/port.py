@@ -1,0 +1,671 @@
+"""numpy restatement of the PyCLES hot-path kernels -- TEST INFRASTRUCTURE ONLY.
+
+Every function follows one reference function (file:line cited) and keeps
+its loop ranges and its floating-point evaluation order, so that on the same
+inputs it agrees with the reference's C to rounding of the transcendental
+functions (bit-exact for the polynomial parts).  Arrays are 3-D views
+``[i, j, k]`` of the flat ghosted fields (k contiguous), shape ``dims.nlg``.
+
+Pinned against the compiled reference (``oracle.ref``) by
+``tests/test_oracle_pin.py``.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .dims import Dims
+
+# generate_parameters.py:19-41 (values as written to parameters.h)
+g = 9.80665
+Rd = 287.1
+Rv = 461.5
+eps_v = 0.6221018418201517
+eps_vi = 1.6074538488331591
+cpd = 1004.0
+cpv = 1859.0
+kappa = 0.2859561752988048
+Tt = 273.16
+T_tilde = 298.15
+p_tilde = 100000.0
+pv_star_t = 611.7
+sd_tilde = 6864.8
+sv_tilde = 10513.6
+pi = 3.141592653589793
+
+
+# ---------------------------------------------------------------------------
+# interpolants, Csrc/advection_interpolation.h
+# ---------------------------------------------------------------------------
+def interp_2(phi, phip1):  # :4-6
+    return 0.5 * (phi + phip1)
+
+
+def interp_4(phim1, phi, phip1, phip2):  # :12-14
+    return (7.0 / 12.0) * (phi + phip1) - (1.0 / 12.0) * (phim1 + phip2)
+
+
+def interp_6(phim2, phim1, phi, phip1, phip2, phip3):  # :20-24
+    return ((37.0 / 60.0) * (phi + phip1) - (2.0 / 15.0) * (phim1 + phip2)
+            + (1.0 / 60.0) * (phim2 + phip3))
+
+
+def interp_weno5(phim2, phim1, phi, phip1, phip2):  # :79-104
+    p0 = (1.0 / 3.0) * phim2 - (7.0 / 6.0) * phim1 + (11.0 / 6.0) * phi
+    p1 = (-1.0 / 6.0) * phim1 + (5.0 / 6.0) * phi + (1.0 / 3.0) * phip1
+    p2 = (1.0 / 3.0) * phi + (5.0 / 6.0) * phip1 - (1.0 / 6.0) * phip2
+    t2a = phi - 2.0 * phip1 + phip2
+    t2b = 3.0 * phi - 4.0 * phip1 + phip2
+    beta2 = 13.0 / 12.0 * t2a * t2a + 0.25 * t2b * t2b
+    t1a = phim1 - 2.0 * phi + phip1
+    t1b = phim1 - phip1
+    beta1 = 13.0 / 12.0 * t1a * t1a + 0.25 * t1b * t1b
+    t0a = phim2 - 2.0 * phim1 + phi
+    t0b = phim2 - 4.0 * phim1 + 3.0 * phi
+    beta0 = 13.0 / 12.0 * t0a * t0a + 0.25 * t0b * t0b
+    alpha0 = 0.1 / ((beta0 + 1e-10) * (beta0 + 1e-10))
+    alpha1 = 0.6 / ((beta1 + 1e-10) * (beta1 + 1e-10))
+    alpha2 = 0.3 / ((beta2 + 1e-10) * (beta2 + 1e-10))
+    alpha_sum_inv = 1.0 / (alpha0 + alpha1 + alpha2)
+    w0 = alpha0 * alpha_sum_inv
+    w1 = alpha1 * alpha_sum_inv
+    w2 = alpha2 * alpha_sum_inv
+    return w0 * p0 + w1 * p1 + w2 * p2
+
+
+def interp_weno7(phim3, phim2, phim1, phi, phip1, phip2, phip3):  # :106-145
+    p0 = (-1.0 / 4.0) * phim3 + (13.0 / 12.0) * phim2 + (-23.0 / 12.0) * phim1 + (25.0 / 12.0) * phi
+    p1 = (1.0 / 12.0) * phim2 + (-5.0 / 12.0) * phim1 + (13.0 / 12.0) * phi + (1.0 / 4.0) * phip1
+    p2 = (-1.0 / 12.0) * phim1 + (7.0 / 12.0) * phi + (7.0 / 12.0) * phip1 + (-1.0 / 12.0) * phip2
+    p3 = (1.0 / 4.0) * phi + (13.0 / 12.0) * phip1 + (-5.0 / 12.0) * phip2 + (1.0 / 12.0) * phip3
+    beta0 = (phim3 * (547.0 * phim3 - 3882.0 * phim2 + 4642.0 * phim1 - 1854.0 * phi)
+             + phim2 * (7043.0 * phim2 - 17246.0 * phim1 + 7042.0 * phi)
+             + phim1 * (11003.0 * phim1 - 9402.0 * phi)
+             + 2107.0 * phi * phi)
+    beta1 = (phim2 * (267.0 * phim2 - 1642.0 * phim1 + 1602.0 * phi - 494.0 * phip1)
+             + phim1 * (2843.0 * phim1 - 5966.0 * phi + 1922.0 * phip1)
+             + phi * (3443.0 * phi - 2522.0 * phip1)
+             + 547.0 * phip1 * phip1)
+    beta2 = (phim1 * (547.0 * phim1 - 2522.0 * phi + 1922.0 * phip1 - 494.0 * phip2)
+             + phi * (3443.0 * phi - 5966.0 * phip1 + 1602.0 * phip2)
+             + phip1 * (2843.0 * phip1 - 1642.0 * phip2)
+             + 267.0 * phip2 * phip2)
+    beta3 = (phi * (2107.0 * phi - 9402.0 * phip1 + 7042.0 * phip2 - 1854.0 * phip3)
+             + phip1 * (11003.0 * phip1 - 17246.0 * phip2 + 4642.0 * phip3)
+             + phip2 * (7043.0 * phip2 - 3882.0 * phip3)
+             + 547.0 * phip3 * phip3)
+    alpha0 = (1.0 / 35.0) / ((beta0 + 1e-10) * (beta0 + 1e-10))
+    alpha1 = (12.0 / 35.0) / ((beta1 + 1e-10) * (beta1 + 1e-10))
+    alpha2 = (18.0 / 35.0) / ((beta2 + 1e-10) * (beta2 + 1e-10))
+    alpha3 = (4.0 / 35.0) / ((beta3 + 1e-10) * (beta3 + 1e-10))
+    alpha_sum_inv = 1.0 / (alpha0 + alpha1 + alpha2 + alpha3)
+    w0 = alpha0 * alpha_sum_inv
+    w1 = alpha1 * alpha_sum_inv
+    w2 = alpha2 * alpha_sum_inv
+    w3 = alpha3 * alpha_sum_inv
+    return w0 * p0 + w1 * p1 + w2 * p2 + w3 * p3
+
+
+# ---------------------------------------------------------------------------
+# index helpers
+# ---------------------------------------------------------------------------
+def _region(shape, lo, hi_off):
+    return tuple(slice(lo, n - hi_off) for n in shape)
+
+
+def _sh(A, reg, d, o):
+    """View of A over region ``reg`` shifted by ``o`` cells along axis d."""
+    s = list(reg)
+    s[d] = slice(reg[d].start + o, reg[d].stop + o)
+    return A[tuple(s)]
+
+
+def _kvec(v, reg, ko=0):
+    """1-D profile over the k-range of ``reg`` (shifted by ko), broadcastable."""
+    return v[reg[2].start + ko: reg[2].stop + ko][None, None, :]
+
+
+# ---------------------------------------------------------------------------
+# scalar advection, Csrc/scalar_advection.h
+# ---------------------------------------------------------------------------
+def advective_fluxes_a(d: Dims, rho0, rho0_half, vel, scalar, flux, direction, order):
+    """weno_fifth_order_a (:319-394) / weno_seventh_order_a (:396-480)."""
+    sh = d.shape
+    V = vel.reshape(sh)
+    S = scalar.reshape(sh)
+    F = flux.reshape(sh)
+    if order == 7:
+        reg = _region(sh, 3, 4)
+        phip = interp_weno7(*[_sh(S, reg, direction, o) for o in (-3, -2, -1, 0, 1, 2, 3)])
+        phim = interp_weno7(*[_sh(S, reg, direction, o) for o in (4, 3, 2, 1, 0, -1, -2)])
+    elif order == 5:
+        reg = _region(sh, 2, 3)
+        phip = interp_weno5(*[_sh(S, reg, direction, o) for o in (-2, -1, 0, 1, 2)])
+        phim = interp_weno5(*[_sh(S, reg, direction, o) for o in (3, 2, 1, 0, -1)])
+    else:
+        raise ValueError("oracle restates WENO5/WENO7 only")
+    u = V[reg]
+    rho = _kvec(rho0 if direction == 2 else rho0_half, reg)
+    F[reg] = 0.5 * ((u + np.abs(u)) * phip + (u - np.abs(u)) * phim) * rho
+
+
+def scalar_flux_divergence(d: Dims, alpha0, alpha0_half, flux, tend, dx, direction):
+    """Csrc/flux_divergence.h:4-32 (uses dims->dxi[d])."""
+    sh = d.shape
+    F = flux.reshape(sh)
+    T = tend.reshape(sh)
+    reg = _region(sh, d.gw, d.gw)
+    a = _kvec(alpha0_half, reg)
+    T[reg] -= a * (F[reg] - _sh(F, reg, direction, -1)) * d.dxi[direction]
+
+
+def momentum_flux_divergence(d: Dims, alpha0, alpha0_half, flux, tend, d_advected, d_advecting):
+    """Csrc/flux_divergence.h:34-60."""
+    sh = d.shape
+    F = flux.reshape(sh)
+    T = tend.reshape(sh)
+    reg = _region(sh, d.gw, d.gw)
+    a = _kvec(alpha0_half if d_advected != 2 else alpha0, reg)
+    T[reg] -= a * (F[reg] - _sh(F, reg, d_advecting, -1)) * d.dxi[d_advecting]
+
+
+def advective_tendencies_m(d: Dims, rho0, rho0_half, alpha0, alpha0_half, vel_advected, vel_advecting,
+                           tend, d_advected, d_advecting, order):
+    """weno_fifth_order_m (Csrc/momentum_advection_weno.h:113-245) and
+    weno_seventh_order_m (:247-400), followed by momentum_flux_divergence."""
+    sh = d.shape
+    A = vel_advected.reshape(sh)
+    G = vel_advecting.reshape(sh)
+    flux = np.zeros(sh)
+    ed, ing = d_advecting, d_advected
+    if order == 7:
+        reg = _region(sh, 3, 4)
+        phip = interp_weno7(*[_sh(A, reg, ed, o) for o in (-3, -2, -1, 0, 1, 2, 3)])
+        phim = interp_weno7(*[_sh(A, reg, ed, o) for o in (4, 3, 2, 1, 0, -1, -2)])
+        vel_adv = interp_6(*[_sh(G, reg, ing, o) for o in (-2, -1, 0, 1, 2, 3)])
+    elif order == 5:
+        reg = _region(sh, 2, 3)
+        phip = interp_weno5(*[_sh(A, reg, ed, o) for o in (-2, -1, 0, 1, 2)])
+        phim = interp_weno5(*[_sh(A, reg, ed, o) for o in (3, 2, 1, 0, -1)])
+        vel_adv = interp_4(*[_sh(G, reg, ing, o) for o in (-1, 0, 1, 2)])
+    else:
+        raise ValueError("oracle restates WENO5/WENO7 only")
+    if d_advected != 2 and d_advecting != 2:
+        rho = _kvec(rho0_half, reg)
+    elif d_advected == 2 and d_advecting == 2:
+        rho = _kvec(rho0_half, reg, 1)
+    else:
+        rho = _kvec(rho0, reg)
+    flux[reg] = 0.5 * ((vel_adv + np.abs(vel_adv)) * phip + (vel_adv - np.abs(vel_adv)) * phim) * rho
+    momentum_flux_divergence(d, alpha0, alpha0_half, flux.reshape(-1), tend, d_advected, d_advecting)
+
+
+# ---------------------------------------------------------------------------
+# thermodynamic functions, Csrc/thermodynamic_functions.h, Csrc/entropies.h
+# ---------------------------------------------------------------------------
+def exner_c(p0):
+    return np.power(p0 / p_tilde, kappa)
+
+
+def pd_c(p0, qt, qv):
+    return p0 * (1.0 - qt) / (1.0 - qt + eps_vi * qv)
+
+
+def pv_c(p0, qt, qv):
+    return p0 * eps_vi * qv / (1.0 - qt + eps_vi * qv)
+
+
+def qv_star_c(p0, qt, pv):
+    return eps_v * (1.0 - qt) * pv / (p0 - pv)
+
+
+def alpha_c(p0, T, qt, qv):
+    return (Rd * T) / p0 * (1.0 - qt + eps_vi * qv)
+
+
+def buoyancy_c(alpha0, alpha):
+    return g * (alpha - alpha0) / alpha0
+
+
+def cpm_c(qt):
+    return (1.0 - qt) * cpd + qt * cpv
+
+
+def sd_c(pd, T):
+    return sd_tilde + cpd * np.log(T / T_tilde) - Rd * np.log(pd / p_tilde)
+
+
+def sv_c(pv, T):
+    return sv_tilde + cpv * np.log(T / T_tilde) - Rv * np.log(pv / p_tilde)
+
+
+def sc_c(L, T):
+    return -L / T
+
+
+def latent_heat_variable(T, lam=1.0):
+    """Microphysics.pxd:71-75."""
+    TC = T - 273.15
+    return (2500.8 - 2.36 * TC + 0.0016 * TC * TC - 0.00006 * TC * TC * TC) * 1000.0
+
+
+class Table:
+    """init_table / lookup (Csrc/lookup.h:16-54)."""
+
+    def __init__(self, x, y):
+        x = np.asarray(x, dtype=np.float64)
+        self.y = np.ascontiguousarray(y, dtype=np.float64)
+        self.x_min = float(np.min(x))
+        self.x_max = float(np.max(x))
+        self.dx = float(x[1] - x[0])
+        self.dxi = 1.0 / self.dx
+
+    def lookup(self, x):
+        indx = np.floor((x - self.x_min) * self.dxi).astype(np.int64)
+        y1 = self.y[indx]
+        y2 = self.y[indx + 1]
+        x1 = self.x_min + self.dx * indx
+        return y1 + (x - x1) * (y2 - y1) * self.dxi
+
+
+def temperature_no_ql(pd, pv, s, qt):
+    """Csrc/thermodynamics_sa.h:10-15."""
+    return T_tilde * np.exp((s - (1.0 - qt) * (sd_tilde - Rd * np.log(pd / p_tilde))
+                             - qt * (sv_tilde - Rv * np.log(pv / p_tilde)))
+                            / ((1.0 - qt) * cpd + qt * cpv))
+
+
+def eos_c(LT: Table, p0, s, qt, max_iter=10_000, T2_seed=None):
+    """Vectorised eos_c (Csrc/thermodynamics_sa.h:17-66).
+
+    Returns T, qv, ql, qi, iterations.  ``T2_seed`` (optional) replaces the
+    first secant point T_2 of :39 -- the learned-guess variant; the loop
+    itself is unchanged.
+    """
+    p0 = np.asarray(p0, dtype=np.float64)
+    s = np.asarray(s, dtype=np.float64)
+    qt = np.asarray(qt, dtype=np.float64)
+    p0, s, qt = np.broadcast_arrays(p0, s, qt)
+    shape = s.shape
+    p0 = p0.reshape(-1).copy()
+    s = s.reshape(-1).copy()
+    qt = qt.reshape(-1).copy()
+    T = np.empty_like(s)
+    qv = qt.copy()
+    ql = np.zeros_like(s)
+    qi = np.zeros_like(s)
+    iters = np.zeros(s.shape, dtype=np.int64)
+    pv_1 = pv_c(p0, qt, qt)
+    pd_1 = p0 - pv_1
+    T_1 = temperature_no_ql(pd_1, pv_1, s, qt)
+    pv_star_1 = LT.lookup(T_1)
+    qv_star_1 = qv_star_c(p0, qt, pv_star_1)
+    unsat = qt <= qv_star_1
+    T[unsat] = T_1[unsat]
+    sat = np.nonzero(~unsat)[0]
+    if sat.size:
+        P, S, Q = p0[sat], s[sat], qt[sat]
+        t1 = T_1[sat]
+        pd1, pv1 = pd_1[sat], pv_1[sat]
+        qvs1 = qv_star_1[sat]
+        sigma_1 = Q - qvs1
+        L_1 = latent_heat_variable(t1)
+        s_1 = sd_c(pd1, t1) * (1.0 - Q) + sv_c(pv1, t1) * Q + sc_c(L_1, t1) * sigma_1
+        f_1 = S - s_1
+        t2 = t1 + sigma_1 * L_1 / ((1.0 - Q) * cpd + qvs1 * cpv)
+        if T2_seed is not None:
+            t2 = np.asarray(T2_seed, dtype=np.float64).reshape(-1)[sat].copy()
+        out_T = np.empty_like(t1)
+        out_qv = np.empty_like(t1)
+        out_sig = np.empty_like(t1)
+        out_lam = np.ones_like(t1)
+        out_it = np.zeros(t1.shape, dtype=np.int64)
+        act = np.arange(sat.size)
+        it = 0
+        while act.size and it < max_iter:
+            it += 1
+            P_, Q_, S_ = P[act], Q[act], S[act]
+            T1_, T2_, F1_ = t1[act], t2[act], f_1[act]
+            pv_star_2 = LT.lookup(T2_)
+            qv_star_2 = qv_star_c(P_, Q_, pv_star_2)
+            pv_2 = pv_c(P_, Q_, qv_star_2)
+            pd_2 = P_ - pv_2
+            sigma_2 = Q_ - qv_star_2
+            L_2 = latent_heat_variable(T2_)
+            s_2 = sd_c(pd_2, T2_) * (1.0 - Q_) + sv_c(pv_2, T2_) * Q_ + sc_c(L_2, T2_) * sigma_2
+            f_2 = S_ - s_2
+            T_n = T2_ - f_2 * (T2_ - T1_) / (f_2 - F1_)
+            t1[act] = T2_
+            t2[act] = T_n
+            f_1[act] = f_2
+            delta_T = np.abs(T_n - T2_)
+            out_T[act] = T_n
+            out_qv[act] = qv_star_2
+            out_sig[act] = sigma_2
+            out_it[act] = it
+            keep = (delta_T >= 1.0e-3) | (sigma_2 < 0.0)
+            act = act[keep]
+        T[sat] = out_T
+        qv[sat] = out_qv
+        ql[sat] = out_lam * out_sig
+        qi[sat] = (1.0 - out_lam) * out_sig
+        iters[sat] = out_it
+    return (T.reshape(shape), qv.reshape(shape), ql.reshape(shape), qi.reshape(shape),
+            iters.reshape(shape))
+
+
+def clip_qt(d: Dims, qt, clip_value):
+    """Csrc/thermodynamics_sa.h:213-219."""
+    np.maximum(qt, clip_value, out=qt)
+
+
+def eos_update_sa(d: Dims, LT: Table, p0, s, qt, T, qv, ql, qi, alpha):
+    """Csrc/thermodynamics_sa.h:68-96 (all ghosted cells)."""
+    sh = d.shape
+    P = np.broadcast_to(p0[None, None, :], sh)
+    T_, qv_, ql_, qi_, it = eos_c(LT, P, s.reshape(sh), qt.reshape(sh))
+    T[:] = T_.reshape(-1)
+    qv[:] = qv_.reshape(-1)
+    ql[:] = ql_.reshape(-1)
+    qi[:] = qi_.reshape(-1)
+    alpha[:] = alpha_c(P, T.reshape(sh), qt.reshape(sh), qv.reshape(sh)).reshape(-1)
+    return it
+
+
+def buoyancy_update_sa(d: Dims, alpha0, alpha, buoyancy, wt):
+    """Csrc/thermodynamics_sa.h:98-132."""
+    sh = d.shape
+    A = alpha.reshape(sh)
+    B = buoyancy.reshape(sh)
+    W = wt.reshape(sh)
+    n2 = sh[2]
+    B[:, :, 0:n2 - 1] = buoyancy_c(alpha0[None, None, 0:n2 - 1], A[:, :, 0:n2 - 1])
+    W[:, :, 1:n2 - 3] = W[:, :, 1:n2 - 3] + interp_2(B[:, :, 1:n2 - 3], B[:, :, 2:n2 - 2])
+
+
+def bvf_sa(d: Dims, LT: Table, p0, T, qt, qv, theta_rho, bvf):
+    """Csrc/thermodynamics_sa.h:134-182."""
+    sh = d.shape
+    n2 = sh[2]
+    Tt_ = T.reshape(sh)
+    QT = qt.reshape(sh)
+    QV = qv.reshape(sh)
+    TR = theta_rho.reshape(sh)
+    BV = bvf.reshape(sh)
+    dzi = 1.0 / d.dx[2]
+    k = slice(1, n2 - 1)
+    TR[:, :, k] = Tt_[:, :, k] * (1.0 - QT[:, :, k] + eps_vi * QV[:, :, k]) / exner_c(p0[None, None, k])
+    k = slice(2, n2 - 2)
+    km = slice(1, n2 - 3)
+    kp = slice(3, n2 - 1)
+    Tk, Tm, Tp = Tt_[:, :, k], Tt_[:, :, km], Tt_[:, :, kp]
+    Qk, Qm, Qp = QT[:, :, k], QT[:, :, km], QT[:, :, kp]
+    sat = QV[:, :, k] < Qk
+    P = np.broadcast_to(p0[None, None, k], Tk.shape)
+    Lv = latent_heat_variable(Tk)
+    pv_star = LT.lookup(Tk)
+    rsl = eps_v * pv_star / (P - pv_star)
+    gamma_w = (g / cpd * (1.0 / (1.0 - Qk)) * (1.0 + Lv * rsl / (Rd * Tk))
+               / (cpm_c(Qk) / cpd + Lv * Lv * (eps_v + rsl) * rsl / (cpd * Rd * Tk * Tk)))
+    dTdz = (interp_2(Tk, Tp) - interp_2(Tm, Tk)) * dzi
+    dqtdz = (interp_2(Qk, Qp) - interp_2(Qm, Qk)) * dzi
+    moist = g / Tk * (dTdz + gamma_w) * (1.0 + Lv * rsl / (Rd * Tk)) - dqtdz / (1.0 - Qk)
+    Rk, Rm, Rp = TR[:, :, k], TR[:, :, km], TR[:, :, kp]
+    dry = g / Rk * (interp_2(Rk, Rp) - interp_2(Rm, Rk)) * dzi
+    BV[:, :, k] = np.where(sat, moist, dry)
+
+
+def thetali_update(d: Dims, p0, T, qt, ql, qi, thetali):
+    """Csrc/thermodynamics_sa.h:185-211 with thetali_c (thermodynamic_functions.h:15-18)."""
+    sh = d.shape
+    P = p0[None, None, :]
+    Tt_ = T.reshape(sh)
+    Lv = latent_heat_variable(Tt_)
+    Q = qt.reshape(sh)
+    theta = Tt_ / exner_c(P)
+    thetali[:] = (theta * np.exp(-Lv * (ql.reshape(sh) / (1.0 - Q) + qi.reshape(sh) / (1.0 - Q))
+                                 / (Tt_ * cpd))).reshape(-1)
+
+
+# dry thermodynamics, Csrc/thermodynamics_dry.h ------------------------------
+def dry_eos_c(pd, s):  # :8-10
+    return T_tilde * (np.exp((s - sd_tilde + Rd * np.log(pd / p_tilde)) / cpd))
+
+
+def eos_update_dry(d: Dims, pd, s, T, alpha):  # :12-37
+    sh = d.shape
+    P = pd[None, None, :]
+    T[:] = dry_eos_c(P, s.reshape(sh)).reshape(-1)
+    alpha[:] = alpha_c(P, T.reshape(sh), 0.0, 0.0).reshape(-1)
+
+
+def buoyancy_update_dry(d: Dims, alpha0, alpha, buoyancy, wt):  # :39-73
+    sh = d.shape
+    A = alpha.reshape(sh)
+    B = buoyancy.reshape(sh)
+    W = wt.reshape(sh)
+    i = slice(0, sh[0] - 1)
+    j = slice(0, sh[1] - 1)
+    k = slice(0, sh[2] - 1)
+    B[i, j, k] = buoyancy_c(alpha0[None, None, k], A[i, j, k])
+    W[i, j, k] += interp_2(B[i, j, k], B[i, j, 1:sh[2]])
+
+
+def bvf_dry(d: Dims, p0, T, theta, bvf):  # :75-110
+    sh = d.shape
+    n2 = sh[2]
+    TH = theta.reshape(sh)
+    BV = bvf.reshape(sh)
+    dzi = 1.0 / d.dx[2]
+    k = slice(1, n2)
+    TH[:, :, k] = T.reshape(sh)[:, :, k] / exner_c(p0[None, None, k])
+    k = slice(2, n2 - 1)
+    BV[:, :, k] = g / TH[:, :, k] * (interp_2(TH[:, :, k], TH[:, :, 3:n2])
+                                     - interp_2(TH[:, :, 1:n2 - 2], TH[:, :, k])) * dzi
+
+
+def entropy_sa(p0, T, qt, ql, qi):
+    """ThermodynamicsSA.entropy (ThermodynamicsSA.pyx:140-159)."""
+    qv = qt - ql - qi
+    pd = pd_c(p0, qt, qv)
+    pv = pv_c(p0, qt, qv)
+    L = latent_heat_variable(T)
+    return sd_c(pd, T) * (1.0 - qt) + sv_c(pv, T) * qt + sc_c(L, T) * (ql + qi)
+
+
+# ---------------------------------------------------------------------------
+# halos, Csrc/prognostic_variables.h + PrognosticVariables.pyx:183-233
+# ---------------------------------------------------------------------------
+def set_bcs(d: Dims, V, dim, s, bc_factor):
+    """set_bcs (Csrc/prognostic_variables.h:205-270) on a 3-D view."""
+    assert dim == 2
+    gw = d.gw
+    n2 = d.shape[2]
+    if s == -1:
+        b = n2 - gw
+        if bc_factor == 1.0:
+            for k in range(gw):
+                V[:, :, b + k] = V[:, :, b - k - 1]
+        elif bc_factor == 2.0:
+            for k in range(gw):
+                V[:, :, b + k] = V[:, :, b - 1]
+        else:
+            V[:, :, b] = 0.0
+            for k in range(1, gw):
+                V[:, :, b + k] = bc_factor * V[:, :, b - k]
+    else:
+        b = gw - 1
+        if bc_factor == 1.0:
+            for k in range(gw):
+                V[:, :, b - k] = V[:, :, b + k + 1]
+        elif bc_factor == 2.0:
+            for k in range(gw):
+                V[:, :, b - k] = V[:, :, b + 1]
+        else:
+            V[:, :, b] = 0.0
+            for k in range(1, gw):
+                V[:, :, b - k] = bc_factor * V[:, :, b + k]
+
+
+def fill_ghosts(d: Dims, field, bc_factor):
+    """One variable of update_all_bcs on a single periodic-x,y rank:
+    x then y self-exchange (build_buffer/buffer_to_values, :11-203),
+    then the z boundary conditions (set_bcs)."""
+    V = field.reshape(d.shape)
+    gw = d.gw
+    for dim in (0, 1):
+        n = d.shape[dim]
+        idx = [slice(None)] * 3
+        src = [slice(None)] * 3
+        # s = -1: upper ghosts receive the lower interior planes
+        idx[dim] = slice(n - gw, n)
+        src[dim] = slice(gw, 2 * gw)
+        V[tuple(idx)] = V[tuple(src)]
+        # s = +1: lower ghosts receive the upper interior planes
+        idx[dim] = slice(0, gw)
+        src[dim] = slice(n - 2 * gw, n - gw)
+        V[tuple(idx)] = V[tuple(src)]
+    set_bcs(d, V, 2, -1, bc_factor)
+    set_bcs(d, V, 2, 1, bc_factor)
+
+
+def update_all_bcs(d: Dims, values, bc_type):
+    for v, bc in enumerate(bc_type):
+        fill_ghosts(d, values[v * d.npg:(v + 1) * d.npg], bc)
+
+
+# ---------------------------------------------------------------------------
+# time stepping, TimeStepping.pyx:131-151
+# ---------------------------------------------------------------------------
+def update_third(values, tendencies, value_copy, rk_step, dt):
+    if rk_step == 0:
+        value_copy[:] = values
+        values += tendencies * dt
+    elif rk_step == 1:
+        values[:] = 0.75 * value_copy + 0.25 * (values + tendencies * dt)
+    else:
+        values[:] = (1.0 / 3.0) * value_copy + (2.0 / 3.0) * (values + tendencies * dt)
+    tendencies[:] = 0.0
+
+
+# ---------------------------------------------------------------------------
+# pressure, PressureSolver.pyx + PressureFFTParallel.pyx (one rank)
+# ---------------------------------------------------------------------------
+def horizontal_mean(d: Dims, values):
+    """ParallelMPI.HorizontalMean (ParallelMPI.pyx:196-241), one rank."""
+    V = values.reshape(d.shape)
+    g_ = d.gw
+    s = V[g_:d.shape[0] - g_, g_:d.shape[1] - g_, :].sum(axis=(0, 1))
+    return s * (1.0 / float(d.n[1] * d.n[0]))
+
+
+def modified_wave_numbers(d: Dims):
+    """PressureFFTParallel.compute_modified_wave_numbers (:64-98)."""
+    out = []
+    for dim in (0, 1):
+        n = d.n[dim]
+        ii = np.arange(n)
+        xi = np.where(ii <= n / 2, ii, ii - n).astype(np.float64)
+        k2 = (2.0 * np.cos((2.0 * pi / n) * xi) - 2.0) / d.dx[dim] / d.dx[dim]
+        k2[0] = 0.0
+        out.append(k2)
+    return out
+
+
+def off_diagonals(d: Dims, rho0):
+    """PressureFFTParallel.compute_off_diagonals (:100-127)."""
+    n = d.n[2]
+    gw = d.gw
+    dzi = d.dxi[2]
+    a = np.zeros(n)
+    c = np.zeros(n)
+    a[0] = 0.0
+    c[0] = dzi * dzi * rho0[gw]
+    for k in range(1, n - 1):
+        a[k] = dzi * dzi * rho0[k + gw - 1]
+        c[k] = dzi * dzi * rho0[k + gw]
+    k = n - 1
+    a[k] = dzi * dzi * rho0[k + gw - 1]
+    c[k] = 0.0
+    return a, c
+
+
+def diagonal(d: Dims, rho0, rho0_half, kx2ky2):
+    """PressureFFTParallel.compute_diagonal (:129-148), vectorised over columns.
+    ``kx2ky2`` holds kx2[i] + ky2[j] per column; returns b[..., k]."""
+    n = d.n[2]
+    gw = d.gw
+    dzi = d.dxi[2]
+    K = np.asarray(kx2ky2)[..., None]
+    b = np.empty(K.shape[:-1] + (n,))
+    b[..., 0] = rho0_half[gw] * K[..., 0] - (rho0[gw]) * dzi * dzi
+    kk = np.arange(1, n - 1)
+    b[..., 1:n - 1] = rho0_half[kk + gw] * K - (rho0[kk + gw] + rho0[kk + gw - 1]) * dzi * dzi
+    k = n - 1
+    b[..., k] = rho0_half[k + gw] * K[..., 0] - (rho0[k + gw - 1]) * dzi * dzi
+    return b
+
+
+def tdma(x, a, b, c):
+    """TDMA.solve (SparseSolvers.pyx:24-44) over the last axis, batched."""
+    n = x.shape[-1]
+    scratch = np.empty_like(b)
+    scratch[..., 0] = c[0] / b[..., 0]
+    x[..., 0] = x[..., 0] / b[..., 0]
+    for i in range(1, n):
+        m = 1.0 / (b[..., i] - a[i] * scratch[..., i - 1])
+        scratch[..., i] = c[i] * m
+        x[..., i] = (x[..., i] - a[i] * x[..., i - 1]) * m
+    for i in range(n - 2, -1, -1):
+        x[..., i] = x[..., i] - scratch[..., i] * x[..., i + 1]
+    return x
+
+
+def poisson_solve(d: Dims, rho0, rho0_half, div, pres):
+    """PressureFFTParallel.solve (:150-219), one rank: the pencil transposes
+    are identity re-layouts, so x-FFT, y-FFT, per-column TDMA on the real and
+    imaginary parts, mode (0,0) zeroed, inverse y then x, real part; ghost
+    cells of the result are zero."""
+    from scipy.fftpack import fft, ifft
+    import warnings
+    D = div.reshape(d.shape)[d.interior()]
+    H = fft(D, axis=0)
+    H = fft(H, axis=1)
+    kx2, ky2 = modified_wave_numbers(d)
+    a, c = off_diagonals(d, rho0)
+    b = diagonal(d, rho0, rho0_half, kx2[:, None] + ky2[None, :])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        xr = tdma(np.ascontiguousarray(H.real), a, b, c)
+        xi = tdma(np.ascontiguousarray(H.imag), a, b, c)
+    Z = xr + 1j * xi
+    Z[0, 0, :] = 0.0
+    Z = ifft(Z, axis=1)
+    Z = ifft(Z, axis=0)
+    P = pres.reshape(d.shape)
+    P[...] = 0.0
+    P[d.interior()] = Z.real
+
+
+def second_order_divergence(d: Dims, alpha0, alpha0_half, vel, div, direction):
+    """PressureSolver.pyx:138-175."""
+    sh = d.shape
+    V = vel.reshape(sh)
+    D = div.reshape(sh)
+    reg = _region(sh, d.gw, d.gw)
+    dxi = 1.0 / d.dx[direction]
+    if direction != 2:
+        ah = _kvec(alpha0_half, reg)
+        D[reg] += (V[reg] / ah - _sh(V, reg, direction, -1) / ah) * dxi
+    else:
+        D[reg] += ((V[reg]) / _kvec(alpha0, reg) - (_sh(V, reg, 2, -1)) / _kvec(alpha0, reg, -1)) * dxi
+
+
+def pressure_correction(d: Dims, p, u, v, w):
+    """PressureSolver.pyx:83-110: range [0, nlg-1) in every dimension."""
+    sh = d.shape
+    P = p.reshape(sh)
+    reg = (slice(0, sh[0] - 1), slice(0, sh[1] - 1), slice(0, sh[2] - 1))
+    Pc = P[reg]
+    u.reshape(sh)[reg] -= (_sh(P, reg, 0, 1) - Pc) * d.dxi[0]
+    v.reshape(sh)[reg] -= (_sh(P, reg, 1, 1) - Pc) * d.dxi[1]
+    w.reshape(sh)[reg] -= (_sh(P, reg, 2, 1) - Pc) * d.dxi[2]

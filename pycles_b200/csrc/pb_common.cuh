@@ -1,0 +1,93 @@
+// Shared definitions for the B200 hot-path kernels.
+//
+// Layout contract (identical to the reference, Csrc/grid.h and
+// PrognosticVariables.pyx:78-79): every field is a flat ghosted array
+// [i][j][k] with k contiguous, istride = nlg1*nlg2, jstride = nlg2.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+
+#include "../../include/pycles_b200.h"
+
+// Physical constants as generate_parameters.py:19-41 writes them
+// (eps_v = Rd/Rv, eps_vi = 1/eps_v, kappa = Rd/cpd, shortest round-trip
+// decimal of the Python double).
+namespace pbc {
+constexpr double g = 9.80665;
+constexpr double Rd = 287.1;
+constexpr double Rv = 461.5;
+constexpr double eps_v = 0.6221018418201517;
+constexpr double eps_vi = 1.6074538488331591;
+constexpr double cpd = 1004.0;
+constexpr double cpv = 1859.0;
+constexpr double kappa = 0.2859561752988048;
+constexpr double T_tilde = 298.15;
+constexpr double p_tilde = 100000.0;
+constexpr double sd_tilde = 6864.8;
+constexpr double sv_tilde = 10513.6;
+}  // namespace pbc
+
+// Error word bits (pb_get_error); kernels OR them in, the host reads once
+// per step.
+#define PB_ERR_TABLE_RANGE 0x1u   // lookup argument outside the pv* table
+#define PB_ERR_SECANT_CAP 0x2u    // saturation-adjustment secant hit its cap
+#define PB_ERR_NONFINITE 0x4u     // non-finite temperature produced
+
+// Defined here: the library is built as one translation unit (pb_all.cu).
+__device__ unsigned int pb_device_error = 0u;
+
+__device__ __forceinline__ void pb_flag(unsigned int bit) { atomicOr(&pb_device_error, bit); }
+
+struct Geo {
+  long long n0, n1, n2;     // nlg
+  long long is, js;         // strides in elements
+  long long gw;
+  long long npg;
+  double dxi0, dxi1, dxi2;
+  double dx2;
+};
+
+static inline Geo make_geo(const pb_dims* d) {
+  Geo g;
+  g.n0 = d->nlg[0];
+  g.n1 = d->nlg[1];
+  g.n2 = d->nlg[2];
+  g.js = g.n2;
+  g.is = g.n1 * g.n2;
+  g.gw = d->gw;
+  g.npg = g.n0 * g.n1 * g.n2;
+  g.dxi0 = d->dxi[0];
+  g.dxi1 = d->dxi[1];
+  g.dxi2 = d->dxi[2];
+  g.dx2 = d->dx[2];
+  return g;
+}
+
+// Validates the geometry fields every entry point relies on.
+int pb_check_dims(const pb_dims* d);
+
+#define PB_CUDA_TRY(expr)                          \
+  do {                                             \
+    cudaError_t _e = (expr);                       \
+    if (_e != cudaSuccess) return PB_ERR_CUDA;     \
+  } while (0)
+
+#define PB_LAUNCH_CHECK()                          \
+  do {                                             \
+    cudaError_t _e = cudaGetLastError();           \
+    if (_e != cudaSuccess) return PB_ERR_CUDA;     \
+  } while (0)
+
+// Host-side count of kernels this library has launched (pb_launch_count).
+inline std::atomic<long long>& pb_launch_counter() {
+  static std::atomic<long long> c{0};
+  return c;
+}
+static inline void pb_note_launch() { pb_launch_counter().fetch_add(1, std::memory_order_relaxed); }
+
+static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+static inline unsigned int ceil_div(long long a, long long b) { return (unsigned int)((a + b - 1) / b); }

@@ -1,0 +1,588 @@
+// Anelastic pressure solve on one GPU.
+//
+// The reference's pencil transposes (ParallelMPI.Pencil) become a choice of
+// layout: the spectral work array is W[k][j][i] (complex, i fastest), so
+// the x-FFT reads physical rows and writes contiguous i, the y-FFT works on
+// j-lines batched over contiguous i, and the Thomas solver gives one thread
+// to each (kx,ky) column with consecutive threads on consecutive i.
+//
+//   hmean_partial/hmean_final  HorizontalMean(w), deterministic two-pass sum
+//   remove_mean                w -= mean[k] on every cell (remove_mean_u3)
+//   zero_ghosts                divergence ghosts = 0 (the reference zeroes the
+//                              whole array before adding the interior terms)
+//   fft_x_fwd                  second_order_divergence (d = 0,1,2 in order)
+//                              + x-FFT of each (j, k) row
+//   fft_y                      y-FFT (forward, or inverse with 1/n1)
+//   tdma                       per-column Thomas (SparseSolvers.pyx:24-44) on
+//                              the complex coefficients, mode (0,0) := 0
+//   fft_x_inv                  inverse x-FFT, 1/n0, real part -> pressure
+//   (ghost fill, sym)          DiagnosticVariables.communicate_variable
+//   correction                 second_order_pressure_correction
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "pb_common.cuh"
+
+namespace {
+
+constexpr int kPartials = 296;  // 2 x 148 SMs
+constexpr int kFftThreads = 256;
+
+struct PLayout {
+  long long partial, mean, twx, twy, kx2, ky2, spec, scr, total;
+};
+
+long long align256(long long x) { return (x + 255) / 256 * 256; }
+
+PLayout playout(const pb_dims* d) {
+  PLayout L;
+  const long long n0 = d->n[0], n1 = d->n[1], n2 = d->n[2];
+  const long long nlg2 = d->nlg[2];
+  long long off = 0;
+  L.partial = off; off += align256((long long)kPartials * nlg2 * 8);
+  L.mean = off;    off += align256(nlg2 * 8);
+  L.twx = off;     off += align256(n0 * 16);
+  L.twy = off;     off += align256(n1 * 16);
+  L.kx2 = off;     off += align256(n0 * 8);
+  L.ky2 = off;     off += align256(n1 * 8);
+  L.spec = off;    off += align256(n0 * n1 * n2 * 16);
+  L.scr = off;     off += align256(n0 * n1 * n2 * 8);
+  L.total = off;
+  return L;
+}
+
+__device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// In-place radix-2 DIT over `nlines` lines of length N (power of two) held
+// in shared memory in bit-reversed order.  tw[m] = exp(-2 pi i m / N).
+__device__ void fft_pow2_lines(double2* buf, int nlines, int N, int logN, const double2* __restrict__ tw,
+                               bool inverse) {
+  const int halfN = N >> 1;
+  for (int s = 1; s <= logN; ++s) {
+    const int half = 1 << (s - 1);
+    const int twstride = N >> s;
+    for (int b = threadIdx.x; b < nlines * halfN; b += blockDim.x) {
+      const int line = b / halfN;
+      const int bb = b - line * halfN;
+      const int group = bb >> (s - 1);
+      const int pos = bb & (half - 1);
+      const int i0 = line * N + group * 2 * half + pos;
+      const int i1 = i0 + half;
+      double2 w = __ldg(tw + pos * twstride);
+      if (inverse) w.y = -w.y;
+      const double2 x0 = buf[i0];
+      const double2 t = cmul(w, buf[i1]);
+      buf[i0] = make_double2(x0.x + t.x, x0.y + t.y);
+      buf[i1] = make_double2(x0.x - t.x, x0.y - t.y);
+    }
+    __syncthreads();
+  }
+}
+
+// Direct DFT for lengths that are not powers of two: out = DFT(in).
+__device__ void dft_lines(const double2* in, double2* out, int nlines, int N, const double2* __restrict__ tw,
+                          bool inverse) {
+  for (int e = threadIdx.x; e < nlines * N; e += blockDim.x) {
+    const int line = e / N;
+    const int m = e - line * N;
+    double2 acc = make_double2(0.0, 0.0);
+    const double2* x = in + line * N;
+    int idx = 0;
+    for (int n = 0; n < N; ++n) {
+      double2 w = __ldg(tw + idx);
+      if (inverse) w.y = -w.y;
+      const double2 t = cmul(w, x[n]);
+      acc.x += t.x;
+      acc.y += t.y;
+      idx += m;
+      if (idx >= N) idx -= N;
+    }
+    out[e] = acc;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int slot(int idx, int N, int logN) {
+  if (!is_pow2(N)) return idx;
+  return logN == 0 ? 0 : (int)(__brev((unsigned)idx) >> (32 - logN));
+}
+
+struct PArgs {
+  const double* rho0;
+  const double* rho0_half;
+  const double* alpha0;
+  const double* alpha0_half;
+  double* u;
+  double* v;
+  double* w;
+  double* div;
+  double* p;
+  double* partial;
+  double* mean;
+  const double2* twx;
+  const double2* twy;
+  const double* kx2;
+  const double* ky2;
+  double2* spec;
+  double* scr;
+  int log0, log1;
+};
+
+// ---- HorizontalMean (ParallelMPI.pyx:196-241) ------------------------------
+__global__ void hmean_partial(Geo g, const double* __restrict__ w, double* __restrict__ partial) {
+  const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw;
+  const long long ncol = nl0 * nl1;
+  for (long long k = threadIdx.x; k < g.n2; k += blockDim.x) {
+    double s = 0.0;
+    for (long long c = blockIdx.x; c < ncol; c += gridDim.x) {
+      const long long i = g.gw + c / nl1;
+      const long long j = g.gw + c % nl1;
+      s += w[i * g.is + j * g.js + k];
+    }
+    partial[(long long)blockIdx.x * g.n2 + k] = s;
+  }
+}
+
+__global__ void hmean_final(Geo g, const double* __restrict__ partial, double* __restrict__ mean, int np,
+                            double n_horizontal_i) {
+  for (long long k = threadIdx.x; k < g.n2; k += blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < np; ++b) s += partial[(long long)b * g.n2 + k];
+    mean[k] = s * n_horizontal_i;
+  }
+}
+
+// remove_mean_u3 (PressureSolver.pyx:113-136): every cell
+__global__ void remove_mean(Geo g, double* __restrict__ w, const double* __restrict__ mean) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < g.npg; t += stride)
+    w[t] = w[t] - mean[t % g.n2];
+}
+
+__device__ __forceinline__ void ghost_decode(const Geo& g, long long t, long long& i, long long& j, long long& k) {
+  const long long gw = g.gw, n0 = g.n0, n1 = g.n1, n2 = g.n2;
+  const long long nl0 = n0 - 2 * gw, nl1 = n1 - 2 * gw;
+  const long long A = 2 * gw * n1 * n2;
+  const long long B = nl0 * 2 * gw * n2;
+  if (t < A) {
+    const long long gi = t / (n1 * n2);
+    const long long r = t - gi * (n1 * n2);
+    i = gi < gw ? gi : n0 - 2 * gw + gi;
+    j = r / n2;
+    k = r - j * n2;
+  } else if (t < A + B) {
+    const long long u = t - A;
+    const long long q = u / (2 * gw * n2);
+    const long long r = u - q * (2 * gw * n2);
+    i = gw + q;
+    const long long gj = r / n2;
+    j = gj < gw ? gj : n1 - 2 * gw + gj;
+    k = r - gj * n2;
+  } else {
+    const long long u = t - A - B;
+    const long long q = u / (nl1 * 2 * gw);
+    const long long r = u - q * (nl1 * 2 * gw);
+    i = gw + q;
+    j = gw + r / (2 * gw);
+    const long long gk = r % (2 * gw);
+    k = gk < gw ? gk : n2 - 2 * gw + gk;
+  }
+}
+
+__global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nghost; t += stride) {
+    long long i, j, k;
+    ghost_decode(g, t, i, j, k);
+    f[i * g.is + j * g.js + k] = 0.0;
+  }
+}
+
+// ---- divergence + forward x-FFT -------------------------------------------
+// block = (interior j, chunk of KC interior levels); smem KC lines of n0.
+__global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC) {
+  extern __shared__ double2 sbuf[];
+  const int N = (int)(g.n0 - 2 * g.gw);
+  const int nz = (int)(g.n2 - 2 * g.gw);
+  const int jl = blockIdx.x;
+  const int k0 = blockIdx.y * KC;
+  const int kc = min(KC, nz - k0);
+  const long long j = g.gw + jl;
+  const bool p2 = is_pow2(N);
+  double2* in = sbuf;
+  const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
+  for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
+    const int kl = e % KC;
+    const int il = e / KC;
+    if (kl >= kc) continue;
+    const long long k = g.gw + k0 + kl;
+    const long long ijk = (g.gw + il) * g.is + j * g.js + k;
+    // second_order_divergence (PressureSolver.pyx:138-175), d = 0, 1, 2
+    const double ah = a.alpha0_half[k];
+    double d = 0.0;
+    d += (a.u[ijk] / ah - a.u[ijk - g.is] / ah) * dxi0;
+    d += (a.v[ijk] / ah - a.v[ijk - g.js] / ah) * dxi1;
+    d += ((a.w[ijk]) / a.alpha0[k] - (a.w[ijk - 1]) / a.alpha0[k - 1]) * dxi2;
+    a.div[ijk] = d;
+    in[kl * N + slot(il, N, a.log0)] = make_double2(d, 0.0);
+  }
+  __syncthreads();
+  double2* res = in;
+  if (p2) {
+    fft_pow2_lines(in, kc, N, a.log0, a.twx, false);
+  } else {
+    res = in + N * KC;
+    dft_lines(in, res, kc, N, a.twx, false);
+  }
+  const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
+  for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
+    const int il = e % N;
+    const int kl = e / N;
+    a.spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il] = res[kl * N + il];
+  }
+}
+
+// ---- y-FFT over W[k][j][i] lines along j, IC columns i per block ----------
+__global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, bool inverse) {
+  extern __shared__ double2 sbuf[];
+  const int Nx = (int)(g.n0 - 2 * g.gw);
+  const int N = (int)(g.n1 - 2 * g.gw);
+  const int kk = blockIdx.y;
+  const int i0 = blockIdx.x * IC;
+  const int ic = min(IC, Nx - i0);
+  const bool p2 = is_pow2(N);
+  double2* in = sbuf;
+  double2* plane = a.spec + (long long)kk * N * Nx;
+  for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
+    const int il = e % IC;
+    const int jl = e / IC;
+    if (il >= ic) continue;
+    in[il * N + slot(jl, N, a.log1)] = plane[(long long)jl * Nx + i0 + il];
+  }
+  __syncthreads();
+  double2* res = in;
+  if (p2) {
+    fft_pow2_lines(in, ic, N, a.log1, a.twy, inverse);
+  } else {
+    res = in + N * IC;
+    dft_lines(in, res, ic, N, a.twy, inverse);
+  }
+  const double sc = inverse ? 1.0 / (double)N : 1.0;
+  for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
+    const int il = e % IC;
+    const int jl = e / IC;
+    if (il >= ic) continue;
+    double2 r = res[il * N + jl];
+    if (inverse) {
+      r.x *= sc;
+      r.y *= sc;
+    }
+    plane[(long long)jl * Nx + i0 + il] = r;
+  }
+}
+
+// ---- per-column tridiagonal solve ------------------------------------------
+// Matrix of PressureFFTParallel.compute_off_diagonals (:100-127) and
+// compute_diagonal (:129-148); Thomas algorithm of TDMA.solve applied to the
+// real and imaginary parts (the matrix is real, so both share m and scratch).
+__global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
+  const int Nx = (int)(g.n0 - 2 * g.gw);
+  const int Ny = (int)(g.n1 - 2 * g.gw);
+  const int nz = (int)(g.n2 - 2 * g.gw);
+  const long long ncol = (long long)Nx * Ny;
+  const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  const int i = (int)(col % Nx);
+  const int j = (int)(col / Nx);
+  double2* x = a.spec + col;
+  double* scr = a.scr + col;
+  if (i == 0 && j == 0) {  // mode (0,0) is set to zero (:197-200)
+    for (int k = 0; k < nz; ++k) x[(long long)k * ncol] = make_double2(0.0, 0.0);
+    return;
+  }
+  const long long gw = g.gw;
+  const double dzi = g.dxi2;
+  const double kk = a.kx2[i] + a.ky2[j];
+  const double* rho0 = a.rho0;
+  const double* rho0h = a.rho0_half;
+  // row 0 (for a single level the last-row formulas overwrite it, :119-127, :145-146)
+  double b, c;
+  if (nz > 1) {
+    b = (rho0h[gw] * kk - (rho0[gw]) * dzi * dzi);
+    c = dzi * dzi * rho0[gw];
+  } else {
+    b = (rho0h[gw] * kk - (rho0[gw - 1]) * dzi * dzi);
+    c = 0.0;
+  }
+  double s_prev = c / b;
+  double2 xp = x[0];
+  xp.x = xp.x / b;
+  xp.y = xp.y / b;
+  x[0] = xp;
+  scr[0] = s_prev;
+  for (int k = 1; k < nz; ++k) {
+    const double ak = dzi * dzi * rho0[k + gw - 1];
+    double ck, bk;
+    if (k < nz - 1) {
+      ck = dzi * dzi * rho0[k + gw];
+      bk = (rho0h[k + gw] * kk - (rho0[k + gw] + rho0[k + gw - 1]) * dzi * dzi);
+    } else {
+      ck = 0.0;
+      bk = (rho0h[k + gw] * kk - (rho0[k + gw - 1]) * dzi * dzi);
+    }
+    const double m = 1.0 / (bk - ak * s_prev);
+    s_prev = ck * m;
+    scr[(long long)k * ncol] = s_prev;
+    double2 xk = x[(long long)k * ncol];
+    xk.x = (xk.x - ak * xp.x) * m;
+    xk.y = (xk.y - ak * xp.y) * m;
+    x[(long long)k * ncol] = xk;
+    xp = xk;
+  }
+  for (int k = nz - 2; k >= 0; --k) {
+    const double sk = scr[(long long)k * ncol];
+    double2 xk = x[(long long)k * ncol];
+    xk.x = xk.x - sk * xp.x;
+    xk.y = xk.y - sk * xp.y;
+    x[(long long)k * ncol] = xk;
+    xp = xk;
+  }
+}
+
+// ---- inverse x-FFT -> pressure ---------------------------------------------
+__global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC) {
+  extern __shared__ double2 sbuf[];
+  const int N = (int)(g.n0 - 2 * g.gw);
+  const int nz = (int)(g.n2 - 2 * g.gw);
+  const int jl = blockIdx.x;
+  const int k0 = blockIdx.y * KC;
+  const int kc = min(KC, nz - k0);
+  const bool p2 = is_pow2(N);
+  double2* in = sbuf;
+  const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
+  for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
+    const int il = e % N;
+    const int kl = e / N;
+    in[kl * N + slot(il, N, a.log0)] = a.spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il];
+  }
+  __syncthreads();
+  double2* res = in;
+  if (p2) {
+    fft_pow2_lines(in, kc, N, a.log0, a.twx, true);
+  } else {
+    res = in + N * KC;
+    dft_lines(in, res, kc, N, a.twx, true);
+  }
+  const double sc = 1.0 / (double)N;
+  const long long j = g.gw + jl;
+  for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
+    const int kl = e % KC;
+    const int il = e / KC;
+    if (kl >= kc) continue;
+    const long long ijk = (g.gw + il) * g.is + j * g.js + g.gw + k0 + kl;
+    a.p[ijk] = res[kl * N + il].x * sc;
+  }
+}
+
+// ---- pressure ghost fill (sym), communicate_variable on one rank -----------
+__global__ void ghost_sym(Geo g, double* __restrict__ f, long long nghost) {
+  const long long gw = g.gw, n0 = g.n0, n1 = g.n1, n2 = g.n2;
+  const long long nl0 = n0 - 2 * gw, nl1 = n1 - 2 * gw;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nghost; t += stride) {
+    long long i, j, k;
+    ghost_decode(g, t, i, j, k);
+    const long long is_ = (i < gw) ? i + nl0 : ((i >= n0 - gw) ? i - nl0 : i);
+    const long long js_ = (j < gw) ? j + nl1 : ((j >= n1 - gw) ? j - nl1 : j);
+    long long ks = k;
+    if (k >= n2 - gw) ks = n2 - gw - 1 - (k - (n2 - gw));
+    else if (k < gw) ks = gw + (gw - 1 - k);
+    f[i * g.is + j * g.js + k] = f[is_ * g.is + js_ * g.js + ks];
+  }
+}
+
+// ---- second_order_pressure_correction (PressureSolver.pyx:83-110) ---------
+__global__ void correction(Geo g, const double* __restrict__ p, double* __restrict__ u, double* __restrict__ v,
+                           double* __restrict__ w) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < g.npg; t += stride) {
+    const long long k = t % g.n2;
+    const long long r = t / g.n2;
+    const long long j = r % g.n1;
+    const long long i = r / g.n1;
+    if (i >= g.n0 - 1 || j >= g.n1 - 1 || k >= g.n2 - 1) continue;
+    const double pc = p[t];
+    u[t] -= (p[t + g.is] - pc) * g.dxi0;
+    v[t] -= (p[t + g.js] - pc) * g.dxi1;
+    w[t] -= (p[t + 1] - pc) * g.dxi2;
+  }
+}
+
+int ilog2_exact(long long n) {
+  int l = 0;
+  while ((1LL << l) < n) ++l;
+  return l;
+}
+
+int stream_blocks(long long work) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long b = (work + 255) / 256;
+  if (b > (long long)sms * 8) b = (long long)sms * 8;
+  return (int)(b < 1 ? 1 : b);
+}
+
+bool pow2(long long n) { return (n & (n - 1)) == 0; }
+
+size_t fft_smem(long long N, int lines) {
+  return (size_t)(pow2(N) ? 1 : 2) * (size_t)N * lines * sizeof(double2);
+}
+
+int lines_for(long long N) {
+  // keep one FFT block's shared memory at or below 64 KiB when possible
+  long long per = (pow2(N) ? 1 : 2) * N * 16;
+  int L = (int)(65536 / per);
+  if (L > 8) L = 8;
+  if (L < 1) L = 1;
+  return L;
+}
+
+}  // namespace
+
+extern "C" long long pb_pressure_workspace_bytes(const pb_dims* dims) {
+  if (pb_check_dims(dims)) return -1;
+  return playout(dims).total;
+}
+
+// PressureFFTParallel.initialize (:27-62): the modified wave numbers
+// (compute_modified_wave_numbers, :64-98) are evaluated on the host with the
+// C library cos, as the reference does, so they match it bit for bit; the
+// FFT twiddles exp(-2 pi i m/N) are evaluated in long double and rounded.
+extern "C" int pb_pressure_init(const pb_dims* dims, void* workspace, long long workspace_bytes) {
+  int rc = pb_check_dims(dims);
+  if (rc) return rc;
+  const PLayout L = playout(dims);
+  if (!workspace || workspace_bytes < L.total) return PB_ERR_WORKSPACE;
+  if (reinterpret_cast<uintptr_t>(workspace) & 255) return PB_ERR_WORKSPACE;
+  const double pi = 3.141592653589793;
+  char* base = static_cast<char*>(workspace);
+  for (int dim = 0; dim < 2; ++dim) {
+    const long n = dims->n[dim];
+    std::vector<double> k2(n);
+    std::vector<double2> tw(n);
+    for (long ii = 0; ii < n; ++ii) {
+      const long i = dims->indx_lo[dim] + ii;
+      double xi;
+      if ((double)i <= (double)n / 2.0) xi = (double)i;
+      else xi = (double)(i - n);
+      k2[ii] = (2.0 * cos((2.0 * pi / (double)n) * xi) - 2.0) / dims->dx[dim] / dims->dx[dim];
+      const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)ii / (long double)n;
+      tw[ii] = make_double2((double)cosl(ang), (double)sinl(ang));
+    }
+    if (dims->indx_lo[dim] == 0) k2[0] = 0.0;
+    PB_CUDA_TRY(cudaMemcpy(base + (dim == 0 ? L.kx2 : L.ky2), k2.data(), n * sizeof(double),
+                           cudaMemcpyHostToDevice));
+    PB_CUDA_TRY(cudaMemcpy(base + (dim == 0 ? L.twx : L.twy), tw.data(), n * sizeof(double2),
+                           cudaMemcpyHostToDevice));
+  }
+  return PB_OK;
+}
+
+static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                               const double* alpha0, const double* alpha0_half, double* u, double* v, double* w,
+                               double* divergence, double* dynamic_pressure, char* base, cudaStream_t st) {
+  const Geo g = make_geo(dims);
+  const PLayout L = playout(dims);
+  PArgs a;
+  a.rho0 = rho0;
+  a.rho0_half = rho0_half;
+  a.alpha0 = alpha0;
+  a.alpha0_half = alpha0_half;
+  a.u = u;
+  a.v = v;
+  a.w = w;
+  a.div = divergence;
+  a.p = dynamic_pressure;
+  a.partial = reinterpret_cast<double*>(base + L.partial);
+  a.mean = reinterpret_cast<double*>(base + L.mean);
+  a.twx = reinterpret_cast<const double2*>(base + L.twx);
+  a.twy = reinterpret_cast<const double2*>(base + L.twy);
+  a.kx2 = reinterpret_cast<const double*>(base + L.kx2);
+  a.ky2 = reinterpret_cast<const double*>(base + L.ky2);
+  a.spec = reinterpret_cast<double2*>(base + L.spec);
+  a.scr = reinterpret_cast<double*>(base + L.scr);
+  const long long Nx = dims->n[0], Ny = dims->n[1], nz = dims->n[2];
+  a.log0 = ilog2_exact(Nx);
+  a.log1 = ilog2_exact(Ny);
+  const long long nghost = g.npg - Nx * Ny * nz;
+
+  hmean_partial<<<kPartials, 256, 0, st>>>(g, w, a.partial);
+  pb_note_launch();
+  hmean_final<<<1, 256, 0, st>>>(g, a.partial, a.mean, kPartials, 1.0 / (double)(Ny * Nx));
+  pb_note_launch();
+  remove_mean<<<stream_blocks(g.npg), 256, 0, st>>>(g, w, a.mean);
+  pb_note_launch();
+  if (nghost > 0) {
+    zero_ghosts<<<stream_blocks(nghost), 256, 0, st>>>(g, divergence, nghost);
+    pb_note_launch();
+  }
+  PB_LAUNCH_CHECK();
+
+  const int KC = lines_for(Nx);
+  const size_t smx = fft_smem(Nx, KC);
+  if (smx > 48 * 1024) {
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+  }
+  fft_x_fwd<<<dim3((unsigned)Ny, ceil_div(nz, KC)), kFftThreads, smx, st>>>(g, a, KC);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  const int IC = lines_for(Ny);
+  const size_t smy = fft_smem(Ny, IC);
+  if (smy > 48 * 1024)
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+  fft_y<<<dim3(ceil_div(Nx, IC), (unsigned)nz), kFftThreads, smy, st>>>(g, a, IC, false);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  tdma_kernel<<<ceil_div(Nx * Ny, 256), 256, 0, st>>>(g, a);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  fft_y<<<dim3(ceil_div(Nx, IC), (unsigned)nz), kFftThreads, smy, st>>>(g, a, IC, true);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  fft_x_inv<<<dim3((unsigned)Ny, ceil_div(nz, KC)), kFftThreads, smx, st>>>(g, a, KC);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  if (nghost > 0) {
+    ghost_sym<<<stream_blocks(nghost), 256, 0, st>>>(g, dynamic_pressure, nghost);
+    pb_note_launch();
+  }
+  correction<<<stream_blocks(g.npg), 256, 0, st>>>(g, dynamic_pressure, u, v, w);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  return PB_OK;
+}
+
+extern "C" int pb_pressure_solve(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                                 const double* alpha0, const double* alpha0_half, double* u, double* v, double* w,
+                                 double* divergence, double* dynamic_pressure, void* workspace,
+                                 long long workspace_bytes, int precision, void* stream) {
+  int rc = pb_check_dims(dims);
+  if (rc) return rc;
+  if (!rho0 || !rho0_half || !alpha0 || !alpha0_half || !u || !v || !w || !divergence || !dynamic_pressure)
+    return PB_ERR_ARG;
+  if (precision != PB_FP64) return PB_ERR_UNSUPPORTED;
+  const PLayout L = playout(dims);
+  if (!workspace || workspace_bytes < L.total) return PB_ERR_WORKSPACE;
+  if (reinterpret_cast<uintptr_t>(workspace) & 255) return PB_ERR_WORKSPACE;
+  if ((!pow2(dims->n[0]) && dims->n[0] > 1024) || (!pow2(dims->n[1]) && dims->n[1] > 1024)) return PB_ERR_UNSUPPORTED;
+  if (dims->n[0] > 8192 || dims->n[1] > 8192) return PB_ERR_UNSUPPORTED;
+  return pressure_solve_impl(dims, rho0, rho0_half, alpha0, alpha0_half, u, v, w, divergence, dynamic_pressure,
+                             static_cast<char*>(workspace), as_stream(stream));
+}

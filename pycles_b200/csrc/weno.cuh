@@ -1,0 +1,123 @@
+// WENO and central interpolants, Csrc/advection_interpolation.h.
+//
+// The FP64 forms keep the reference's term order (the compiler may contract
+// a*b+c into FMAs, which moves results by at most a few ulp).  The FP32
+// forms are used by the precision path through weno5_mixed / weno7_mixed:
+// the stencil is shifted by its centre value in FP64, the WENO arithmetic
+// (candidate polynomials, smoothness indicators, weights) runs in FP32 on
+// the differences, and the centre is added back in FP64.  WENO is exactly
+// invariant to that shift in real arithmetic, and working on differences
+// keeps the FP32 smoothness indicators free of the rounding noise of the
+// absolute values.
+#pragma once
+
+template <typename R>
+__device__ __forceinline__ R interp_4(R phim1, R phi, R phip1, R phip2) {
+  // advection_interpolation.h:12-14
+  return R(7.0 / 12.0) * (phi + phip1) - R(1.0 / 12.0) * (phim1 + phip2);
+}
+
+template <typename R>
+__device__ __forceinline__ R interp_6(R phim2, R phim1, R phi, R phip1, R phip2, R phip3) {
+  // advection_interpolation.h:20-24
+  return (R(37.0 / 60.0) * (phi + phip1) - R(2.0 / 15.0) * (phim1 + phip2) +
+          R(1.0 / 60.0) * (phim2 + phip3));
+}
+
+template <typename R>
+__device__ __forceinline__ R weno5(R phim2, R phim1, R phi, R phip1, R phip2) {
+  // advection_interpolation.h:79-104
+  const R p0 = R(1.0 / 3.0) * phim2 - R(7.0 / 6.0) * phim1 + R(11.0 / 6.0) * phi;
+  const R p1 = R(-1.0 / 6.0) * phim1 + R(5.0 / 6.0) * phi + R(1.0 / 3.0) * phip1;
+  const R p2 = R(1.0 / 3.0) * phi + R(5.0 / 6.0) * phip1 - R(1.0 / 6.0) * phip2;
+  const R a2 = phi - R(2.0) * phip1 + phip2;
+  const R b2 = R(3.0) * phi - R(4.0) * phip1 + phip2;
+  const R beta2 = R(13.0 / 12.0) * a2 * a2 + R(0.25) * b2 * b2;
+  const R a1 = phim1 - R(2.0) * phi + phip1;
+  const R b1 = phim1 - phip1;
+  const R beta1 = R(13.0 / 12.0) * a1 * a1 + R(0.25) * b1 * b1;
+  const R a0 = phim2 - R(2.0) * phim1 + phi;
+  const R b0 = phim2 - R(4.0) * phim1 + R(3.0) * phi;
+  const R beta0 = R(13.0 / 12.0) * a0 * a0 + R(0.25) * b0 * b0;
+  const R e0 = beta0 + R(1e-10);
+  const R e1 = beta1 + R(1e-10);
+  const R e2 = beta2 + R(1e-10);
+  const R alpha0 = R(0.1) / (e0 * e0);
+  const R alpha1 = R(0.6) / (e1 * e1);
+  const R alpha2 = R(0.3) / (e2 * e2);
+  const R alpha_sum_inv = R(1.0) / (alpha0 + alpha1 + alpha2);
+  const R w0 = alpha0 * alpha_sum_inv;
+  const R w1 = alpha1 * alpha_sum_inv;
+  const R w2 = alpha2 * alpha_sum_inv;
+  return w0 * p0 + w1 * p1 + w2 * p2;
+}
+
+template <typename R>
+__device__ __forceinline__ R weno7(R phim3, R phim2, R phim1, R phi, R phip1, R phip2, R phip3) {
+  // advection_interpolation.h:106-145
+  const R p0 = R(-1.0 / 4.0) * phim3 + R(13.0 / 12.0) * phim2 + R(-23.0 / 12.0) * phim1 +
+               R(25.0 / 12.0) * phi;
+  const R p1 = R(1.0 / 12.0) * phim2 + R(-5.0 / 12.0) * phim1 + R(13.0 / 12.0) * phi +
+               R(1.0 / 4.0) * phip1;
+  const R p2 = R(-1.0 / 12.0) * phim1 + R(7.0 / 12.0) * phi + R(7.0 / 12.0) * phip1 +
+               R(-1.0 / 12.0) * phip2;
+  const R p3 = R(1.0 / 4.0) * phi + R(13.0 / 12.0) * phip1 + R(-5.0 / 12.0) * phip2 +
+               R(1.0 / 12.0) * phip3;
+  const R beta0 = (phim3 * (R(547.0) * phim3 - R(3882.0) * phim2 + R(4642.0) * phim1 - R(1854.0) * phi) +
+                   phim2 * (R(7043.0) * phim2 - R(17246.0) * phim1 + R(7042.0) * phi) +
+                   phim1 * (R(11003.0) * phim1 - R(9402.0) * phi) + R(2107.0) * phi * phi);
+  const R beta1 = (phim2 * (R(267.0) * phim2 - R(1642.0) * phim1 + R(1602.0) * phi - R(494.0) * phip1) +
+                   phim1 * (R(2843.0) * phim1 - R(5966.0) * phi + R(1922.0) * phip1) +
+                   phi * (R(3443.0) * phi - R(2522.0) * phip1) + R(547.0) * phip1 * phip1);
+  const R beta2 = (phim1 * (R(547.0) * phim1 - R(2522.0) * phi + R(1922.0) * phip1 - R(494.0) * phip2) +
+                   phi * (R(3443.0) * phi - R(5966.0) * phip1 + R(1602.0) * phip2) +
+                   phip1 * (R(2843.0) * phip1 - R(1642.0) * phip2) + R(267.0) * phip2 * phip2);
+  const R beta3 = (phi * (R(2107.0) * phi - R(9402.0) * phip1 + R(7042.0) * phip2 - R(1854.0) * phip3) +
+                   phip1 * (R(11003.0) * phip1 - R(17246.0) * phip2 + R(4642.0) * phip3) +
+                   phip2 * (R(7043.0) * phip2 - R(3882.0) * phip3) + R(547.0) * phip3 * phip3);
+  const R e0 = beta0 + R(1e-10);
+  const R e1 = beta1 + R(1e-10);
+  const R e2 = beta2 + R(1e-10);
+  const R e3 = beta3 + R(1e-10);
+  const R alpha0 = R(1.0 / 35.0) / (e0 * e0);
+  const R alpha1 = R(12.0 / 35.0) / (e1 * e1);
+  const R alpha2 = R(18.0 / 35.0) / (e2 * e2);
+  const R alpha3 = R(4.0 / 35.0) / (e3 * e3);
+  const R alpha_sum_inv = R(1.0) / (alpha0 + alpha1 + alpha2 + alpha3);
+  const R w0 = alpha0 * alpha_sum_inv;
+  const R w1 = alpha1 * alpha_sum_inv;
+  const R w2 = alpha2 * alpha_sum_inv;
+  const R w3 = alpha3 * alpha_sum_inv;
+  return w0 * p0 + w1 * p1 + w2 * p2 + w3 * p3;
+}
+
+// Face value from a stencil held in an array: ORDER 5 reads v[0..4]
+// (upwind-positive: centre v[2]), ORDER 7 reads v[0..6] (centre v[3]).
+// F32 selects the shifted mixed-precision evaluation described above.
+template <int ORDER, bool F32>
+__device__ __forceinline__ double weno_face(double a0, double a1, double a2, double a3, double a4,
+                                            double a5 = 0.0, double a6 = 0.0) {
+  if constexpr (ORDER == 5) {
+    if constexpr (!F32) {
+      return weno5<double>(a0, a1, a2, a3, a4);
+    } else {
+      const float r = weno5<float>((float)(a0 - a2), (float)(a1 - a2), 0.0f, (float)(a3 - a2),
+                                   (float)(a4 - a2));
+      return a2 + (double)r;
+    }
+  } else {
+    if constexpr (!F32) {
+      return weno7<double>(a0, a1, a2, a3, a4, a5, a6);
+    } else {
+      const float r = weno7<float>((float)(a0 - a3), (float)(a1 - a3), (float)(a2 - a3), 0.0f,
+                                   (float)(a4 - a3), (float)(a5 - a3), (float)(a6 - a3));
+      return a3 + (double)r;
+    }
+  }
+}
+
+// Upwind face flux 0.5*((u+|u|)phi+ + (u-|u|)phi-)*rho
+// (Csrc/scalar_advection.h:363 and momentum_advection_weno.h:172).
+__device__ __forceinline__ double upwind_flux(double vel, double phip, double phim, double rho) {
+  return 0.5 * ((vel + fabs(vel)) * phip + (vel - fabs(vel)) * phim) * rho;
+}

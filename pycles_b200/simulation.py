@@ -1,0 +1,123 @@
+"""Hot-path driver: Simulation3d.run (Simulation3d.pyx:140-189) restricted to
+the components built here, in the reference's order per RK stage.
+
+    sim = HotPathSimulation(namelist)
+    sim.initialize()          # reference state + seeded initial condition
+    sim.run(nsteps)           # as Simulation3d.run (pre-loop bcs + Th.update)
+    sim.step()                # one time step = three RK stages
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _capi, cases
+from .advection import MomentumAdvection, ScalarAdvection
+from .grid import Grid
+from .pressure import PressureSolver
+from .reference_state import ReferenceState
+from .thermodynamics import ThermodynamicsDry, ThermodynamicsSA
+from .time_stepping import TimeStepping
+from .variables import DiagnosticVariables, PrognosticVariables
+
+
+def namelist_for(case: str, nx: int, ny: int, nz: int, dx: float, dy: float, dz: float, gw: int = 3,
+                 dt: float = 1.0, scalar_order: int = 5, momentum_order: int = 5, precision: str = "fp64"):
+    return {
+        "case": case,
+        "grid": {"dims": 3, "nx": nx, "ny": ny, "nz": nz, "gw": gw, "dx": dx, "dy": dy, "dz": dz},
+        "scalar_transport": {"order": scalar_order},
+        "momentum_transport": {"order": momentum_order},
+        "time_stepping": {"ts_type": 3, "dt_initial": dt, "dt_max": dt, "t_max": 1e30},
+        "thermodynamics": {"do_qt_clipping": True},
+        "gpu": {"precision": precision},
+    }
+
+
+# the measured configurations (synthetic seeded states of these shapes)
+CONFIGS = {
+    "c1_dry_cbl": dict(case="dry_cbl", nx=32, ny=32, nz=32, dx=50.0, dy=50.0, dz=50.0, gw=3, dt=0.5),
+    "c2_bomex": dict(case="bomex", nx=64, ny=64, nz=75, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0),
+    "c3_bomex": dict(case="bomex", nx=256, ny=256, nz=128, dx=50.0, dy=50.0, dz=20.0, gw=3, dt=1.0),
+    "c5_dycoms": dict(case="dycoms", nx=512, ny=512, nz=256, dx=35.0, dy=35.0, dz=5.0, gw=4, dt=0.25,
+                      scalar_order=7, momentum_order=5),
+}
+
+
+class HotPathSimulation:
+    def __init__(self, namelist, device="cuda"):
+        self.namelist = namelist
+        self.device = torch.device(device)
+        self.case = namelist.get("case", "bomex")
+        Gr = self.Gr = Grid(namelist)
+        Gr.device = self.device
+        self.PV = PrognosticVariables(Gr)
+        self.DV = DiagnosticVariables()
+        self.moist = self.case != "dry_cbl"
+        self.Th = ThermodynamicsSA(namelist) if self.moist else ThermodynamicsDry(namelist)
+        self.SA = ScalarAdvection(namelist)
+        self.MA = MomentumAdvection(namelist)
+        self.Pr = PressureSolver()
+        self.TS = TimeStepping()
+        self.RS = ReferenceState(Gr)
+        PV = self.PV
+        PV.add_variable("u", "m/s", "u", "u velocity component", "sym", "velocity")
+        PV.set_velocity_direction("u", 0)
+        PV.add_variable("v", "m/s", "v", "v velocity component", "sym", "velocity")
+        PV.set_velocity_direction("v", 1)
+        PV.add_variable("w", "m/s", "w", "w velocity component", "asym", "velocity")
+        PV.set_velocity_direction("w", 2)
+        self.Th.initialize(Gr, PV, self.DV)
+        self.Pr.initialize(namelist, Gr, self.RS, self.DV)
+        PV.initialize(Gr, device=self.device)
+        self.DV.initialize(Gr, device=self.device)
+        self.SA.initialize(Gr, PV)
+        self.MA.initialize(Gr, PV)
+        self.TS.initialize(namelist, PV)
+        _capi.load()
+
+    # state ---------------------------------------------------------------
+    def initialize(self, seed=0):
+        """Reference state + seeded initial condition of the case."""
+        fields = cases.CASES[self.case](self.Gr, self.RS, self.Th, seed=seed)
+        self.load_fields(fields)
+        return fields
+
+    def load_fields(self, fields: dict):
+        for name, arr in fields.items():
+            self.PV.field(name, self.Gr).copy_(torch.as_tensor(np.ascontiguousarray(arr), dtype=torch.float64))
+
+    def set_reference_state(self, profiles: dict):
+        self.RS.set_profiles(profiles, device=self.device)
+
+    def host_fields(self) -> dict:
+        return {n: self.PV.field(n, self.Gr).cpu().numpy() for n in self.PV.index_name}
+
+    # time stepping ---------------------------------------------------------
+    def stage(self, rk_step: int, stream=None):
+        """One RK stage in the order of Simulation3d.pyx:159-178."""
+        Gr, PV, DV, RS = self.Gr, self.PV, self.DV, self.RS
+        self.Th.update(Gr, RS, PV, DV, stream=stream)
+        self.SA.update(Gr, RS, PV, DV, stream=stream)
+        self.MA.update(Gr, RS, PV, stream=stream)
+        self.TS.rk_step = rk_step
+        self.TS.update(Gr, PV, stream=stream)
+        PV.Update_all_bcs(Gr, stream=stream)
+        self.Pr.update(Gr, RS, DV, PV, stream=stream)
+
+    def step(self, stream=None):
+        for rk in range(self.TS.n_rk_steps):
+            self.stage(rk, stream=stream)
+
+    def run(self, nsteps: int, stream=None):
+        """Simulation3d.run: ghost fill and a thermodynamics update before the
+        loop (its first output), then nsteps time steps."""
+        self.PV.Update_all_bcs(self.Gr, stream=stream)
+        self.Th.update(self.Gr, self.RS, self.PV, self.DV, stream=stream)
+        for _ in range(nsteps):
+            self.step(stream=stream)
+
+    def check_device_errors(self):
+        word = _capi.get_error()
+        if word:
+            raise _capi.PbError(f"device error word 0x{word:x} (table range=1, secant cap=2, non-finite=4)")

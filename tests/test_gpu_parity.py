@@ -1,0 +1,215 @@
+"""GPU parity: every hot-path component through the C ABI against the CPU
+oracle (numpy restatement, itself pinned to the reference's compiled C) on
+the same seeded inputs.
+
+Tolerances (relative L2 per field):
+  * prognostic / diagnostic fields after one call, FP64 plain form: 1e-12
+  * tendencies (differences of O(flux) terms, so FMA-contraction rounding is
+    amplified by flux/tendency): 1e-10
+"""
+import numpy as np
+import pytest
+
+from helpers import gpu_dv, gpu_fields, gpu_sim, gpu_tends, host_case, oracle_sim, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-12
+TEND_TOL = 1e-10
+
+MOIST_SMALL = dict(case="bomex", nx=16, ny=12, nz=20, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
+MOIST_W7 = dict(case="bomex", nx=12, ny=16, nz=18, dx=100.0, dy=100.0, dz=40.0, gw=4, dt=1.0,
+                scalar_order=7, momentum_order=7)
+DRY_SMALL = dict(case="dry_cbl", nx=16, ny=16, nz=16, dx=50.0, dy=50.0, dz=50.0, gw=3, dt=0.5)
+ODD = dict(case="bomex", nx=12, ny=10, nz=14, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
+
+
+def _stir(fields, seed=1, amp=0.5):
+    """Add seeded velocity structure so that every advection branch is hit."""
+    rng = np.random.default_rng(seed)
+    out = dict(fields)
+    for n in ("u", "v", "w"):
+        out[n] = fields[n] + amp * rng.standard_normal(fields[n].shape)
+    return out
+
+
+def _setup(cfg, stir=True, seed=0):
+    nl, rs, f = host_case(**cfg, seed=seed)
+    if stir:
+        f = _stir(f)
+    return nl, rs, f
+
+
+def _bcs_both(o, g):
+    o.update_all_bcs()
+    g.PV.Update_all_bcs(g.Gr)
+
+
+@pytest.mark.parametrize("cfg", [MOIST_SMALL, ODD, MOIST_W7], ids=["weno5", "odd", "weno7"])
+def test_scalar_advection(cfg):
+    nl, rs, f = _setup(cfg)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    _bcs_both(o, g)
+    o.sa_update()
+    g.SA.update(g.Gr, g.RS, g.PV, g.DV)
+    gt = gpu_tends(g)
+    for n in ("s", "qt"):
+        assert rel_l2(gt[n], o.tend(n)) < TEND_TOL, n
+
+
+@pytest.mark.parametrize("cfg", [MOIST_SMALL, ODD, MOIST_W7], ids=["weno5", "odd", "weno7"])
+def test_momentum_advection(cfg):
+    nl, rs, f = _setup(cfg)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    _bcs_both(o, g)
+    o.ma_update()
+    g.MA.update(g.Gr, g.RS, g.PV)
+    gt = gpu_tends(g)
+    for n in ("u", "v", "w"):
+        assert rel_l2(gt[n], o.tend(n)) < TEND_TOL, n
+
+
+def test_scalar_fluxes_exposed():
+    """ScalarAdvection.flux on the faces the divergence reads."""
+    import torch
+    nl, rs, f = _setup(MOIST_SMALL)
+    nl["gpu"] = {"keep_scalar_fluxes": True}
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    g.SA.keep_fluxes = True
+    g.SA.initialize(g.Gr, g.PV)
+    _bcs_both(o, g)
+    o.sa_update()
+    g.SA.update(g.Gr, g.RS, g.PV, g.DV)
+    torch.cuda.synchronize()
+    gf = g.SA.flux.cpu().numpy().reshape(2, 3, *g.Gr.shape)
+    of = o.flux.reshape(2, 3, *g.Gr.shape)
+    gw = nl["grid"]["gw"]
+    sh = g.Gr.shape
+    for d in range(3):
+        sl = [slice(gw, sh[a] - gw) for a in range(3)]
+        sl[d] = slice(gw - 1, sh[d] - gw)
+        assert rel_l2(gf[(slice(None), d) + tuple(sl)], of[(slice(None), d) + tuple(sl)]) < 1e-13
+
+
+def test_thermo_sa():
+    nl, rs, f = _setup(MOIST_SMALL, stir=False)
+    # raise qt so that part of the column is saturated
+    f = dict(f)
+    f["qt"] = f["qt"] + 6e-3
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    _bcs_both(o, g)
+    o.th_update()
+    g.Th.update(g.Gr, g.RS, g.PV, g.DV)
+    gd, gt = gpu_dv(g), gpu_tends(g)
+    assert (o.dv["ql"] > 0).any() and (o.dv["ql"] == 0).any()
+    for n in ("temperature", "qv", "ql", "alpha", "buoyancy", "theta_rho", "buoyancy_frequency", "thetali"):
+        assert rel_l2(gd[n], o.dv[n]) < FIELD_TOL, n
+    assert rel_l2(gt["w"], o.tend("w")) < FIELD_TOL
+    assert np.array_equal(gd["qi"] == 0, o.dv["qi"] == 0)
+    it = g.Th.iter_stats.cpu().numpy()
+    assert it[1] == int((o.dv["ql"] > 0).sum()) or it[1] >= int((o.dv["ql"] > 0).sum())
+    assert it[0] == int(o.secant_iters.sum())
+
+
+def test_thermo_dry():
+    nl, rs, f = _setup(DRY_SMALL, stir=False)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    _bcs_both(o, g)
+    o.th_update()
+    g.Th.update(g.Gr, g.RS, g.PV, g.DV)
+    gd, gt = gpu_dv(g), gpu_tends(g)
+    for n in ("temperature", "alpha", "buoyancy", "theta", "buoyancy_frequency"):
+        assert rel_l2(gd[n], o.dv[n]) < FIELD_TOL, n
+    assert rel_l2(gt["w"], o.tend("w")) < FIELD_TOL
+
+
+def test_ghost_fill_exact():
+    nl, rs, f = _setup(ODD)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    _bcs_both(o, g)
+    gf = gpu_fields(g)
+    for n in o.names:
+        assert np.array_equal(gf[n], o.var(n)), n
+
+
+def test_rk3_stages():
+    nl, rs, f = _setup(MOIST_SMALL)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    rng = np.random.default_rng(3)
+    tend = rng.standard_normal(o.tendencies.shape)
+    import torch
+    for rk in range(3):
+        o.tendencies[:] = tend * (rk + 1)
+        g.PV.tendencies.copy_(torch.as_tensor(tend * (rk + 1)))
+        o.ts_update(rk)
+        g.TS.rk_step = rk
+        g.TS.update(g.Gr, g.PV)
+        gf = gpu_fields(g)
+        for n in o.names:
+            assert rel_l2(gf[n], o.var(n)) < 1e-15, (rk, n)
+        assert float(g.PV.tendencies.abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("cfg", [MOIST_SMALL, ODD, DRY_SMALL], ids=["pow2ish", "odd", "dry"])
+def test_pressure(cfg):
+    nl, rs, f = _setup(cfg)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    _bcs_both(o, g)
+    o.pr_update()
+    g.Pr.update(g.Gr, g.RS, g.DV, g.PV)
+    gf, gd = gpu_fields(g), gpu_dv(g)
+    assert rel_l2(gd["divergence"], o.dv["divergence"]) < FIELD_TOL
+    assert rel_l2(gd["dynamic_pressure"], o.dv["dynamic_pressure"]) < 1e-11
+    for n in ("u", "v", "w"):
+        assert rel_l2(gf[n], o.var(n)) < FIELD_TOL, n
+
+
+@pytest.mark.parametrize("cfg", [MOIST_SMALL, DRY_SMALL, MOIST_W7], ids=["moist", "dry", "weno7"])
+def test_one_step(cfg):
+    """The plain-form gate: every prognostic field after one full step
+    (three RK stages of the hot path) within 1e-12 relative L2."""
+    nl, rs, f = _setup(cfg, stir=False)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    _bcs_both(o, g)
+    o.step()
+    g.step()
+    gf = gpu_fields(g)
+    for n in o.names:
+        assert rel_l2(gf[n], o.var(n)) < FIELD_TOL, n
+
+
+def test_run_matches_simulation3d_prologue():
+    """run(): ghost fill + thermodynamics before the loop, as Simulation3d.run."""
+    nl, rs, f = _setup(MOIST_SMALL, stir=False)
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    o.update_all_bcs()
+    o.th_update()
+    o.step()
+    o.step()
+    g.run(2)
+    gf = gpu_fields(g)
+    for n in o.names:
+        assert rel_l2(gf[n], o.var(n)) < FIELD_TOL, n
+
+
+def test_device_error_flags():
+    """Fault injection on the host side of the boundary: an out-of-table
+    temperature and a secant cap of one iteration set the error word; the
+    context stays usable."""
+    from pycles_b200 import _capi
+    nl, rs, f = _setup(MOIST_SMALL, stir=False)
+    f = dict(f)
+    f["qt"] = f["qt"] + 6e-3
+    g = gpu_sim(nl, rs, f)
+    g.PV.Update_all_bcs(g.Gr)
+    _capi.clear_error()
+    g.Th.max_secant_iter = 1
+    g.Th.update(g.Gr, g.RS, g.PV, g.DV)
+    assert _capi.get_error() & _capi.ERR_SECANT_CAP
+    _capi.clear_error()
+    g.Th.max_secant_iter = 100
+    g.PV.field("s", g.Gr).add_(5000.0)  # far outside the pv* table
+    g.Th.update(g.Gr, g.RS, g.PV, g.DV)
+    assert _capi.get_error() & _capi.ERR_TABLE_RANGE
+    _capi.clear_error()
+    assert _capi.get_error() == 0
