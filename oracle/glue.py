@@ -93,7 +93,7 @@ def reference_state(d: Dims, Pg, Tg, qtg, moist=True, backend="ref", table_xy=No
     sg = entropy(Pg, Tg, qtg, 0.0, 0.0)
 
     def rhs(p, z):
-        T, ql, qi = eos(np.exp(p), sg, qtg)
+        T, ql, qi = eos(float(np.exp(p[0])), sg, qtg)
         return -port.g / (port.Rd * T * (1.0 - qtg + port.eps_vi * (qtg - ql - qi)))
 
     z = np.array(d.z[g_ - 1:-g_ + 1])

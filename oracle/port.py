@@ -560,12 +560,15 @@ def horizontal_mean(d: Dims, values):
 
 def modified_wave_numbers(d: Dims):
     """PressureFFTParallel.compute_modified_wave_numbers (:64-98)."""
+    import math
     out = []
     for dim in (0, 1):
         n = d.n[dim]
-        ii = np.arange(n)
-        xi = np.where(ii <= n / 2, ii, ii - n).astype(np.float64)
-        k2 = (2.0 * np.cos((2.0 * pi / n) * xi) - 2.0) / d.dx[dim] / d.dx[dim]
+        k2 = np.empty(n)
+        for i in range(n):
+            xi = float(i) if i <= n / 2 else float(i - n)
+            # libm cos, as the reference's `from libc.math cimport cos`
+            k2[i] = (2.0 * math.cos((2.0 * pi / n) * xi) - 2.0) / d.dx[dim] / d.dx[dim]
         k2[0] = 0.0
         out.append(k2)
     return out

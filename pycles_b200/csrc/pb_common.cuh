@@ -41,6 +41,15 @@ __device__ unsigned int pb_device_error = 0u;
 
 __device__ __forceinline__ void pb_flag(unsigned int bit) { atomicOr(&pb_device_error, bit); }
 
+// Separately rounded IEEE operations.  The compiler contracts a*b+c into an
+// FMA; where a result is formed by cancellation (the divergence of a nearly
+// solenoidal field, alpha - alpha0, near-singular tridiagonal rows) that one
+// rounding difference shows up at 1e-12 relative, so these spots use the
+// reference's separately rounded sequence.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
 struct Geo {
   long long n0, n1, n2;     // nlg
   long long is, js;         // strides in elements

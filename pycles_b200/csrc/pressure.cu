@@ -226,9 +226,9 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
     // second_order_divergence (PressureSolver.pyx:138-175), d = 0, 1, 2
     const double ah = a.alpha0_half[k];
     double d = 0.0;
-    d += (a.u[ijk] / ah - a.u[ijk - g.is] / ah) * dxi0;
-    d += (a.v[ijk] / ah - a.v[ijk - g.js] / ah) * dxi1;
-    d += ((a.w[ijk]) / a.alpha0[k] - (a.w[ijk - 1]) / a.alpha0[k - 1]) * dxi2;
+    d = add_rn(d, mul_rn(sub_rn(a.u[ijk] / ah, a.u[ijk - g.is] / ah), dxi0));
+    d = add_rn(d, mul_rn(sub_rn(a.v[ijk] / ah, a.v[ijk - g.js] / ah), dxi1));
+    d = add_rn(d, mul_rn(sub_rn((a.w[ijk]) / a.alpha0[k], (a.w[ijk - 1]) / a.alpha0[k - 1]), dxi2));
     a.div[ijk] = d;
     in[kl * N + slot(il, N, a.log0)] = make_double2(d, 0.0);
   }
@@ -314,10 +314,10 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
   // row 0 (for a single level the last-row formulas overwrite it, :119-127, :145-146)
   double b, c;
   if (nz > 1) {
-    b = (rho0h[gw] * kk - (rho0[gw]) * dzi * dzi);
-    c = dzi * dzi * rho0[gw];
+    b = sub_rn(mul_rn(rho0h[gw], kk), mul_rn(mul_rn(rho0[gw], dzi), dzi));
+    c = mul_rn(mul_rn(dzi, dzi), rho0[gw]);
   } else {
-    b = (rho0h[gw] * kk - (rho0[gw - 1]) * dzi * dzi);
+    b = sub_rn(mul_rn(rho0h[gw], kk), mul_rn(mul_rn(rho0[gw - 1], dzi), dzi));
     c = 0.0;
   }
   double s_prev = c / b;
@@ -327,29 +327,29 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
   x[0] = xp;
   scr[0] = s_prev;
   for (int k = 1; k < nz; ++k) {
-    const double ak = dzi * dzi * rho0[k + gw - 1];
+    const double ak = mul_rn(mul_rn(dzi, dzi), rho0[k + gw - 1]);
     double ck, bk;
     if (k < nz - 1) {
-      ck = dzi * dzi * rho0[k + gw];
-      bk = (rho0h[k + gw] * kk - (rho0[k + gw] + rho0[k + gw - 1]) * dzi * dzi);
+      ck = mul_rn(mul_rn(dzi, dzi), rho0[k + gw]);
+      bk = sub_rn(mul_rn(rho0h[k + gw], kk), mul_rn(mul_rn(add_rn(rho0[k + gw], rho0[k + gw - 1]), dzi), dzi));
     } else {
       ck = 0.0;
-      bk = (rho0h[k + gw] * kk - (rho0[k + gw - 1]) * dzi * dzi);
+      bk = sub_rn(mul_rn(rho0h[k + gw], kk), mul_rn(mul_rn(rho0[k + gw - 1], dzi), dzi));
     }
-    const double m = 1.0 / (bk - ak * s_prev);
-    s_prev = ck * m;
+    const double m = 1.0 / sub_rn(bk, mul_rn(ak, s_prev));
+    s_prev = mul_rn(ck, m);
     scr[(long long)k * ncol] = s_prev;
     double2 xk = x[(long long)k * ncol];
-    xk.x = (xk.x - ak * xp.x) * m;
-    xk.y = (xk.y - ak * xp.y) * m;
+    xk.x = mul_rn(sub_rn(xk.x, mul_rn(ak, xp.x)), m);
+    xk.y = mul_rn(sub_rn(xk.y, mul_rn(ak, xp.y)), m);
     x[(long long)k * ncol] = xk;
     xp = xk;
   }
   for (int k = nz - 2; k >= 0; --k) {
     const double sk = scr[(long long)k * ncol];
     double2 xk = x[(long long)k * ncol];
-    xk.x = xk.x - sk * xp.x;
-    xk.y = xk.y - sk * xp.y;
+    xk.x = sub_rn(xk.x, mul_rn(sk, xp.x));
+    xk.y = sub_rn(xk.y, mul_rn(sk, xp.y));
     x[(long long)k * ncol] = xk;
     xp = xk;
   }
@@ -418,9 +418,9 @@ __global__ void correction(Geo g, const double* __restrict__ p, double* __restri
     const long long i = r / g.n1;
     if (i >= g.n0 - 1 || j >= g.n1 - 1 || k >= g.n2 - 1) continue;
     const double pc = p[t];
-    u[t] -= (p[t + g.is] - pc) * g.dxi0;
-    v[t] -= (p[t + g.js] - pc) * g.dxi1;
-    w[t] -= (p[t + 1] - pc) * g.dxi2;
+    u[t] = sub_rn(u[t], mul_rn(sub_rn(p[t + g.is], pc), g.dxi0));
+    v[t] = sub_rn(v[t], mul_rn(sub_rn(p[t + g.js], pc), g.dxi1));
+    w[t] = sub_rn(w[t], mul_rn(sub_rn(p[t + 1], pc), g.dxi2));
   }
 }
 

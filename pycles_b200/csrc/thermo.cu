@@ -19,11 +19,13 @@ __device__ __forceinline__ double pv_c(double p0, double qt, double qv) {
 __device__ __forceinline__ double qv_star_c(double p0, double qt, double pv) {
   return eps_v * (1.0 - qt) * pv / (p0 - pv);
 }
+// alpha and buoyancy: buoyancy cancels ~3 digits of alpha, so both keep the
+// reference's separately rounded operations.
 __device__ __forceinline__ double alpha_c(double p0, double T, double qt, double qv) {
-  return (Rd * T) / p0 * (1.0 - qt + eps_vi * qv);
+  return mul_rn((Rd * T) / p0, add_rn(sub_rn(1.0, qt), mul_rn(eps_vi, qv)));
 }
 __device__ __forceinline__ double buoyancy_c(double alpha0, double alpha) {
-  return g * (alpha - alpha0) / alpha0;
+  return mul_rn(g, sub_rn(alpha, alpha0)) / alpha0;
 }
 __device__ __forceinline__ double cpm_c(double qt) { return (1.0 - qt) * cpd + qt * cpv; }
 __device__ __forceinline__ double sd_c(double pd, double T) {
@@ -279,7 +281,7 @@ __global__ void thermo_dry_kernel(Geo geo, DryArgs a, long long ncols) {
     // eos_c (Csrc/thermodynamics_dry.h:8-10), eos_update (:12-37)
     T = T_tilde * (exp((a.s[idx] - sd_tilde + Rd * log(pd / p_tilde)) / cpd));
     a.T[idx] = T;
-    const double al = (Rd * T) / pd * (1.0 - 0.0 + eps_vi * 0.0);
+    const double al = mul_rn((Rd * T) / pd, 1.0);
     a.alpha[idx] = al;
     // buoyancy_update (:39-73): i < n0-1, j < n1-1, k < n2-1
     const bool bij = (i < geo.n0 - 1) && (j < geo.n1 - 1);

@@ -1,0 +1,103 @@
+"""Generate the golden fixtures of the hot path from the reference's own C.
+
+    python tests/golden/make_golden.py
+
+Needs oracle/_ref (the reference's C kernels and its Cython TDMA compiled
+from the reference tree by oracle/build_ref.py).  For each case it stores
+the seeded input state and reference-state profiles, and the outputs of the
+reference kernels driven by the restated glue (oracle.glue, backend "ref"):
+thermodynamics, scalar advection, momentum advection, pressure, one full
+time step, and Simulation3d.run's prologue + one step.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+CASES = {
+    "moist_w5": dict(case="bomex", nx=12, ny=10, nz=16, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0),
+    "moist_w7": dict(case="bomex", nx=8, ny=12, nz=14, dx=100.0, dy=100.0, dz=40.0, gw=4, dt=1.0,
+                     scalar_order=7, momentum_order=7),
+    "dry_w5": dict(case="dry_cbl", nx=8, ny=8, nz=12, dx=50.0, dy=50.0, dz=50.0, gw=3, dt=0.5),
+}
+
+
+def stir(fields, seed=1, amp=0.5):
+    rng = np.random.default_rng(seed)
+    out = dict(fields)
+    for n in ("u", "v", "w"):
+        out[n] = fields[n] + amp * rng.standard_normal(fields[n].shape)
+    if "qt" in out:
+        out["qt"] = fields["qt"] + 6e-3  # part of the column saturated
+    return out
+
+
+def make(name, cfg):
+    from helpers import host_case, oracle_sim
+    from oracle import ref
+    assert ref.available(), "oracle/_ref missing: run oracle/build_ref.py"
+    nl, rs, f0 = host_case(**cfg)
+    f = stir(f0)
+    out = {"rs_" + k: v for k, v in rs.items()}
+    for k, v in f.items():
+        out["in_" + k] = v
+    # whole-step outputs start from the unstirred state (white-noise
+    # velocities are not a state a time step should be asked to take)
+    for k, v in f0.items():
+        out["in0_" + k] = v
+
+    def sim(fields=f):
+        s = oracle_sim(nl, rs, fields, backend="ref")
+        s.update_all_bcs()
+        return s
+
+    s = sim()
+    for k in s.names:
+        out["bcs_" + k] = s.var(k).copy()
+    s.th_update()
+    for k, v in s.dv.items():
+        out["th_" + k] = v.copy()
+    out["th_wtend"] = s.tend("w").copy()
+    s = sim()
+    s.sa_update()
+    for k in s.names[3:]:
+        out["sa_" + k] = s.tend(k).copy()
+    s = sim()
+    s.ma_update()
+    for k in ("u", "v", "w"):
+        out["ma_" + k] = s.tend(k).copy()
+    s = sim()
+    s.pr_update()
+    for k in ("u", "v", "w"):
+        out["pr_" + k] = s.var(k).copy()
+    out["pr_p"] = s.dv["dynamic_pressure"].copy()
+    out["pr_div"] = s.dv["divergence"].copy()
+    s = sim(f0)
+    s.step()
+    for k in s.names:
+        out["step_" + k] = s.var(k).copy()
+    s = oracle_sim(nl, rs, f0, backend="ref")
+    s.update_all_bcs()
+    s.th_update()
+    s.step()
+    for k in s.names:
+        out["run1_" + k] = s.var(k).copy()
+    meta = np.array([repr(cfg)])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=meta, **out)
+
+
+def main():
+    for name, cfg in CASES.items():
+        make(name, cfg)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,185 @@
+"""Pins the oracle: the numpy restatement (oracle/port.py) against the
+reference's own C kernels compiled from the reference tree (oracle/_ref),
+the reference TDMA's known-answer test, and the committed golden fixtures
+(tests/golden/*.npz, generated from the reference C by make_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, host_case, oracle_sim, rel_l2
+
+from oracle import port, ref
+
+needs_ref = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built (needs the reference tree)")
+
+SMALL = dict(case="bomex", nx=10, ny=8, nz=14, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
+
+
+def _stirred(cfg, qt_boost=6e-3):
+    nl, rs, f = host_case(**cfg)
+    rng = np.random.default_rng(7)
+    f = dict(f)
+    for n in ("u", "v", "w"):
+        f[n] = f[n] + 0.5 * rng.standard_normal(f[n].shape)
+    if "qt" in f:
+        f["qt"] = f["qt"] + qt_boost
+    return nl, rs, f
+
+
+def test_tdma_known_answer():
+    """SparseSolvers.pyx:49-60: a=[0,-1,-1,-1], b=4, c=[-1,-1,-1,0], d=[5,5,10,23] -> [2,3,5,7]."""
+    a = np.array([0, -1, -1, -1], dtype=float)
+    b = np.array([[4, 4, 4, 4]], dtype=float)
+    c = np.array([-1, -1, -1, 0], dtype=float)
+    d = np.array([[5, 5, 10, 23]], dtype=float)
+    port.tdma(d, a, b, c)
+    assert np.allclose(d[0], [2, 3, 5, 7], rtol=0, atol=1e-14)
+
+
+@needs_ref
+def test_tdma_port_matches_reference_cython():
+    mod = ref.tdma_module()
+    if mod is None:
+        pytest.skip("reference SparseSolvers not cythonized")
+    rng = np.random.default_rng(0)
+    n = 37
+    a = rng.standard_normal(n)
+    c = rng.standard_normal(n)
+    b = 6.0 + rng.standard_normal(n)
+    x = rng.standard_normal(n)
+    x_ref = x.copy()
+    mod.tdma_solve(x_ref, a.copy(), b.copy(), c.copy())
+    x_port = x.copy()[None, :]
+    port.tdma(x_port, a, b[None, :], c)
+    assert np.array_equal(x_port[0], x_ref)
+
+
+@needs_ref
+@pytest.mark.parametrize("order", [5, 7])
+def test_advection_port_vs_reference(order):
+    cfg = dict(SMALL, gw=4) if order == 7 else SMALL
+    cfg = dict(cfg, scalar_order=order, momentum_order=order)
+    nl, rs, f = _stirred(cfg)
+    a, b = oracle_sim(nl, rs, f, "ref"), oracle_sim(nl, rs, f, "port")
+    a.update_all_bcs()
+    b.update_all_bcs()
+    a.sa_update()
+    b.sa_update()
+    a.ma_update()
+    b.ma_update()
+    for n in a.names:
+        assert rel_l2(b.tend(n), a.tend(n)) < 1e-14, n
+
+
+@needs_ref
+def test_thermo_port_vs_reference():
+    nl, rs, f = _stirred(SMALL)
+    a, b = oracle_sim(nl, rs, f, "ref"), oracle_sim(nl, rs, f, "port")
+    a.update_all_bcs()
+    b.update_all_bcs()
+    a.th_update()
+    b.th_update()
+    assert (a.dv["ql"] > 0).any()
+    # numpy's log/exp and glibc's differ by an ulp now and then; the vertical
+    # derivative in the buoyancy frequency amplifies that to ~1e-14
+    for k in a.dv:
+        assert rel_l2(b.dv[k], a.dv[k]) < 1e-12, k
+    assert rel_l2(b.tend("w"), a.tend("w")) < 1e-13
+
+
+@needs_ref
+def test_dry_thermo_port_vs_reference():
+    nl, rs, f = host_case("dry_cbl", 8, 8, 12, 50.0, 50.0, 50.0)
+    a, b = oracle_sim(nl, rs, f, "ref"), oracle_sim(nl, rs, f, "port")
+    a.update_all_bcs()
+    b.update_all_bcs()
+    a.th_update()
+    b.th_update()
+    # buoyancy = g (alpha - alpha0)/alpha0 cancels three digits of alpha
+    for k in a.dv:
+        assert rel_l2(b.dv[k], a.dv[k]) < 1e-11, k
+    assert rel_l2(b.tend("w"), a.tend("w")) < 1e-11
+
+
+@needs_ref
+def test_halo_port_vs_reference_exact():
+    nl, rs, f = _stirred(dict(SMALL, gw=4))
+    a, b = oracle_sim(nl, rs, f, "ref"), oracle_sim(nl, rs, f, "port")
+    a.update_all_bcs()
+    b.update_all_bcs()
+    assert np.array_equal(a.values, b.values)
+
+
+@needs_ref
+def test_reference_state_port_vs_reference():
+    from oracle import glue
+    from helpers import oracle_dims
+    nl, _, _ = host_case(**SMALL)
+    d = oracle_dims(nl)
+    r1 = glue.reference_state(d, 1.015e5, 300.4, 0.02245, moist=True, backend="ref")
+    r2 = glue.reference_state(d, 1.015e5, 300.4, 0.02245, moist=True, backend="port")
+    for k in r1:
+        assert rel_l2(r2[k], r1[k]) < 1e-14, k
+
+
+def test_package_reference_state_matches_oracle():
+    """The package's host-side reference-state integration (init only) agrees
+    with the oracle's restatement of ReferenceState.initialize."""
+    from oracle import glue
+    from helpers import oracle_dims
+    nl, rs, _ = host_case(**SMALL)
+    d = oracle_dims(nl)
+    r = glue.reference_state(d, 1.015e5, 300.4, 0.02245, moist=True, backend="port")
+    for k in r:
+        assert rel_l2(rs[k], r[k]) < 1e-13, k
+
+
+@pytest.mark.parametrize("name", ["moist_w5", "moist_w7", "dry_w5"])
+def test_golden_fixtures_port(name):
+    """The numpy restatement reproduces the reference-generated goldens."""
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    cfg = eval(str(z["meta"][0]))  # the dict literal make_golden.py wrote
+    from pycles_b200.simulation import namelist_for
+    nl = namelist_for(**cfg)
+    rs = {k[3:]: z[k] for k in z.files if k.startswith("rs_")}
+    f = {k[3:]: z[k] for k in z.files if k.startswith("in_")}
+    f0 = {k[4:]: z[k] for k in z.files if k.startswith("in0_")}
+
+    def sim(fields=f):
+        s = oracle_sim(nl, rs, fields, "port")
+        s.update_all_bcs()
+        return s
+
+    s = sim()
+    for k in s.names:
+        assert np.array_equal(s.var(k), z["bcs_" + k]), k
+    s.th_update()
+    for k in s.dv:
+        assert rel_l2(s.dv[k], z["th_" + k]) < 1e-11, k
+    s = sim()
+    s.sa_update()
+    for k in s.names[3:]:
+        assert rel_l2(s.tend(k), z["sa_" + k]) < 1e-14, k
+    s = sim()
+    s.ma_update()
+    for k in ("u", "v", "w"):
+        assert rel_l2(s.tend(k), z["ma_" + k]) < 1e-14, k
+    s = sim()
+    s.pr_update()
+    assert rel_l2(s.dv["dynamic_pressure"], z["pr_p"]) < 1e-13
+    for k in ("u", "v", "w"):
+        assert rel_l2(s.var(k), z["pr_" + k]) < 1e-14, k
+    # v and w start at zero here, so after a step they are formed entirely
+    # from buoyancy and the pressure correction: an ulp of difference between
+    # numpy's and glibc's exp/log in the temperature reaches them at ~2e-13.
+    s = sim(f0)
+    s.step()
+    for k in s.names:
+        assert rel_l2(s.var(k), z["step_" + k]) < 1e-12, k
+    s = oracle_sim(nl, rs, f0, "port")
+    s.update_all_bcs()
+    s.th_update()
+    s.step()
+    for k in s.names:
+        assert rel_l2(s.var(k), z["run1_" + k]) < 1e-12, k
