@@ -47,20 +47,41 @@ def nvcc() -> str:
     return "nvcc"
 
 
+# Translation units and their extra flags.  The thermodynamics are compiled
+# without FMA contraction so that the temperature follows the reference's
+# separately rounded arithmetic (see csrc/crmath.cuh).
+UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"])]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, cwd=CSRC, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + r.stdout.decode()[-4000:])
+    return r.stdout.decode()
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    objs = []
+    log = []
+    for src, extra in UNITS:
+        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
+        cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
+        cmd.remove("-shared")
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        log.append(_run(cmd))
+        objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + NVCC_FLAGS + [os.path.join(CSRC, "pb_all.cu"), "-o", tmp]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, cwd=CSRC, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
-    if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout.decode()[-4000:])
+    _run([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC"] + objs
+         + ["-o", tmp])
     os.replace(tmp, LIB)
+    for o in objs:
+        os.remove(o)
     if verbose:
-        print(r.stdout.decode())
+        print("\n".join(log))
     return LIB
 
 

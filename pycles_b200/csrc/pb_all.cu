@@ -1,7 +1,6 @@
-// Single translation unit for libpycles_b200.so: the device error word and
-// the shared helpers are visible to every kernel without relocatable
-// device code.
+// Translation unit 1 of libpycles_b200.so: time stepping, ghost fills,
+// advection, pressure.  The thermodynamics are translation unit 2
+// (thermo.cu), compiled without FMA contraction.
 #include "timestep.cu"
 #include "advection.cu"
-#include "thermo.cu"
 #include "pressure.cu"

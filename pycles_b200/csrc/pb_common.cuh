@@ -36,10 +36,11 @@ constexpr double sv_tilde = 10513.6;
 #define PB_ERR_SECANT_CAP 0x2u    // saturation-adjustment secant hit its cap
 #define PB_ERR_NONFINITE 0x4u     // non-finite temperature produced
 
-// Defined here: the library is built as one translation unit (pb_all.cu).
-__device__ unsigned int pb_device_error = 0u;
+// Device address of this device's error word (defined in timestep.cu); the
+// library has two translation units, so kernels receive it as an argument.
+unsigned int* pb_error_word_ptr();
 
-__device__ __forceinline__ void pb_flag(unsigned int bit) { atomicOr(&pb_device_error, bit); }
+__device__ __forceinline__ void pb_flag_at(unsigned int* word, unsigned int bit) { atomicOr(word, bit); }
 
 // Separately rounded IEEE operations.  The compiler contracts a*b+c into an
 // FMA; where a result is formed by cancellation (the divergence of a nearly

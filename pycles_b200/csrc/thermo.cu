@@ -1,9 +1,14 @@
-// Saturation-adjustment and dry thermodynamics.
+// Saturation-adjustment and dry thermodynamics (translation unit 2).
 //
 // One thread block owns whole (i,j) columns, one thread per level k, so the
 // vertical neighbours that buoyancy_update_sa / bvf_sa need come from shared
 // memory and every cell's state is computed exactly once.
+//
+// Compiled with -fmad=false and with correctly rounded exp/log (crmath.cuh):
+// the temperature then follows the reference's separately rounded C
+// arithmetic bit for bit (see crmath.cuh for why that matters here).
 #include "pb_common.cuh"
+#include "crmath.cuh"
 
 namespace thermo_k {
 
@@ -29,10 +34,10 @@ __device__ __forceinline__ double buoyancy_c(double alpha0, double alpha) {
 }
 __device__ __forceinline__ double cpm_c(double qt) { return (1.0 - qt) * cpd + qt * cpv; }
 __device__ __forceinline__ double sd_c(double pd, double T) {
-  return sd_tilde + cpd * log(T / T_tilde) - Rd * log(pd / p_tilde);
+  return sd_tilde + cpd * crm::log(T / T_tilde) - Rd * crm::log(pd / p_tilde);
 }
 __device__ __forceinline__ double sv_c(double pv, double T) {
-  return sv_tilde + cpv * log(T / T_tilde) - Rv * log(pv / p_tilde);
+  return sv_tilde + cpv * crm::log(T / T_tilde) - Rv * crm::log(pv / p_tilde);
 }
 __device__ __forceinline__ double sc_c(double L, double T) { return -L / T; }
 __device__ __forceinline__ double interp_2(double a, double b) { return 0.5 * (a + b); }
@@ -45,11 +50,11 @@ __device__ __forceinline__ double latent_heat(double T) {
 
 // lookup (Csrc/lookup.h:48-54) with a range check the reference lacks:
 // out-of-table arguments flag PB_ERR_TABLE_RANGE and are clamped.
-__device__ __forceinline__ double table_lookup(const pb_table& t, double x) {
+__device__ __forceinline__ double table_lookup(const pb_table& t, double x, unsigned int* err) {
   const double fi = floor((x - t.x_min) * t.dxi);
   long long indx;
   if (!(fi >= 0.0 && fi <= (double)(t.n - 2))) {
-    pb_flag(PB_ERR_TABLE_RANGE);
+    pb_flag_at(err, PB_ERR_TABLE_RANGE);
     indx = (fi >= 0.0) ? t.n - 2 : 0;
   } else {
     indx = (long long)fi;
@@ -62,9 +67,9 @@ __device__ __forceinline__ double table_lookup(const pb_table& t, double x) {
 
 // temperature_no_ql (Csrc/thermodynamics_sa.h:10-15)
 __device__ __forceinline__ double temperature_no_ql(double pd, double pv, double s, double qt) {
-  return T_tilde * exp((s - (1.0 - qt) * (sd_tilde - Rd * log(pd / p_tilde)) -
-                        qt * (sv_tilde - Rv * log(pv / p_tilde))) /
-                       ((1.0 - qt) * cpd + qt * cpv));
+  return T_tilde * crm::exp((s - (1.0 - qt) * (sd_tilde - Rd * crm::log(pd / p_tilde)) -
+                             qt * (sv_tilde - Rv * crm::log(pv / p_tilde))) /
+                            ((1.0 - qt) * cpd + qt * cpv));
 }
 
 struct EosOut {
@@ -79,7 +84,7 @@ struct EosOut {
 // secant point T_2 (:39) by a learned guess; the loop and its stopping test
 // stay the reference's.
 __device__ __forceinline__ EosOut eos_sa(const pb_table& LT, double p0, double s, double qt, int max_iter,
-                                         bool use_seed, double seed) {
+                                         bool use_seed, double seed, unsigned int* err) {
   EosOut o;
   o.qv = qt;
   o.ql = 0.0;
@@ -88,7 +93,7 @@ __device__ __forceinline__ EosOut eos_sa(const pb_table& LT, double p0, double s
   const double pv_1 = pv_c(p0, qt, qt);
   const double pd_1 = p0 - pv_1;
   double T_1 = temperature_no_ql(pd_1, pv_1, s, qt);
-  const double pv_star_1 = table_lookup(LT, T_1);
+  const double pv_star_1 = table_lookup(LT, T_1, err);
   const double qv_star_1 = qv_star_c(p0, qt, pv_star_1);
   if (qt <= qv_star_1) {
     o.T = T_1;
@@ -106,7 +111,7 @@ __device__ __forceinline__ EosOut eos_sa(const pb_table& LT, double p0, double s
   double qv_star_2, sigma_2;
   int it = 0;
   do {
-    const double pv_star_2 = table_lookup(LT, T_2);
+    const double pv_star_2 = table_lookup(LT, T_2, err);
     qv_star_2 = qv_star_c(p0, qt, pv_star_2);
     const double pv_2 = pv_c(p0, qt, qv_star_2);
     const double pd_2 = p0 - pv_2;
@@ -121,7 +126,7 @@ __device__ __forceinline__ EosOut eos_sa(const pb_table& LT, double p0, double s
     delta_T = fabs(T_2 - T_1);
     ++it;
     if (it >= max_iter) {
-      if (delta_T >= 1.0e-3 || sigma_2 < 0.0) pb_flag(PB_ERR_SECANT_CAP);
+      if (delta_T >= 1.0e-3 || sigma_2 < 0.0) pb_flag_at(err, PB_ERR_SECANT_CAP);
       break;
     }
   } while (delta_T >= 1.0e-3 || sigma_2 < 0.0);
@@ -151,6 +156,7 @@ struct SaArgs {
   double* wt;
   const double* seed;        // learned T_2 per cell (nullable)
   unsigned long long* stats; // {iterations, saturated cells} (nullable)
+  unsigned int* err;         // device error word
   int clip;
   int max_iter;
 };
@@ -179,10 +185,10 @@ __global__ void thermo_sa_kernel(Geo geo, SaArgs a, long long ncols) {
       a.qt[idx] = qt;
     }
     const double s = a.s[idx];
-    const EosOut e = eos_sa(a.LT, p0, s, qt, a.max_iter, a.seed != nullptr, a.seed ? a.seed[idx] : 0.0);
+    const EosOut e = eos_sa(a.LT, p0, s, qt, a.max_iter, a.seed != nullptr, a.seed ? a.seed[idx] : 0.0, a.err);
     T = e.T;
     qv = e.qv;
-    if (!isfinite(T)) pb_flag(PB_ERR_NONFINITE);
+    if (!isfinite(T)) pb_flag_at(a.err, PB_ERR_NONFINITE);
     my_it = (unsigned long long)e.iters;
     my_sat = e.sat ? 1ull : 0ull;
     a.T[idx] = T;
@@ -195,7 +201,7 @@ __global__ void thermo_sa_kernel(Geo geo, SaArgs a, long long ncols) {
     const double exner = pow(p0 / p_tilde, kappa);
     const double Lv = latent_heat(T);
     const double theta = T / exner;
-    a.thetali[idx] = theta * exp(-Lv * (e.ql / (1.0 - qt) + e.qi / (1.0 - qt)) / (T * cpd));
+    a.thetali[idx] = theta * crm::exp(-Lv * (e.ql / (1.0 - qt) + e.qi / (1.0 - qt)) / (T * cpd));
     // bvf_sa first loop (:147-157): theta_rho on k in [1, n2-1)
     double thr = 0.0;
     if (k >= 1 && k < n2 - 1) {
@@ -223,7 +229,7 @@ __global__ void thermo_sa_kernel(Geo geo, SaArgs a, long long ncols) {
       double bv;
       if (qv < qt) {
         const double Lv = latent_heat(T);
-        const double pv_star = table_lookup(a.LT, T);
+        const double pv_star = table_lookup(a.LT, T, a.err);
         const double rsl = eps_v * pv_star / (p0 - pv_star);
         const double gamma_w = g / cpd * (1.0 / (1.0 - qt)) * (1.0 + Lv * rsl / (Rd * T)) /
                                (cpm_c(qt) / cpd + Lv * Lv * (eps_v + rsl) * rsl / (cpd * Rd * T * T));
@@ -279,7 +285,7 @@ __global__ void thermo_dry_kernel(Geo geo, DryArgs a, long long ncols) {
     idx = col * n2 + k;
     const double pd = a.pd[k];
     // eos_c (Csrc/thermodynamics_dry.h:8-10), eos_update (:12-37)
-    T = T_tilde * (exp((a.s[idx] - sd_tilde + Rd * log(pd / p_tilde)) / cpd));
+    T = T_tilde * (crm::exp((a.s[idx] - sd_tilde + Rd * crm::log(pd / p_tilde)) / cpd));
     a.T[idx] = T;
     const double al = mul_rn((Rd * T) / pd, 1.0);
     a.alpha[idx] = al;
@@ -355,6 +361,8 @@ extern "C" int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const do
   a.wt = w_tend;
   a.seed = nullptr;
   a.stats = reinterpret_cast<unsigned long long*>(secant_iters);
+  a.err = pb_error_word_ptr();
+  if (!a.err) return PB_ERR_CUDA;
   a.clip = clip_qt;
   a.max_iter = max_iter;
   dim3 blk;

@@ -1,7 +1,25 @@
 // SSP-RK3 stage update and ghost-cell fills.
 #include <string.h>
 
+#include <mutex>
+
 #include "pb_common.cuh"
+
+__device__ unsigned int pb_device_error = 0u;
+
+unsigned int* pb_error_word_ptr() {
+  static std::mutex mu;
+  static void* addr[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[dev] == nullptr) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, pb_device_error) != cudaSuccess) return nullptr;
+    addr[dev] = p;
+  }
+  return static_cast<unsigned int*>(addr[dev]);
+}
 
 namespace {
 
@@ -18,19 +36,18 @@ __global__ void __launch_bounds__(256) rk3_kernel(double* __restrict__ v, double
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) {
     double2 vv = v2[i];
     const double2 tt = t2[i];
+    // separately rounded, as the reference's C loop (the kernel is
+    // bandwidth bound, so this costs nothing)
     if (STAGE == 0) {
       c2[i] = vv;
-      vv.x += tt.x * dt;
-      vv.y += tt.y * dt;
+      vv.x = add_rn(vv.x, mul_rn(tt.x, dt));
+      vv.y = add_rn(vv.y, mul_rn(tt.y, dt));
     } else {
       const double2 cc = c2[i];
-      if (STAGE == 1) {
-        vv.x = 0.75 * cc.x + 0.25 * (vv.x + tt.x * dt);
-        vv.y = 0.75 * cc.y + 0.25 * (vv.y + tt.y * dt);
-      } else {
-        vv.x = (1.0 / 3.0) * cc.x + (2.0 / 3.0) * (vv.x + tt.x * dt);
-        vv.y = (1.0 / 3.0) * cc.y + (2.0 / 3.0) * (vv.y + tt.y * dt);
-      }
+      const double a = (STAGE == 1) ? 0.75 : (1.0 / 3.0);
+      const double b = (STAGE == 1) ? 0.25 : (2.0 / 3.0);
+      vv.x = add_rn(mul_rn(a, cc.x), mul_rn(b, add_rn(vv.x, mul_rn(tt.x, dt))));
+      vv.y = add_rn(mul_rn(a, cc.y), mul_rn(b, add_rn(vv.y, mul_rn(tt.y, dt))));
     }
     v2[i] = vv;
     t2[i] = make_double2(0.0, 0.0);
@@ -39,11 +56,11 @@ __global__ void __launch_bounds__(256) rk3_kernel(double* __restrict__ v, double
     const long long i = n - 1;
     if (STAGE == 0) {
       c[i] = v[i];
-      v[i] += t[i] * dt;
+      v[i] = add_rn(v[i], mul_rn(t[i], dt));
     } else if (STAGE == 1) {
-      v[i] = 0.75 * c[i] + 0.25 * (v[i] + t[i] * dt);
+      v[i] = add_rn(mul_rn(0.75, c[i]), mul_rn(0.25, add_rn(v[i], mul_rn(t[i], dt))));
     } else {
-      v[i] = (1.0 / 3.0) * c[i] + (2.0 / 3.0) * (v[i] + t[i] * dt);
+      v[i] = add_rn(mul_rn(1.0 / 3.0, c[i]), mul_rn(2.0 / 3.0, add_rn(v[i], mul_rn(t[i], dt))));
     }
     t[i] = 0.0;
   }

@@ -91,6 +91,62 @@ __device__ __forceinline__ R weno7(R phim3, R phim2, R phim1, R phi, R phip1, R 
   return w0 * p0 + w1 * p1 + w2 * p2 + w3 * p3;
 }
 
+// The same WENO5/WENO7 interpolants with a single division.  The normalised
+// weights w_k = (d_k/q_k) / sum_j (d_j/q_j), q_k = (beta_k + eps)^2, equal
+// n_k / sum_j n_j with n_k = d_k * prod_{j != k} q_j, so one reciprocal of
+// the sum replaces the reference's 4 (WENO5) or 5 (WENO7) divisions.  In
+// FP64 the products stay far from the range limits (q >= 1e-20, and q <= 1e10
+// for any physical jump), and the result differs from the reference's
+// formula by rounding only.  Used by the FP64 form: FP64 division is a
+// multi-instruction sequence, and the advection is FP64-pipe bound.
+__device__ __forceinline__ double weno5_1div(double phim2, double phim1, double phi, double phip1, double phip2) {
+  const double p0 = (1.0 / 3.0) * phim2 - (7.0 / 6.0) * phim1 + (11.0 / 6.0) * phi;
+  const double p1 = (-1.0 / 6.0) * phim1 + (5.0 / 6.0) * phi + (1.0 / 3.0) * phip1;
+  const double p2 = (1.0 / 3.0) * phi + (5.0 / 6.0) * phip1 - (1.0 / 6.0) * phip2;
+  const double a2 = phi - 2.0 * phip1 + phip2;
+  const double b2 = 3.0 * phi - 4.0 * phip1 + phip2;
+  const double a1 = phim1 - 2.0 * phi + phip1;
+  const double b1 = phim1 - phip1;
+  const double a0 = phim2 - 2.0 * phim1 + phi;
+  const double b0 = phim2 - 4.0 * phim1 + 3.0 * phi;
+  const double e0 = (13.0 / 12.0) * a0 * a0 + 0.25 * b0 * b0 + 1e-10;
+  const double e1 = (13.0 / 12.0) * a1 * a1 + 0.25 * b1 * b1 + 1e-10;
+  const double e2 = (13.0 / 12.0) * a2 * a2 + 0.25 * b2 * b2 + 1e-10;
+  const double q0 = e0 * e0, q1 = e1 * e1, q2 = e2 * e2;
+  const double n0 = 0.1 * (q1 * q2);
+  const double n1 = 0.6 * (q0 * q2);
+  const double n2 = 0.3 * (q0 * q1);
+  return (n0 * p0 + n1 * p1 + n2 * p2) / (n0 + n1 + n2);
+}
+
+__device__ __forceinline__ double weno7_1div(double phim3, double phim2, double phim1, double phi, double phip1,
+                                             double phip2, double phip3) {
+  const double p0 = (-1.0 / 4.0) * phim3 + (13.0 / 12.0) * phim2 + (-23.0 / 12.0) * phim1 + (25.0 / 12.0) * phi;
+  const double p1 = (1.0 / 12.0) * phim2 + (-5.0 / 12.0) * phim1 + (13.0 / 12.0) * phi + (1.0 / 4.0) * phip1;
+  const double p2 = (-1.0 / 12.0) * phim1 + (7.0 / 12.0) * phi + (7.0 / 12.0) * phip1 + (-1.0 / 12.0) * phip2;
+  const double p3 = (1.0 / 4.0) * phi + (13.0 / 12.0) * phip1 + (-5.0 / 12.0) * phip2 + (1.0 / 12.0) * phip3;
+  const double beta0 = (phim3 * (547.0 * phim3 - 3882.0 * phim2 + 4642.0 * phim1 - 1854.0 * phi) +
+                        phim2 * (7043.0 * phim2 - 17246.0 * phim1 + 7042.0 * phi) +
+                        phim1 * (11003.0 * phim1 - 9402.0 * phi) + 2107.0 * phi * phi);
+  const double beta1 = (phim2 * (267.0 * phim2 - 1642.0 * phim1 + 1602.0 * phi - 494.0 * phip1) +
+                        phim1 * (2843.0 * phim1 - 5966.0 * phi + 1922.0 * phip1) +
+                        phi * (3443.0 * phi - 2522.0 * phip1) + 547.0 * phip1 * phip1);
+  const double beta2 = (phim1 * (547.0 * phim1 - 2522.0 * phi + 1922.0 * phip1 - 494.0 * phip2) +
+                        phi * (3443.0 * phi - 5966.0 * phip1 + 1602.0 * phip2) +
+                        phip1 * (2843.0 * phip1 - 1642.0 * phip2) + 267.0 * phip2 * phip2);
+  const double beta3 = (phi * (2107.0 * phi - 9402.0 * phip1 + 7042.0 * phip2 - 1854.0 * phip3) +
+                        phip1 * (11003.0 * phip1 - 17246.0 * phip2 + 4642.0 * phip3) +
+                        phip2 * (7043.0 * phip2 - 3882.0 * phip3) + 547.0 * phip3 * phip3);
+  const double e0 = beta0 + 1e-10, e1 = beta1 + 1e-10, e2 = beta2 + 1e-10, e3 = beta3 + 1e-10;
+  const double q0 = e0 * e0, q1 = e1 * e1, q2 = e2 * e2, q3 = e3 * e3;
+  const double q01 = q0 * q1, q23 = q2 * q3;
+  const double n0 = (1.0 / 35.0) * (q1 * q23);
+  const double n1 = (12.0 / 35.0) * (q0 * q23);
+  const double n2 = (18.0 / 35.0) * (q3 * q01);
+  const double n3 = (4.0 / 35.0) * (q2 * q01);
+  return (n0 * p0 + n1 * p1 + n2 * p2 + n3 * p3) / (n0 + n1 + n2 + n3);
+}
+
 // Face value from a stencil held in an array: ORDER 5 reads v[0..4]
 // (upwind-positive: centre v[2]), ORDER 7 reads v[0..6] (centre v[3]).
 // F32 selects the shifted mixed-precision evaluation described above.
