@@ -219,6 +219,32 @@ int pb_pressure_solve(const pb_dims* dims, const double* rho0, const double* rho
                       double* w, double* divergence, double* dynamic_pressure, void* workspace,
                       long long workspace_bytes, int precision, void* stream);
 
+/*
+ * pb_pressure_solve for callers that cannot allocate device memory.  No
+ * counterpart in the reference.  Same inputs, outputs and results as
+ * pb_pressure_solve (FP64), but its scratch lives in a fixed file-scope
+ * device array inside the library instead of a caller workspace, for code
+ * that may not call cudaMalloc (a graph capture that must not allocate, an
+ * allocator policy that forbids late device allocations, a host binding
+ * without a device allocator).
+ *   Limit : pb_pressure_workspace_bytes(dims) must not exceed
+ *           PB_PRESSURE_NOALLOC_MAX_BYTES (64 MiB, e.g. 128 x 128 x 160);
+ *           larger grids return PB_ERR_WORKSPACE.  Every GPU that loads the
+ *           library holds the 64 MiB until the process exits.
+ *   Set-up: the first call on a device, and the first call after the grid
+ *           changes, takes the array's device address (cudaGetSymbolAddress)
+ *           and fills the grid constants synchronously -- make that first
+ *           call before any stream capture.
+ *   Races : all calls on a device share the array (it keeps the last call's
+ *           contents; nothing needs clearing, every word read is written
+ *           first in the same call), so calls that may overlap on the GPU
+ *           must be ordered by the caller.
+ */
+#define PB_PRESSURE_NOALLOC_MAX_BYTES (64ll << 20)
+int pb_pressure_solve_noalloc(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                              const double* alpha0, const double* alpha0_half, double* u, double* v,
+                              double* w, double* divergence, double* dynamic_pressure, void* stream);
+
 /* ------------------------------------------------------------------------
  * Errors
  * --------------------------------------------------------------------- */

@@ -57,6 +57,7 @@ SIGNATURES = {
     "pb_pressure_workspace_bytes": (_LL, [_DIMS]),
     "pb_pressure_init": (_I, [_DIMS, _P, _LL]),
     "pb_pressure_solve": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
+    "pb_pressure_solve_noalloc": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "pb_get_error": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "pb_clear_error": (_I, [_P]),
     "pb_status_string": (ctypes.c_char_p, [_I]),

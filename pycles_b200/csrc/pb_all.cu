@@ -4,3 +4,4 @@
 #include "timestep.cu"
 #include "advection.cu"
 #include "pressure.cu"
+#include "pressure_noalloc.cu"
