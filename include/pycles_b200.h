@@ -139,7 +139,10 @@ int pb_momentum_advection(const pb_dims* dims, const double* rho0, const double*
  * (:68-96, per-cell eos_c secant :17-66 and alpha_c), buoyancy_update_sa
  * (:98-132, adds to w_tend), bvf_sa (:134-182), thetali_update (:185-211).
  * Latent heat: latent_heat_variable, lambda = 1 (Microphysics.pxd:65-75).
- *   mlp (nullable)        : learned seed for the secant's second point.
+ *   mlp (nullable)        : learned seed for the secant's second point
+ *                           (no counterpart in the reference); the seeds of
+ *                           the saturated cells are evaluated first into
+ *                           seed_scratch (npg doubles, required with mlp).
  *   secant_iters (nullable): device long long[2]; receives
  *                           {sum of secant iterations, saturated cells}.
  *   max_iter              : secant iteration cap (the reference has none);
@@ -149,7 +152,7 @@ int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const double* alpha
                  const pb_table* table, const double* s, double* qt, double* T, double* qv,
                  double* ql, double* qi, double* alpha, double* buoyancy, double* theta_rho,
                  double* bvf, double* thetali, double* w_tend, int clip_qt, const pb_mlp* mlp,
-                 long long* secant_iters, int max_iter, void* stream);
+                 double* seed_scratch, long long* secant_iters, int max_iter, void* stream);
 
 /*
  * ThermodynamicsDry.update (ThermodynamicsDry.pyx:105-120): eos_update
@@ -159,6 +162,44 @@ int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const double* alpha
 int pb_thermo_dry(const pb_dims* dims, const double* p0_half, const double* alpha0_half,
                   const double* s, double* T, double* alpha, double* buoyancy, double* theta,
                   double* bvf, double* w_tend, void* stream);
+
+/*
+ * ThermodynamicsSA.eos (ThermodynamicsSA.pyx:169-174) for n points: eos_c
+ * (Csrc/thermodynamics_sa.h:17-66) on (p0[i], s[i], qt[i]) -> T[i], ql[i],
+ * qi[i] (ql, qi nullable), iters[i] = secant iterations (nullable; 0 for
+ * unsaturated points).  seed (nullable) replaces the secant's second point.
+ */
+int pb_eos_sa(const pb_table* table, const double* p0, const double* s, const double* qt,
+              const double* seed, double* T, double* ql, double* qi, int* iters, long long n,
+              int max_iter, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned seed (no counterpart in the reference).  BF16 tensor-core
+ * (mma.sync m16n8k16, FP32 accumulation) forward and backward passes of the
+ * 3 -> 64 -> 64 -> 1 SiLU MLP of pb_mlp.  Packed FP32 parameter vector
+ * (PB_MLP_NPARAM = 4417): W1[64][3], b1[64], W2[64][64], b2[64], w3[64], b3.
+ * --------------------------------------------------------------------- */
+#define PB_MLP_NPARAM 4417
+
+/* T_seed[i] = out_mean + out_scale * MLP(normalised p0[i], s[i], qt[i]). */
+int pb_mlp_forward(const pb_mlp* mlp, const double* p0, const double* s, const double* qt,
+                   double* T_seed, long long n, void* stream);
+
+/*
+ * Adds the gradient of sum_i 0.5 (MLP(x_i) - target_i)^2 to grad[PB_MLP_NPARAM]
+ * and the loss sum to *loss (both FP32, device, accumulated).  x: n x 3
+ * inputs already normalised to [-1, 1]; target: n normalised outputs.
+ */
+int pb_mlp_grad(const pb_mlp* mlp, const float* x, const float* target, long long n, float* grad,
+                float* loss, void* stream);
+
+/*
+ * One Adam step on the FP32 master parameters (grad scaled by grad_scale),
+ * then refreshes the BF16 weights and FP32 biases the kernels read.
+ */
+int pb_mlp_adam(float* params, float* m, float* v, const float* grad, int step, float lr, float beta1,
+                float beta2, float eps, float grad_scale, void* w1, float* b1, void* w2, float* b2,
+                void* w3, float* b3, void* stream);
 
 /* ------------------------------------------------------------------------
  * Time stepping and boundary conditions
@@ -213,11 +254,16 @@ int pb_pressure_init(const pb_dims* dims, void* workspace, long long workspace_b
  *   workspace : >= pb_pressure_workspace_bytes(dims) bytes, 256-byte aligned,
  *               initialised by pb_pressure_init.
  *   n[0], n[1] : any size; powers of two take the radix-2 path.
+ *   precision  : PB_FP64 -- the reference method in FP64 (refine_sweeps
+ *                ignored).  PB_FP32 -- the precision form: FFTs in FP32,
+ *                tridiagonal solves in FP64, then refine_sweeps (0..8)
+ *                iterative-refinement sweeps p += solve(div - A p) with the
+ *                residual evaluated in FP64 (no counterpart in the reference).
  */
 int pb_pressure_solve(const pb_dims* dims, const double* rho0, const double* rho0_half,
                       const double* alpha0, const double* alpha0_half, double* u, double* v,
                       double* w, double* divergence, double* dynamic_pressure, void* workspace,
-                      long long workspace_bytes, int precision, void* stream);
+                      long long workspace_bytes, int precision, int refine_sweeps, void* stream);
 
 /*
  * pb_pressure_solve for callers that cannot allocate device memory.  No

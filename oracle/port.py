@@ -11,9 +11,35 @@ Pinned against the compiled reference (``oracle.ref``) by
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 from .dims import Dims
+
+# The reference evaluates exp/log/pow with the C library; numpy's vectorised
+# versions differ from it in the last bit now and then, which the buoyancy's
+# cancellation amplifies.  These call the C library (Python's math module)
+# elementwise so the restatement matches the reference's transcendentals
+# bit for bit.
+_vlog = np.frompyfunc(math.log, 1, 1)
+_vexp = np.frompyfunc(math.exp, 1, 1)
+_vpow = np.frompyfunc(math.pow, 2, 1)
+
+
+def _log(x):
+    r = _vlog(np.asarray(x, dtype=np.float64))
+    return np.asarray(r, dtype=np.float64)
+
+
+def _exp(x):
+    r = _vexp(np.asarray(x, dtype=np.float64))
+    return np.asarray(r, dtype=np.float64)
+
+
+def _pow(x, y):
+    r = _vpow(np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64))
+    return np.asarray(r, dtype=np.float64)
 
 # generate_parameters.py:19-41 (values as written to parameters.h)
 g = 9.80665
@@ -203,7 +229,7 @@ def advective_tendencies_m(d: Dims, rho0, rho0_half, alpha0, alpha0_half, vel_ad
 # thermodynamic functions, Csrc/thermodynamic_functions.h, Csrc/entropies.h
 # ---------------------------------------------------------------------------
 def exner_c(p0):
-    return np.power(p0 / p_tilde, kappa)
+    return _pow(p0 / p_tilde, kappa)
 
 
 def pd_c(p0, qt, qv):
@@ -231,11 +257,11 @@ def cpm_c(qt):
 
 
 def sd_c(pd, T):
-    return sd_tilde + cpd * np.log(T / T_tilde) - Rd * np.log(pd / p_tilde)
+    return sd_tilde + cpd * _log(T / T_tilde) - Rd * _log(pd / p_tilde)
 
 
 def sv_c(pv, T):
-    return sv_tilde + cpv * np.log(T / T_tilde) - Rv * np.log(pv / p_tilde)
+    return sv_tilde + cpv * _log(T / T_tilde) - Rv * _log(pv / p_tilde)
 
 
 def sc_c(L, T):
@@ -269,9 +295,9 @@ class Table:
 
 def temperature_no_ql(pd, pv, s, qt):
     """Csrc/thermodynamics_sa.h:10-15."""
-    return T_tilde * np.exp((s - (1.0 - qt) * (sd_tilde - Rd * np.log(pd / p_tilde))
-                             - qt * (sv_tilde - Rv * np.log(pv / p_tilde)))
-                            / ((1.0 - qt) * cpd + qt * cpv))
+    return T_tilde * _exp((s - (1.0 - qt) * (sd_tilde - Rd * _log(pd / p_tilde))
+                           - qt * (sv_tilde - Rv * _log(pv / p_tilde)))
+                          / ((1.0 - qt) * cpd + qt * cpv))
 
 
 def eos_c(LT: Table, p0, s, qt, max_iter=10_000, T2_seed=None):
@@ -422,13 +448,13 @@ def thetali_update(d: Dims, p0, T, qt, ql, qi, thetali):
     Lv = latent_heat_variable(Tt_)
     Q = qt.reshape(sh)
     theta = Tt_ / exner_c(P)
-    thetali[:] = (theta * np.exp(-Lv * (ql.reshape(sh) / (1.0 - Q) + qi.reshape(sh) / (1.0 - Q))
-                                 / (Tt_ * cpd))).reshape(-1)
+    thetali[:] = (theta * _exp(-Lv * (ql.reshape(sh) / (1.0 - Q) + qi.reshape(sh) / (1.0 - Q))
+                               / (Tt_ * cpd))).reshape(-1)
 
 
 # dry thermodynamics, Csrc/thermodynamics_dry.h ------------------------------
 def dry_eos_c(pd, s):  # :8-10
-    return T_tilde * (np.exp((s - sd_tilde + Rd * np.log(pd / p_tilde)) / cpd))
+    return T_tilde * (_exp((s - sd_tilde + Rd * _log(pd / p_tilde)) / cpd))
 
 
 def eos_update_dry(d: Dims, pd, s, T, alpha):  # :12-37

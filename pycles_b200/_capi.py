@@ -42,6 +42,7 @@ class PbMlp(ctypes.Structure):
 PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_UNSUPPORTED, PB_ERR_WORKSPACE = 0, 1, 2, 3, 4
 PB_FP64, PB_FP32 = 0, 1
 ERR_TABLE_RANGE, ERR_SECANT_CAP, ERR_NONFINITE = 0x1, 0x2, 0x4
+MLP_NPARAM = 4417
 
 # name -> (restype, argtypes); every symbol include/pycles_b200.h declares
 _I, _LL, _D, _P = ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p
@@ -50,13 +51,18 @@ SIGNATURES = {
     "pb_scalar_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _I, _I, _P]),
     "pb_momentum_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P]),
     "pb_thermo_sa": (_I, [_DIMS, _P, _P, ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
-                          _P, _I, ctypes.POINTER(PbMlp), _P, _I, _P]),
+                          _P, _I, ctypes.POINTER(PbMlp), _P, _P, _I, _P]),
+    "pb_eos_sa": (_I, [ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
+    "pb_mlp_forward": (_I, [ctypes.POINTER(PbMlp), _P, _P, _P, _P, _LL, _P]),
+    "pb_mlp_grad": (_I, [ctypes.POINTER(PbMlp), _P, _P, _LL, _P, _P, _P]),
+    "pb_mlp_adam": (_I, [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                         ctypes.c_float, _P, _P, _P, _P, _P, _P, _P]),
     "pb_thermo_dry": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "pb_rk3_update": (_I, [_P, _P, _P, _LL, _D, _I, _P]),
     "pb_update_all_bcs": (_I, [_DIMS, _P, _P, _I, _P]),
     "pb_pressure_workspace_bytes": (_LL, [_DIMS]),
     "pb_pressure_init": (_I, [_DIMS, _P, _LL]),
-    "pb_pressure_solve": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
+    "pb_pressure_solve": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _I, _P]),
     "pb_pressure_solve_noalloc": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "pb_get_error": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "pb_clear_error": (_I, [_P]),

@@ -68,18 +68,25 @@ __global__ void __launch_bounds__(128) scalar_march(Geo g, ScalarArgs a, int chu
 
   double win[NS][W];
   double fprev[NS];
+  double nxt[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
 #pragma unroll
     for (int m = 0; m < W - 1; ++m) win[q][m] = a.s[q][(c0 - 1 - R + 1 + m) * sD + base];
+    nxt[q] = a.s[q][(c0 - 1 + R) * sD + base];
     fprev[q] = 0.0;
   }
+  double vnxt = a.vel[(c0 - 1) * sD + base];
   for (long long f = c0 - 1; f < c1; ++f) {
     const long long idx = f * sD + base;
-    const double vel = a.vel[idx];
+    const double vel = vnxt;
+    // software prefetch of the next face's loads, consumed one iteration later
+    const bool more = f + 1 < c1;
+    if (more) vnxt = a.vel[idx + sD];
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
-      win[q][W - 1] = a.s[q][(f + R) * sD + base];
+      win[q][W - 1] = nxt[q];
+      if (more) nxt[q] = a.s[q][(f + 1 + R) * sD + base];
       double phip, phim;
       if constexpr (ORDER == 5) {
         phip = weno_face<5, F32>(win[q][0], win[q][1], win[q][2], win[q][3], win[q][4]);
@@ -170,16 +177,22 @@ __global__ void __launch_bounds__(128) momentum_march(Geo g, MomArgs a, int chun
 
   double win[3][W];
   double fprev[3];
+  double nxt[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
 #pragma unroll
     for (int m = 0; m < W - 1; ++m) win[c][m] = a.vel[c][(c0 - 1 - R + 1 + m) * sD + base];
+    nxt[c] = a.vel[c][(c0 - 1 + R) * sD + base];
     fprev[c] = 0.0;
   }
   for (long long f = c0 - 1; f < c1; ++f) {
     const long long idx = f * sD + base;
+    const bool more = f + 1 < c1;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) win[c][W - 1] = a.vel[c][(f + R) * sD + base];
+    for (int c = 0; c < 3; ++c) {
+      win[c][W - 1] = nxt[c];
+      if (more) nxt[c] = a.vel[c][(f + 1 + R) * sD + base];
+    }
     // window position of face f is R-1
 #pragma unroll
     for (int c = 0; c < 3; ++c) {

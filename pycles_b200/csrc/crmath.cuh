@@ -92,8 +92,15 @@ __device__ __forceinline__ double log(double x) {
   const int j = (int)(mbits >> 44);                                        // top 8 bits
   const double c = 1.0 + (double)j * (1.0 / 256.0);
   const double f = __dsub_rn(mm, c);  // exact
-  const double vh = f / c;
-  const double vl = fma(-vh, c, f) / c;
+  // v = f/c to ~2^-105 without a division: vh = f*(1/c) is off by at most a
+  // few ulp, the remainder f - vh*c is exact (FMA), and its quotient by c
+  // needs only a relative accuracy of 2^-50
+  const double rc = __ldg(CRM_INVC_TAB + j);
+  const double vh0 = __dmul_rn(f, rc);
+  const double vl0 = __dmul_rn(fma(-vh0, c, f), rc);
+  const dd v = fast_two_sum(vh0, vl0);
+  const double vh = v.hi;
+  const double vl = v.lo;
   // log1p(v) = v - v^2/2 + v^3 (1/3 - v/4 + v^2/5 - v^3/6 + v^4/7 - v^5/8 + v^6/9)
   const double tail =
       vh * vh * vh *

@@ -1,0 +1,152 @@
+// Learned saturation-adjustment seed: a 3 -> 64 -> 64 -> 1 SiLU MLP.
+//
+// One warp evaluates a tile of 16 samples.  Layer 1 (K = 3) and layer 3
+// (N = 1) run on the FP32 pipes; the 64 x 64 layer runs on the tensor cores
+// with mma.sync m16n8k16 (BF16 operands, FP32 accumulation).  Each lane
+// computes exactly the layer-1 activations that its A fragments hold, so no
+// shuffles or shared memory are needed between layers:
+//   A fragment (16x16, row-major), lane = 4*g + t (g = lane/4, t = lane%4):
+//     regs 0/1/2/3 = rows {g, g+8, g, g+8} x cols {2t, 2t, 2t+8, 2t+8} (+0,+1)
+//   B fragment (16x8, column-major): regs 0/1 = k {2t, 2t+8} (+0,+1), n = g
+//   C fragment (16x8): c0,c1 = row g, cols 2t,2t+1; c2,c3 = row g+8
+// so the C fragments of n-tiles 2kt and 2kt+1 are, reinterpreted, the A
+// fragment of k-tile kt (used by the backward pass).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace mlpk {
+
+constexpr int H = 64;
+// packed parameter layout (FP32 masters and gradients)
+constexpr int OFF_W1 = 0;                // [64][3]
+constexpr int OFF_B1 = OFF_W1 + H * 3;   // [64]
+constexpr int OFF_W2 = OFF_B1 + H;       // [64][64] (row = output unit)
+constexpr int OFF_B2 = OFF_W2 + H * H;   // [64]
+constexpr int OFF_W3 = OFF_B2 + H;       // [64]
+constexpr int OFF_B3 = OFF_W3 + H;       // [1]
+constexpr int NPARAM = OFF_B3 + 1;
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Weights staged in shared memory by the block.
+struct Smem {
+  float w1[H * 3];
+  float b1[H];
+  __nv_bfloat16 w2[H * H];  // [n][k]
+  float b2[H];
+  float w3[H];
+  float b3;
+};
+
+// Loads BF16 weights + FP32 biases into shared memory (whole block).
+__device__ __forceinline__ void stage_weights(Smem& sm, const __nv_bfloat16* w1, const float* b1,
+                                              const __nv_bfloat16* w2, const float* b2, const __nv_bfloat16* w3,
+                                              const float* b3) {
+  for (int i = threadIdx.x; i < H * H; i += blockDim.x) sm.w2[i] = w2[i];
+  for (int i = threadIdx.x; i < H * 3; i += blockDim.x) sm.w1[i] = __bfloat162float(w1[i]);
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    sm.b1[i] = b1[i];
+    sm.b2[i] = b2[i];
+    sm.w3[i] = __bfloat162float(w3[i]);
+  }
+  if (threadIdx.x == 0) sm.b3 = b3[0];
+}
+
+// Forward pass of one 16-row tile.  xr0/xr1: the 3 normalised inputs of the
+// lane's rows g and g+8.  Returns y for rows g (y0) and g+8 (y1), valid on
+// lanes with t == 0 (all lanes of a group hold the same value after the
+// reduction).  Optionally keeps z1, h1 fragments, z2, h2 for the backward pass.
+struct Tile {
+  float z1[4][4][2];   // [ktile][reg][pair]  (rows/cols as the A fragment)
+  uint32_t a1[4][4];   // BF16 h1 A fragments
+  float z2[8][4];      // [ntile][c-reg]
+  float h2[8][4];
+};
+
+__device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3], const float xr1[3], float& y0,
+                                             float& y1, Tile* keep) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  uint32_t a1[4][4];
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const float* x = (r & 1) ? xr1 : xr0;
+      const int col = kt * 16 + 2 * t + ((r & 2) ? 8 : 0);
+      float h[2];
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        const int c = col + p;
+        const float z = sm.b1[c] + sm.w1[c * 3 + 0] * x[0] + sm.w1[c * 3 + 1] * x[1] + sm.w1[c * 3 + 2] * x[2];
+        if (keep) keep->z1[kt][r][p] = z;
+        h[p] = silu(z);
+      }
+      a1[kt][r] = pack_bf16(h[0], h[1]);
+    }
+  }
+  if (keep) {
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) keep->a1[kt][r] = a1[kt][r];
+  }
+  float p0 = 0.0f, p1 = 0.0f;
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      const int n = nt * 8 + g;
+      const int k = kt * 16 + 2 * t;
+      uint32_t b[2];
+      b[0] = *reinterpret_cast<const uint32_t*>(&sm.w2[n * H + k]);
+      b[1] = *reinterpret_cast<const uint32_t*>(&sm.w2[n * H + k + 8]);
+      mma_bf16_16816(c, a1[kt], b);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int col = nt * 8 + 2 * t + (q & 1);
+      const float z = c[q] + sm.b2[col];
+      const float h = silu(z);
+      if (keep) {
+        keep->z2[nt][q] = z;
+        keep->h2[nt][q] = h;
+      }
+      if (q < 2) p0 += sm.w3[col] * h;
+      else p1 += sm.w3[col] * h;
+    }
+  }
+  // reduce over the 4 lanes of the group (they hold the other columns)
+  p0 += __shfl_xor_sync(0xffffffffu, p0, 1);
+  p0 += __shfl_xor_sync(0xffffffffu, p0, 2);
+  p1 += __shfl_xor_sync(0xffffffffu, p1, 1);
+  p1 += __shfl_xor_sync(0xffffffffu, p1, 2);
+  y0 = p0 + sm.b3;
+  y1 = p1 + sm.b3;
+}
+
+__device__ __forceinline__ float norm_in(double v, float lo, float hi) {
+  return (float)(2.0 * (v - (double)lo) / ((double)hi - (double)lo) - 1.0);
+}
+
+}  // namespace mlpk

@@ -5,3 +5,4 @@
 #include "advection.cu"
 #include "pressure.cu"
 #include "pressure_noalloc.cu"
+#include "mlp.cu"

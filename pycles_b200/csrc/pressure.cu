@@ -31,7 +31,7 @@ constexpr int kPartials = 296;  // 2 x 148 SMs
 constexpr int kFftThreads = 256;
 
 struct PLayout {
-  long long partial, mean, twx, twy, kx2, ky2, spec, scr, total;
+  long long partial, mean, twx, twy, twxf, twyf, kx2, ky2, spec, scr, total;
 };
 
 long long align256(long long x) { return (x + 255) / 256 * 256; }
@@ -45,6 +45,8 @@ PLayout playout(const pb_dims* d) {
   L.mean = off;    off += align256(nlg2 * 8);
   L.twx = off;     off += align256(n0 * 16);
   L.twy = off;     off += align256(n1 * 16);
+  L.twxf = off;    off += align256(n0 * 8);
+  L.twyf = off;    off += align256(n1 * 8);
   L.kx2 = off;     off += align256(n0 * 8);
   L.ky2 = off;     off += align256(n1 * 8);
   L.spec = off;    off += align256(n0 * n1 * n2 * 16);
@@ -55,14 +57,28 @@ PLayout playout(const pb_dims* d) {
 
 __device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 
+// Complex arithmetic on double2 (plain form) or float2 (precision form).
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+template <class C> __device__ __forceinline__ C czero();
+template <> __device__ __forceinline__ double2 czero<double2>() { return make_double2(0.0, 0.0); }
+template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.0f, 0.0f); }
+template <class C> __device__ __forceinline__ C creal(double x);
+template <> __device__ __forceinline__ double2 creal<double2>(double x) { return make_double2(x, 0.0); }
+template <> __device__ __forceinline__ float2 creal<float2>(double x) { return make_float2((float)x, 0.0f); }
 
 // In-place radix-2 DIT over `nlines` lines of length N (power of two) held
 // in shared memory in bit-reversed order.  tw[m] = exp(-2 pi i m / N).
-__device__ void fft_pow2_lines(double2* buf, int nlines, int N, int logN, const double2* __restrict__ tw,
-                               bool inverse) {
+template <class C>
+__device__ void fft_pow2_lines(C* buf, int nlines, int N, int logN, const C* __restrict__ tw, bool inverse) {
   const int halfN = N >> 1;
   for (int s = 1; s <= logN; ++s) {
     const int half = 1 << (s - 1);
@@ -74,32 +90,30 @@ __device__ void fft_pow2_lines(double2* buf, int nlines, int N, int logN, const 
       const int pos = bb & (half - 1);
       const int i0 = line * N + group * 2 * half + pos;
       const int i1 = i0 + half;
-      double2 w = __ldg(tw + pos * twstride);
+      C w = tw[pos * twstride];
       if (inverse) w.y = -w.y;
-      const double2 x0 = buf[i0];
-      const double2 t = cmul(w, buf[i1]);
-      buf[i0] = make_double2(x0.x + t.x, x0.y + t.y);
-      buf[i1] = make_double2(x0.x - t.x, x0.y - t.y);
+      const C x0 = buf[i0];
+      const C t = cmul(w, buf[i1]);
+      buf[i0] = cadd(x0, t);
+      buf[i1] = csub(x0, t);
     }
     __syncthreads();
   }
 }
 
 // Direct DFT for lengths that are not powers of two: out = DFT(in).
-__device__ void dft_lines(const double2* in, double2* out, int nlines, int N, const double2* __restrict__ tw,
-                          bool inverse) {
+template <class C>
+__device__ void dft_lines(const C* in, C* out, int nlines, int N, const C* __restrict__ tw, bool inverse) {
   for (int e = threadIdx.x; e < nlines * N; e += blockDim.x) {
     const int line = e / N;
     const int m = e - line * N;
-    double2 acc = make_double2(0.0, 0.0);
-    const double2* x = in + line * N;
+    C acc = czero<C>();
+    const C* x = in + line * N;
     int idx = 0;
     for (int n = 0; n < N; ++n) {
-      double2 w = __ldg(tw + idx);
+      C w = tw[idx];
       if (inverse) w.y = -w.y;
-      const double2 t = cmul(w, x[n]);
-      acc.x += t.x;
-      acc.y += t.y;
+      acc = cadd(acc, cmul(w, x[n]));
       idx += m;
       if (idx >= N) idx -= N;
     }
@@ -127,12 +141,21 @@ struct PArgs {
   double* mean;
   const double2* twx;
   const double2* twy;
+  const float2* twxf;
+  const float2* twyf;
   const double* kx2;
   const double* ky2;
-  double2* spec;
+  void* spec;     // double2 (plain form) or float2 (precision form) W[k][j][i]
   double* scr;
   int log0, log1;
 };
+
+template <class C> __device__ __forceinline__ const C* twx_of(const PArgs& a);
+template <> __device__ __forceinline__ const double2* twx_of<double2>(const PArgs& a) { return a.twx; }
+template <> __device__ __forceinline__ const float2* twx_of<float2>(const PArgs& a) { return a.twxf; }
+template <class C> __device__ __forceinline__ const C* twy_of(const PArgs& a);
+template <> __device__ __forceinline__ const double2* twy_of<double2>(const PArgs& a) { return a.twy; }
+template <> __device__ __forceinline__ const float2* twy_of<float2>(const PArgs& a) { return a.twyf; }
 
 // ---- HorizontalMean (ParallelMPI.pyx:196-241) ------------------------------
 __global__ void hmean_partial(Geo g, const double* __restrict__ w, double* __restrict__ partial) {
@@ -204,10 +227,19 @@ __global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
   }
 }
 
-// ---- divergence + forward x-FFT -------------------------------------------
+// ---- divergence (or refinement residual) + forward x-FFT --------------------
 // block = (interior j, chunk of KC interior levels); smem KC lines of n0.
+// RESID = false: the right-hand side is second_order_divergence
+//   (PressureSolver.pyx:138-175, d = 0, 1, 2 in order), written to `div`.
+// RESID = true: the right-hand side is the residual div - A p of the current
+//   pressure, A being the operator the spectral solve inverts (second
+//   differences in x and y, the rows of compute_off_diagonals /
+//   compute_diagonal in z); used by the iterative refinement of the
+//   precision form.
+template <class C, bool RESID>
 __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC) {
-  extern __shared__ double2 sbuf[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* in = reinterpret_cast<C*>(smraw);
   const int N = (int)(g.n0 - 2 * g.gw);
   const int nz = (int)(g.n2 - 2 * g.gw);
   const int jl = blockIdx.x;
@@ -215,7 +247,6 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
   const int kc = min(KC, nz - k0);
   const long long j = g.gw + jl;
   const bool p2 = is_pow2(N);
-  double2* in = sbuf;
   const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
   for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
     const int kl = e % KC;
@@ -223,42 +254,56 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
     if (kl >= kc) continue;
     const long long k = g.gw + k0 + kl;
     const long long ijk = (g.gw + il) * g.is + j * g.js + k;
-    // second_order_divergence (PressureSolver.pyx:138-175), d = 0, 1, 2
-    const double ah = a.alpha0_half[k];
-    double d = 0.0;
-    d = add_rn(d, mul_rn(sub_rn(a.u[ijk] / ah, a.u[ijk - g.is] / ah), dxi0));
-    d = add_rn(d, mul_rn(sub_rn(a.v[ijk] / ah, a.v[ijk - g.js] / ah), dxi1));
-    d = add_rn(d, mul_rn(sub_rn((a.w[ijk]) / a.alpha0[k], (a.w[ijk - 1]) / a.alpha0[k - 1]), dxi2));
-    a.div[ijk] = d;
-    in[kl * N + slot(il, N, a.log0)] = make_double2(d, 0.0);
+    double d;
+    if (!RESID) {
+      const double ah = a.alpha0_half[k];
+      d = 0.0;
+      d = add_rn(d, mul_rn(sub_rn(a.u[ijk] / ah, a.u[ijk - g.is] / ah), dxi0));
+      d = add_rn(d, mul_rn(sub_rn(a.v[ijk] / ah, a.v[ijk - g.js] / ah), dxi1));
+      d = add_rn(d, mul_rn(sub_rn((a.w[ijk]) / a.alpha0[k], (a.w[ijk - 1]) / a.alpha0[k - 1]), dxi2));
+      a.div[ijk] = d;
+    } else {
+      const double* p = a.p;
+      const double pc = p[ijk];
+      const double lap_h = a.rho0_half[k] * ((p[ijk + g.is] - 2.0 * pc + p[ijk - g.is]) * (dxi0 * dxi0) +
+                                             (p[ijk + g.js] - 2.0 * pc + p[ijk - g.js]) * (dxi1 * dxi1));
+      const long long kk = k - g.gw;
+      double vert = 0.0;
+      if (kk < nz - 1) vert += a.rho0[k] * (p[ijk + 1] - pc);
+      if (kk > 0) vert -= a.rho0[k - 1] * (pc - p[ijk - 1]);
+      d = a.div[ijk] - (lap_h + vert * (dxi2 * dxi2));
+    }
+    in[kl * N + slot(il, N, a.log0)] = creal<C>(d);
   }
   __syncthreads();
-  double2* res = in;
+  C* res = in;
   if (p2) {
-    fft_pow2_lines(in, kc, N, a.log0, a.twx, false);
+    fft_pow2_lines<C>(in, kc, N, a.log0, twx_of<C>(a), false);
   } else {
     res = in + N * KC;
-    dft_lines(in, res, kc, N, a.twx, false);
+    dft_lines<C>(in, res, kc, N, twx_of<C>(a), false);
   }
+  C* spec = reinterpret_cast<C*>(a.spec);
   const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
   for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
     const int il = e % N;
     const int kl = e / N;
-    a.spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il] = res[kl * N + il];
+    spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il] = res[kl * N + il];
   }
 }
 
 // ---- y-FFT over W[k][j][i] lines along j, IC columns i per block ----------
+template <class C>
 __global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, bool inverse) {
-  extern __shared__ double2 sbuf[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* in = reinterpret_cast<C*>(smraw);
   const int Nx = (int)(g.n0 - 2 * g.gw);
   const int N = (int)(g.n1 - 2 * g.gw);
   const int kk = blockIdx.y;
   const int i0 = blockIdx.x * IC;
   const int ic = min(IC, Nx - i0);
   const bool p2 = is_pow2(N);
-  double2* in = sbuf;
-  double2* plane = a.spec + (long long)kk * N * Nx;
+  C* plane = reinterpret_cast<C*>(a.spec) + (long long)kk * N * Nx;
   for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
     const int il = e % IC;
     const int jl = e / IC;
@@ -266,19 +311,19 @@ __global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, boo
     in[il * N + slot(jl, N, a.log1)] = plane[(long long)jl * Nx + i0 + il];
   }
   __syncthreads();
-  double2* res = in;
+  C* res = in;
   if (p2) {
-    fft_pow2_lines(in, ic, N, a.log1, a.twy, inverse);
+    fft_pow2_lines<C>(in, ic, N, a.log1, twy_of<C>(a), inverse);
   } else {
     res = in + N * IC;
-    dft_lines(in, res, ic, N, a.twy, inverse);
+    dft_lines<C>(in, res, ic, N, twy_of<C>(a), inverse);
   }
   const double sc = inverse ? 1.0 / (double)N : 1.0;
   for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
     const int il = e % IC;
     const int jl = e / IC;
     if (il >= ic) continue;
-    double2 r = res[il * N + jl];
+    C r = res[il * N + jl];
     if (inverse) {
       r.x *= sc;
       r.y *= sc;
@@ -287,10 +332,19 @@ __global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, boo
   }
 }
 
-// ---- per-column tridiagonal solve ------------------------------------------
+__device__ __forceinline__ void to_d(double2 c, double& x, double& y) { x = c.x; y = c.y; }
+__device__ __forceinline__ void to_d(float2 c, double& x, double& y) { x = c.x; y = c.y; }
+template <class C> __device__ __forceinline__ C from_d(double x, double y);
+template <> __device__ __forceinline__ double2 from_d<double2>(double x, double y) { return make_double2(x, y); }
+template <> __device__ __forceinline__ float2 from_d<float2>(double x, double y) {
+  return make_float2((float)x, (float)y);
+}
+
+// ---- per-column tridiagonal solve (always FP64 arithmetic) -----------------
 // Matrix of PressureFFTParallel.compute_off_diagonals (:100-127) and
 // compute_diagonal (:129-148); Thomas algorithm of TDMA.solve applied to the
 // real and imaginary parts (the matrix is real, so both share m and scratch).
+template <class C>
 __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
   const int Nx = (int)(g.n0 - 2 * g.gw);
   const int Ny = (int)(g.n1 - 2 * g.gw);
@@ -300,10 +354,10 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
   if (col >= ncol) return;
   const int i = (int)(col % Nx);
   const int j = (int)(col / Nx);
-  double2* x = a.spec + col;
+  C* x = reinterpret_cast<C*>(a.spec) + col;
   double* scr = a.scr + col;
   if (i == 0 && j == 0) {  // mode (0,0) is set to zero (:197-200)
-    for (int k = 0; k < nz; ++k) x[(long long)k * ncol] = make_double2(0.0, 0.0);
+    for (int k = 0; k < nz; ++k) x[(long long)k * ncol] = from_d<C>(0.0, 0.0);
     return;
   }
   const long long gw = g.gw;
@@ -321,10 +375,11 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
     c = 0.0;
   }
   double s_prev = c / b;
-  double2 xp = x[0];
-  xp.x = xp.x / b;
-  xp.y = xp.y / b;
-  x[0] = xp;
+  double xpx, xpy;
+  to_d(x[0], xpx, xpy);
+  xpx = xpx / b;
+  xpy = xpy / b;
+  x[0] = from_d<C>(xpx, xpy);
   scr[0] = s_prev;
   for (int k = 1; k < nz; ++k) {
     const double ak = mul_rn(mul_rn(dzi, dzi), rho0[k + gw - 1]);
@@ -339,45 +394,53 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
     const double m = 1.0 / sub_rn(bk, mul_rn(ak, s_prev));
     s_prev = mul_rn(ck, m);
     scr[(long long)k * ncol] = s_prev;
-    double2 xk = x[(long long)k * ncol];
-    xk.x = mul_rn(sub_rn(xk.x, mul_rn(ak, xp.x)), m);
-    xk.y = mul_rn(sub_rn(xk.y, mul_rn(ak, xp.y)), m);
-    x[(long long)k * ncol] = xk;
-    xp = xk;
+    double xkx, xky;
+    to_d(x[(long long)k * ncol], xkx, xky);
+    xkx = mul_rn(sub_rn(xkx, mul_rn(ak, xpx)), m);
+    xky = mul_rn(sub_rn(xky, mul_rn(ak, xpy)), m);
+    // keep the FP64 forward-sweep values for the back substitution
+    x[(long long)k * ncol] = from_d<C>(xkx, xky);
+    xpx = xkx;
+    xpy = xky;
   }
+  // back substitution from the last value, reading the stored sweep values
   for (int k = nz - 2; k >= 0; --k) {
     const double sk = scr[(long long)k * ncol];
-    double2 xk = x[(long long)k * ncol];
-    xk.x = sub_rn(xk.x, mul_rn(sk, xp.x));
-    xk.y = sub_rn(xk.y, mul_rn(sk, xp.y));
-    x[(long long)k * ncol] = xk;
-    xp = xk;
+    double xkx, xky;
+    to_d(x[(long long)k * ncol], xkx, xky);
+    xkx = sub_rn(xkx, mul_rn(sk, xpx));
+    xky = sub_rn(xky, mul_rn(sk, xpy));
+    x[(long long)k * ncol] = from_d<C>(xkx, xky);
+    xpx = xkx;
+    xpy = xky;
   }
 }
 
-// ---- inverse x-FFT -> pressure ---------------------------------------------
+// ---- inverse x-FFT -> pressure (ACC: add to the current pressure) ----------
+template <class C, bool ACC>
 __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC) {
-  extern __shared__ double2 sbuf[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* in = reinterpret_cast<C*>(smraw);
   const int N = (int)(g.n0 - 2 * g.gw);
   const int nz = (int)(g.n2 - 2 * g.gw);
   const int jl = blockIdx.x;
   const int k0 = blockIdx.y * KC;
   const int kc = min(KC, nz - k0);
   const bool p2 = is_pow2(N);
-  double2* in = sbuf;
+  const C* spec = reinterpret_cast<const C*>(a.spec);
   const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
   for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
     const int il = e % N;
     const int kl = e / N;
-    in[kl * N + slot(il, N, a.log0)] = a.spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il];
+    in[kl * N + slot(il, N, a.log0)] = spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il];
   }
   __syncthreads();
-  double2* res = in;
+  C* res = in;
   if (p2) {
-    fft_pow2_lines(in, kc, N, a.log0, a.twx, true);
+    fft_pow2_lines<C>(in, kc, N, a.log0, twx_of<C>(a), true);
   } else {
     res = in + N * KC;
-    dft_lines(in, res, kc, N, a.twx, true);
+    dft_lines<C>(in, res, kc, N, twx_of<C>(a), true);
   }
   const double sc = 1.0 / (double)N;
   const long long j = g.gw + jl;
@@ -386,7 +449,9 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
     const int il = e / KC;
     if (kl >= kc) continue;
     const long long ijk = (g.gw + il) * g.is + j * g.js + g.gw + k0 + kl;
-    a.p[ijk] = res[kl * N + il].x * sc;
+    const double val = (double)res[kl * N + il].x * sc;
+    if (ACC) a.p[ijk] += val;
+    else a.p[ijk] = val;
   }
 }
 
@@ -440,8 +505,8 @@ int stream_blocks(long long work) {
 
 bool pow2(long long n) { return (n & (n - 1)) == 0; }
 
-size_t fft_smem(long long N, int lines) {
-  return (size_t)(pow2(N) ? 1 : 2) * (size_t)N * lines * sizeof(double2);
+size_t fft_smem(long long N, int lines, size_t elem) {
+  return (size_t)(pow2(N) ? 1 : 2) * (size_t)N * lines * elem;
 }
 
 int lines_for(long long N) {
@@ -490,13 +555,59 @@ extern "C" int pb_pressure_init(const pb_dims* dims, void* workspace, long long 
                            cudaMemcpyHostToDevice));
     PB_CUDA_TRY(cudaMemcpy(base + (dim == 0 ? L.twx : L.twy), tw.data(), n * sizeof(double2),
                            cudaMemcpyHostToDevice));
+    std::vector<float2> twf(n);
+    for (long ii = 0; ii < n; ++ii) twf[ii] = make_float2((float)tw[ii].x, (float)tw[ii].y);
+    PB_CUDA_TRY(cudaMemcpy(base + (dim == 0 ? L.twxf : L.twyf), twf.data(), n * sizeof(float2),
+                           cudaMemcpyHostToDevice));
   }
+  return PB_OK;
+}
+
+template <class C>
+static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t st) {
+  const long long Nx = g.n0 - 2 * g.gw, Ny = g.n1 - 2 * g.gw, nz = g.n2 - 2 * g.gw;
+  const int KC = lines_for(Nx);
+  const size_t smx = fft_smem(Nx, KC, sizeof(C));
+  const int IC = lines_for(Ny);
+  const size_t smy = fft_smem(Ny, IC, sizeof(C));
+  if (smx > 48 * 1024) {
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+  }
+  if (smy > 48 * 1024)
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+  const dim3 gx((unsigned)Ny, ceil_div(nz, KC));
+  const dim3 gy(ceil_div(Nx, IC), (unsigned)nz);
+  if (resid)
+    fft_x_fwd<C, true><<<gx, kFftThreads, smx, st>>>(g, a, KC);
+  else
+    fft_x_fwd<C, false><<<gx, kFftThreads, smx, st>>>(g, a, KC);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  fft_y<C><<<gy, kFftThreads, smy, st>>>(g, a, IC, false);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  tdma_kernel<C><<<ceil_div(Nx * Ny, 256), 256, 0, st>>>(g, a);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  fft_y<C><<<gy, kFftThreads, smy, st>>>(g, a, IC, true);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  if (acc)
+    fft_x_inv<C, true><<<gx, kFftThreads, smx, st>>>(g, a, KC);
+  else
+    fft_x_inv<C, false><<<gx, kFftThreads, smx, st>>>(g, a, KC);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
   return PB_OK;
 }
 
 static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const double* rho0_half,
                                const double* alpha0, const double* alpha0_half, double* u, double* v, double* w,
-                               double* divergence, double* dynamic_pressure, char* base, cudaStream_t st) {
+                               double* divergence, double* dynamic_pressure, char* base, int precision,
+                               int refine_sweeps, cudaStream_t st) {
   const Geo g = make_geo(dims);
   const PLayout L = playout(dims);
   PArgs a;
@@ -513,9 +624,11 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
   a.mean = reinterpret_cast<double*>(base + L.mean);
   a.twx = reinterpret_cast<const double2*>(base + L.twx);
   a.twy = reinterpret_cast<const double2*>(base + L.twy);
+  a.twxf = reinterpret_cast<const float2*>(base + L.twxf);
+  a.twyf = reinterpret_cast<const float2*>(base + L.twyf);
   a.kx2 = reinterpret_cast<const double*>(base + L.kx2);
   a.ky2 = reinterpret_cast<const double*>(base + L.ky2);
-  a.spec = reinterpret_cast<double2*>(base + L.spec);
+  a.spec = base + L.spec;
   a.scr = reinterpret_cast<double*>(base + L.scr);
   const long long Nx = dims->n[0], Ny = dims->n[1], nz = dims->n[2];
   a.log0 = ilog2_exact(Nx);
@@ -534,31 +647,21 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
   }
   PB_LAUNCH_CHECK();
 
-  const int KC = lines_for(Nx);
-  const size_t smx = fft_smem(Nx, KC);
-  if (smx > 48 * 1024) {
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+  int rc;
+  if (precision == PB_FP64) {
+    if ((rc = fft_solve<double2>(g, a, false, false, st))) return rc;
+  } else {
+    // precision form: FP32 FFTs, FP64 tridiagonal solve, then refinement
+    // sweeps p += solve(div - A p) on the FP64 residual
+    if ((rc = fft_solve<float2>(g, a, false, false, st))) return rc;
+    for (int s = 0; s < refine_sweeps; ++s) {
+      if (nghost > 0) {
+        ghost_sym<<<stream_blocks(nghost), 256, 0, st>>>(g, dynamic_pressure, nghost);
+        pb_note_launch();
+      }
+      if ((rc = fft_solve<float2>(g, a, true, true, st))) return rc;
+    }
   }
-  fft_x_fwd<<<dim3((unsigned)Ny, ceil_div(nz, KC)), kFftThreads, smx, st>>>(g, a, KC);
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
-  const int IC = lines_for(Ny);
-  const size_t smy = fft_smem(Ny, IC);
-  if (smy > 48 * 1024)
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
-  fft_y<<<dim3(ceil_div(Nx, IC), (unsigned)nz), kFftThreads, smy, st>>>(g, a, IC, false);
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
-  tdma_kernel<<<ceil_div(Nx * Ny, 256), 256, 0, st>>>(g, a);
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
-  fft_y<<<dim3(ceil_div(Nx, IC), (unsigned)nz), kFftThreads, smy, st>>>(g, a, IC, true);
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
-  fft_x_inv<<<dim3((unsigned)Ny, ceil_div(nz, KC)), kFftThreads, smx, st>>>(g, a, KC);
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
   if (nghost > 0) {
     ghost_sym<<<stream_blocks(nghost), 256, 0, st>>>(g, dynamic_pressure, nghost);
     pb_note_launch();
@@ -572,17 +675,18 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
 extern "C" int pb_pressure_solve(const pb_dims* dims, const double* rho0, const double* rho0_half,
                                  const double* alpha0, const double* alpha0_half, double* u, double* v, double* w,
                                  double* divergence, double* dynamic_pressure, void* workspace,
-                                 long long workspace_bytes, int precision, void* stream) {
+                                 long long workspace_bytes, int precision, int refine_sweeps, void* stream) {
   int rc = pb_check_dims(dims);
   if (rc) return rc;
   if (!rho0 || !rho0_half || !alpha0 || !alpha0_half || !u || !v || !w || !divergence || !dynamic_pressure)
     return PB_ERR_ARG;
-  if (precision != PB_FP64) return PB_ERR_UNSUPPORTED;
+  if (precision != PB_FP64 && precision != PB_FP32) return PB_ERR_ARG;
+  if (refine_sweeps < 0 || refine_sweeps > 8) return PB_ERR_ARG;
   const PLayout L = playout(dims);
   if (!workspace || workspace_bytes < L.total) return PB_ERR_WORKSPACE;
   if (reinterpret_cast<uintptr_t>(workspace) & 255) return PB_ERR_WORKSPACE;
   if ((!pow2(dims->n[0]) && dims->n[0] > 1024) || (!pow2(dims->n[1]) && dims->n[1] > 1024)) return PB_ERR_UNSUPPORTED;
   if (dims->n[0] > 8192 || dims->n[1] > 8192) return PB_ERR_UNSUPPORTED;
   return pressure_solve_impl(dims, rho0, rho0_half, alpha0, alpha0_half, u, v, w, divergence, dynamic_pressure,
-                             static_cast<char*>(workspace), as_stream(stream));
+                             static_cast<char*>(workspace), precision, refine_sweeps, as_stream(stream));
 }

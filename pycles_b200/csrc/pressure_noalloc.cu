@@ -80,5 +80,5 @@ extern "C" int pb_pressure_solve_noalloc(const pb_dims* dims, const double* rho0
     base = slot.addr;
   }
   return pressure_solve_impl(dims, rho0, rho0_half, alpha0, alpha0_half, u, v, w, divergence, dynamic_pressure,
-                             static_cast<char*>(base), as_stream(stream));
+                             static_cast<char*>(base), PB_FP64, 0, as_stream(stream));
 }

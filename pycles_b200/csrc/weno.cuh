@@ -119,24 +119,39 @@ __device__ __forceinline__ double weno5_1div(double phim2, double phim1, double 
   return (n0 * p0 + n1 * p1 + n2 * p2) / (n0 + n1 + n2);
 }
 
+// a*(c0 a + c1 b + c2 c + c3 d) + b*(c4 b + c5 c + c6 d) + c*(c7 c + c8 d) + c9 d d,
+// every product and sum rounded separately, left to right, as the C source
+// of advection_interpolation.h:116-131 evaluates it.
+__device__ __forceinline__ double w7_beta(double a, double b, double c, double d, double c0, double c1, double c2,
+                                          double c3, double c4, double c5, double c6, double c7, double c8,
+                                          double c9) {
+  const double i1 = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(c0, a), __dmul_rn(c1, b)), __dmul_rn(c2, c)),
+                              __dmul_rn(c3, d));
+  const double i2 = __dadd_rn(__dadd_rn(__dmul_rn(c4, b), __dmul_rn(c5, c)), __dmul_rn(c6, d));
+  const double i3 = __dadd_rn(__dmul_rn(c7, c), __dmul_rn(c8, d));
+  const double g4 = __dmul_rn(__dmul_rn(c9, d), d);
+  return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, i1), __dmul_rn(b, i2)), __dmul_rn(c, i3)), g4);
+}
+
 __device__ __forceinline__ double weno7_1div(double phim3, double phim2, double phim1, double phi, double phip1,
                                              double phip2, double phip3) {
   const double p0 = (-1.0 / 4.0) * phim3 + (13.0 / 12.0) * phim2 + (-23.0 / 12.0) * phim1 + (25.0 / 12.0) * phi;
   const double p1 = (1.0 / 12.0) * phim2 + (-5.0 / 12.0) * phim1 + (13.0 / 12.0) * phi + (1.0 / 4.0) * phip1;
   const double p2 = (-1.0 / 12.0) * phim1 + (7.0 / 12.0) * phi + (7.0 / 12.0) * phip1 + (-1.0 / 12.0) * phip2;
   const double p3 = (1.0 / 4.0) * phi + (13.0 / 12.0) * phip1 + (-5.0 / 12.0) * phip2 + (1.0 / 12.0) * phip3;
-  const double beta0 = (phim3 * (547.0 * phim3 - 3882.0 * phim2 + 4642.0 * phim1 - 1854.0 * phi) +
-                        phim2 * (7043.0 * phim2 - 17246.0 * phim1 + 7042.0 * phi) +
-                        phim1 * (11003.0 * phim1 - 9402.0 * phi) + 2107.0 * phi * phi);
-  const double beta1 = (phim2 * (267.0 * phim2 - 1642.0 * phim1 + 1602.0 * phi - 494.0 * phip1) +
-                        phim1 * (2843.0 * phim1 - 5966.0 * phi + 1922.0 * phip1) +
-                        phi * (3443.0 * phi - 2522.0 * phip1) + 547.0 * phip1 * phip1);
-  const double beta2 = (phim1 * (547.0 * phim1 - 2522.0 * phi + 1922.0 * phip1 - 494.0 * phip2) +
-                        phi * (3443.0 * phi - 5966.0 * phip1 + 1602.0 * phip2) +
-                        phip1 * (2843.0 * phip1 - 1642.0 * phip2) + 267.0 * phip2 * phip2);
-  const double beta3 = (phi * (2107.0 * phi - 9402.0 * phip1 + 7042.0 * phip2 - 1854.0 * phip3) +
-                        phip1 * (11003.0 * phip1 - 17246.0 * phip2 + 4642.0 * phip3) +
-                        phip2 * (7043.0 * phip2 - 3882.0 * phip3) + 547.0 * phip3 * phip3);
+  // The WENO7 smoothness indicators are quadratic forms in the stencil
+  // values themselves, whose terms (~1e4 phi^2) cancel down to (dphi)^2: a
+  // contracted FMA moves beta by ~1e-10 relative, which reaches the weights.
+  // They are therefore evaluated with the reference's separately rounded
+  // operations in its order.
+  const double beta0 = w7_beta(phim3, phim2, phim1, phi, 547.0, -3882.0, 4642.0, -1854.0, 7043.0, -17246.0, 7042.0,
+                               11003.0, -9402.0, 2107.0);
+  const double beta1 = w7_beta(phim2, phim1, phi, phip1, 267.0, -1642.0, 1602.0, -494.0, 2843.0, -5966.0, 1922.0,
+                               3443.0, -2522.0, 547.0);
+  const double beta2 = w7_beta(phim1, phi, phip1, phip2, 547.0, -2522.0, 1922.0, -494.0, 3443.0, -5966.0, 1602.0,
+                               2843.0, -1642.0, 267.0);
+  const double beta3 = w7_beta(phi, phip1, phip2, phip3, 2107.0, -9402.0, 7042.0, -1854.0, 11003.0, -17246.0,
+                               4642.0, 7043.0, -3882.0, 547.0);
   const double e0 = beta0 + 1e-10, e1 = beta1 + 1e-10, e2 = beta2 + 1e-10, e3 = beta3 + 1e-10;
   const double q0 = e0 * e0, q1 = e1 * e1, q2 = e2 * e2, q3 = e3 * e3;
   const double q01 = q0 * q1, q23 = q2 * q3;
@@ -147,6 +162,20 @@ __device__ __forceinline__ double weno7_1div(double phim3, double phim2, double 
   return (n0 * p0 + n1 * p1 + n2 * p2 + n3 * p3) / (n0 + n1 + n2 + n3);
 }
 
+// FP32 value type whose division is the fast approximate one (__fdividef,
+// ~2 ulp): the precision form's WENO weights are ratios of smoothness
+// indicators and need no correctly rounded division.
+struct FastF {
+  float v;
+  __device__ __forceinline__ FastF() : v(0.0f) {}
+  __device__ __forceinline__ explicit FastF(float x) : v(x) {}
+  __device__ __forceinline__ explicit FastF(double x) : v((float)x) {}
+};
+__device__ __forceinline__ FastF operator+(FastF a, FastF b) { return FastF(a.v + b.v); }
+__device__ __forceinline__ FastF operator-(FastF a, FastF b) { return FastF(a.v - b.v); }
+__device__ __forceinline__ FastF operator*(FastF a, FastF b) { return FastF(a.v * b.v); }
+__device__ __forceinline__ FastF operator/(FastF a, FastF b) { return FastF(__fdividef(a.v, b.v)); }
+
 // Face value from a stencil held in an array: ORDER 5 reads v[0..4]
 // (upwind-positive: centre v[2]), ORDER 7 reads v[0..6] (centre v[3]).
 // F32 selects the shifted mixed-precision evaluation described above.
@@ -155,18 +184,19 @@ __device__ __forceinline__ double weno_face(double a0, double a1, double a2, dou
                                             double a5 = 0.0, double a6 = 0.0) {
   if constexpr (ORDER == 5) {
     if constexpr (!F32) {
-      return weno5<double>(a0, a1, a2, a3, a4);
+      return weno5_1div(a0, a1, a2, a3, a4);
     } else {
-      const float r = weno5<float>((float)(a0 - a2), (float)(a1 - a2), 0.0f, (float)(a3 - a2),
-                                   (float)(a4 - a2));
+      const float r = weno5<FastF>(FastF((float)(a0 - a2)), FastF((float)(a1 - a2)), FastF(0.0f),
+                                   FastF((float)(a3 - a2)), FastF((float)(a4 - a2))).v;
       return a2 + (double)r;
     }
   } else {
     if constexpr (!F32) {
-      return weno7<double>(a0, a1, a2, a3, a4, a5, a6);
+      return weno7_1div(a0, a1, a2, a3, a4, a5, a6);
     } else {
-      const float r = weno7<float>((float)(a0 - a3), (float)(a1 - a3), (float)(a2 - a3), 0.0f,
-                                   (float)(a4 - a3), (float)(a5 - a3), (float)(a6 - a3));
+      const float r = weno7<FastF>(FastF((float)(a0 - a3)), FastF((float)(a1 - a3)), FastF((float)(a2 - a3)),
+                                   FastF(0.0f), FastF((float)(a4 - a3)), FastF((float)(a5 - a3)),
+                                   FastF((float)(a6 - a3))).v;
       return a3 + (double)r;
     }
   }

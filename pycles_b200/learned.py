@@ -1,0 +1,166 @@
+"""Learned initial guess for the saturation-adjustment secant.
+
+A 3 -> 64 -> 64 -> 1 SiLU MLP maps (p0, s, qt), each normalised to [-1, 1]
+over p0 in [5e4, 1.02e5] Pa, s in [6800, 7100] J/kg/K, qt in [0, 0.025],
+to the temperature that seeds the secant of eos_c in place of its
+linearised second point (Csrc/thermodynamics_sa.h:39).  The secant loop
+itself is unchanged and still runs to the reference tolerance, so the
+network can only change how many iterations a cell takes.
+
+Training pairs come from the plain FP64 secant (pb_eos_sa) on saturated
+(p0, s, qt) samples; training runs on the GPU with this library's own BF16
+tensor-core forward/backward kernels (pb_mlp_grad) and Adam (pb_mlp_adam).
+No counterpart in the reference.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _capi
+
+IN_LO = (5.0e4, 6800.0, 0.0)
+IN_HI = (1.02e5, 7100.0, 0.025)
+H = 64
+OFF = {"w1": (0, H * 3), "b1": (H * 3, H), "w2": (H * 3 + H, H * H), "b2": (H * 3 + H + H * H, H),
+       "w3": (H * 3 + 2 * H + H * H, H), "b3": (H * 3 + 3 * H + H * H, 1)}
+
+
+class SeedMLP:
+    def __init__(self, device="cuda", seed=0, out_mean=285.0, out_scale=15.0):
+        self.device = torch.device(device)
+        g = torch.Generator().manual_seed(seed)
+        p = torch.zeros(_capi.MLP_NPARAM, dtype=torch.float32)
+        # He-style initialisation of the weights, zero biases
+        for name, fan_in in (("w1", 3), ("w2", H), ("w3", H)):
+            o, n = OFF[name]
+            p[o:o + n] = torch.randn(n, generator=g) * math.sqrt(2.0 / fan_in)
+        self.params = p.to(self.device)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.grad = torch.zeros_like(self.params)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        self.step_count = 0
+        self.out_mean = float(out_mean)
+        self.out_scale = float(out_scale)
+        self.w1 = torch.empty(H * 3, dtype=torch.bfloat16, device=self.device)
+        self.w2 = torch.empty(H * H, dtype=torch.bfloat16, device=self.device)
+        self.w3 = torch.empty(H, dtype=torch.bfloat16, device=self.device)
+        self.b1 = torch.empty(H, dtype=torch.float32, device=self.device)
+        self.b2 = torch.empty(H, dtype=torch.float32, device=self.device)
+        self.b3 = torch.empty(1, dtype=torch.float32, device=self.device)
+        self._sync_copies()
+
+    def _sync_copies(self):
+        for name in ("w1", "w2", "w3", "b1", "b2", "b3"):
+            o, n = OFF[name]
+            getattr(self, name).copy_(self.params[o:o + n].to(getattr(self, name).dtype))
+
+    def struct(self) -> _capi.PbMlp:
+        s = _capi.PbMlp()
+        s.w1, s.b1, s.w2, s.b2, s.w3, s.b3 = (getattr(self, n).data_ptr() for n in ("w1", "b1", "w2", "b2", "w3", "b3"))
+        for i in range(3):
+            s.in_lo[i] = IN_LO[i]
+            s.in_hi[i] = IN_HI[i]
+        s.out_mean = self.out_mean
+        s.out_scale = self.out_scale
+        return s
+
+    # ------------------------------------------------------------------
+    @staticmethod
+    def normalise(p0, s, qt):
+        x = torch.stack([2.0 * (a - lo) / (hi - lo) - 1.0 for a, lo, hi in zip((p0, s, qt), IN_LO, IN_HI)], dim=1)
+        return x.to(torch.float32).contiguous()
+
+    def forward(self, p0, s, qt, stream=None):
+        """Seeds for point lists (CUDA float64 tensors) through pb_mlp_forward."""
+        out = torch.empty_like(p0)
+        st = self.struct()
+        _capi.check(_capi.load().pb_mlp_forward(ctypes.byref(st), p0.data_ptr(), s.data_ptr(), qt.data_ptr(),
+                                                out.data_ptr(), p0.numel(), _capi.stream_handle(stream)),
+                    "pb_mlp_forward")
+        return out
+
+    def grad_batch(self, x, target, stream=None):
+        """Zeroes and fills self.grad / self.loss for one batch (pb_mlp_grad)."""
+        self.grad.zero_()
+        self.loss.zero_()
+        st = self.struct()
+        _capi.check(_capi.load().pb_mlp_grad(ctypes.byref(st), x.data_ptr(), target.data_ptr(), x.shape[0],
+                                             self.grad.data_ptr(), self.loss.data_ptr(),
+                                             _capi.stream_handle(stream)), "pb_mlp_grad")
+
+    def adam(self, lr, n, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
+        self.step_count += 1
+        _capi.check(_capi.load().pb_mlp_adam(
+            self.params.data_ptr(), self.m.data_ptr(), self.v.data_ptr(), self.grad.data_ptr(), self.step_count,
+            lr, beta1, beta2, eps, 1.0 / float(n), self.w1.data_ptr(), self.b1.data_ptr(), self.w2.data_ptr(),
+            self.b2.data_ptr(), self.w3.data_ptr(), self.b3.data_ptr(), _capi.stream_handle(stream)), "pb_mlp_adam")
+
+    def train(self, p0, s, qt, T, epochs=3, batch=16384, lr=3e-3, lr_final=1e-4, seed=0, log=None):
+        """Mini-batch Adam on (p0, s, qt) -> T pairs (CUDA float64 tensors)."""
+        x = self.normalise(p0, s, qt)
+        y = ((T - self.out_mean) / self.out_scale).to(torch.float32).contiguous()
+        n = x.shape[0]
+        g = torch.Generator(device=x.device).manual_seed(seed)
+        nb = max(1, n // batch)
+        total = epochs * nb
+        it = 0
+        hist = []
+        for ep in range(epochs):
+            perm = torch.randperm(n, device=x.device, generator=g)
+            for b in range(nb):
+                sel = perm[b * batch:(b + 1) * batch]
+                xb = x[sel].contiguous()
+                yb = y[sel].contiguous()
+                self.grad_batch(xb, yb)
+                lr_t = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * it / max(1, total)))
+                self.adam(lr_t, xb.shape[0])
+                it += 1
+            hist.append(float(self.loss.item()) / float(batch))
+            if log:
+                log(f"epoch {ep}: batch loss {hist[-1]:.3e}")
+        return hist
+
+
+def training_pairs(thermo, p0, s, qt, max_iter=100):
+    """(p0, s, qt) -> (T, secant iterations) from the plain FP64 secant
+    (pb_eos_sa); keeps the saturated points (iterations > 0)."""
+    table = thermo.CC.device_table(p0.device)
+    T = torch.empty_like(p0)
+    its = torch.empty(p0.numel(), dtype=torch.int32, device=p0.device)
+    _capi.check(_capi.load().pb_eos_sa(ctypes.byref(table), p0.data_ptr(), s.data_ptr(), qt.data_ptr(), None,
+                                       T.data_ptr(), None, None, its.data_ptr(), p0.numel(), max_iter,
+                                       _capi.stream_handle(None)), "pb_eos_sa")
+    keep = its > 0
+    return p0[keep], s[keep], qt[keep], T[keep], its[keep]
+
+
+def secant_iterations(thermo, p0, s, qt, seed=None, max_iter=100):
+    """Per-point secant iterations (and T) with or without a seed."""
+    table = thermo.CC.device_table(p0.device)
+    T = torch.empty_like(p0)
+    its = torch.empty(p0.numel(), dtype=torch.int32, device=p0.device)
+    _capi.check(_capi.load().pb_eos_sa(ctypes.byref(table), p0.data_ptr(), s.data_ptr(), qt.data_ptr(),
+                                       seed.data_ptr() if seed is not None else None, T.data_ptr(), None, None,
+                                       its.data_ptr(), p0.numel(), max_iter, _capi.stream_handle(None)),
+                "pb_eos_sa")
+    return T, its
+
+
+def sample_inputs(states, n, rng_seed=0, jitter=(200.0, 3.0, 5e-4), device="cuda"):
+    """n (p0, s, qt) samples drawn from simulation states (list of (p0 per cell,
+    s, qt) flat tensors) with a small seeded jitter, clipped to the input box."""
+    g = torch.Generator(device=device).manual_seed(rng_seed)
+    P = torch.cat([st[0] for st in states])
+    S = torch.cat([st[1] for st in states])
+    Q = torch.cat([st[2] for st in states])
+    idx = torch.randint(0, P.numel(), (n,), device=device, generator=g)
+    out = []
+    for a, j, lo, hi in zip((P, S, Q), jitter, IN_LO, IN_HI):
+        v = a[idx] + j * (2.0 * torch.rand(n, device=device, generator=g, dtype=torch.float64) - 1.0)
+        out.append(v.clamp(lo, hi))
+    return out

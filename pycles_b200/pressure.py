@@ -15,9 +15,12 @@ from . import _capi
 
 
 class PressureSolver:
-    def __init__(self):
+    def __init__(self, namelist=None):
         self.workspace = None
-        self.precision = _capi.PB_FP64
+        gpu = (namelist or {}).get("gpu", {})
+        p = str(gpu.get("precision", "fp64")).lower()
+        self.precision = _capi.PB_FP32 if p in ("fp32", "mixed", "precision") else _capi.PB_FP64
+        self.refine_sweeps = int(gpu.get("pressure_refine_sweeps", 1))
 
     def initialize(self, namelist, Gr, RS, DV, PM=None):
         DV.add_variables("dynamic_pressure", "Pa", "p", "dynamic pressure", "sym", PM)
@@ -43,6 +46,6 @@ class PressureSolver:
             ctypes.byref(Gr.dims), _capi.ptr(RS.d_rho0), _capi.ptr(RS.d_rho0_half), _capi.ptr(RS.d_alpha0),
             _capi.ptr(RS.d_alpha0_half), _capi.ptr(u), _capi.ptr(v), _capi.ptr(w),
             _capi.ptr(DV.field("divergence", Gr)), _capi.ptr(DV.field("dynamic_pressure", Gr)),
-            _capi.ptr(self.workspace), nbytes, self.precision, _capi.stream_handle(stream))
+            _capi.ptr(self.workspace), nbytes, self.precision, self.refine_sweeps, _capi.stream_handle(stream))
         _capi.check(rc, "pb_pressure_solve")
         PV.update_all_bcs(Gr, PM, stream=stream)

@@ -57,7 +57,7 @@ class HotPathSimulation:
         self.Th = ThermodynamicsSA(namelist) if self.moist else ThermodynamicsDry(namelist)
         self.SA = ScalarAdvection(namelist)
         self.MA = MomentumAdvection(namelist)
-        self.Pr = PressureSolver()
+        self.Pr = PressureSolver(namelist)
         self.TS = TimeStepping()
         self.RS = ReferenceState(Gr)
         PV = self.PV

@@ -234,9 +234,16 @@ class ThermodynamicsSA:
         f = DV.field
         if self.iter_stats is None or self.iter_stats.device != PV.values.device:
             self.iter_stats = torch.zeros(2, dtype=torch.int64, device=PV.values.device)
-        seed_fn = getattr(self, "_seeded_update", None)
-        if self.mlp is not None and seed_fn is not None:
-            return seed_fn(Gr, RS, PV, DV, stream)
+        mlp_struct = None
+        seed_scratch = None
+        if self.mlp is not None:
+            # learned path: seeds of the saturated cells first (no counterpart
+            # in the reference), then the unchanged secant
+            if getattr(self, "_seed_scratch", None) is None or self._seed_scratch.numel() != Gr.dims.npg:
+                self._seed_scratch = torch.empty(Gr.dims.npg, dtype=torch.float64, device=PV.values.device)
+            self._mlp_struct = self.mlp.struct()
+            mlp_struct = ctypes.byref(self._mlp_struct)
+            seed_scratch = _capi.ptr(self._seed_scratch)
         table = self.CC.device_table(PV.values.device)
         rc = L.pb_thermo_sa(ctypes.byref(Gr.dims), _capi.ptr(RS.d_p0_half), _capi.ptr(RS.d_alpha0_half),
                             ctypes.byref(table), _capi.ptr(PV.field("s", Gr)), _capi.ptr(PV.field("qt", Gr)),
@@ -244,7 +251,7 @@ class ThermodynamicsSA:
                             _capi.ptr(f("qi", Gr)), _capi.ptr(f("alpha", Gr)), _capi.ptr(f("buoyancy", Gr)),
                             _capi.ptr(f("theta_rho", Gr)), _capi.ptr(f("buoyancy_frequency", Gr)),
                             _capi.ptr(f("thetali", Gr)), _capi.ptr(PV.tendency("w", Gr)),
-                            1 if self.do_qt_clipping else 0, None, _capi.ptr(self.iter_stats),
+                            1 if self.do_qt_clipping else 0, mlp_struct, seed_scratch, _capi.ptr(self.iter_stats),
                             self.max_secant_iter, _capi.stream_handle(stream))
         _capi.check(rc, "pb_thermo_sa")
 

@@ -68,7 +68,7 @@ def test_invalid_arguments_rejected_without_device():
     assert L.pb_scalar_advection(ctypes.byref(Gr3.dims), p, p, p, p, p, p, p, 0, None, None, None, 7, 0,
                                  None) == _capi.PB_ERR_UNSUPPORTED  # WENO7 needs gw >= 4
     assert L.pb_rk3_update(p, p, p, 10, 1.0, 3, None) == _capi.PB_ERR_ARG
-    assert L.pb_pressure_solve(d, p, p, p, p, p, p, p, p, p, None, 0, 0, None) == _capi.PB_ERR_WORKSPACE
+    assert L.pb_pressure_solve(d, p, p, p, p, p, p, p, p, p, None, 0, 0, 0, None) == _capi.PB_ERR_WORKSPACE
     assert L.pb_status_string(3) == b"unsupported configuration"
 
 

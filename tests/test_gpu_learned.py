@@ -1,0 +1,114 @@
+"""The learned secant seed: BF16 tensor-core forward/backward kernels against
+an FP64 CPU MLP (gradient check), training on pairs from the plain secant,
+and what the trained network gains over the method without it.
+
+Tolerances: forward and gradient within 3e-2 relative (BF16 operands of the
+64x64 layer; the CPU reference evaluates the same BF16-rounded weights in
+FP64).  The secant still runs to |dT| < 1e-3 K, so seeded and plain
+temperatures agree to that tolerance.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _cpu_mlp(params, x, out_mean, out_scale, bf16):
+    """FP64 forward/backward of the same network (CPU oracle of the MLP)."""
+    from pycles_b200.learned import H, OFF
+    P = params.astype(np.float64)
+
+    def get(n):
+        o, k = OFF[n]
+        return P[o:o + k]
+
+    def q(a):  # round to BF16 like the kernels' stored weights/operands
+        if not bf16:
+            return a
+        t = torch.tensor(a, dtype=torch.float32).to(torch.bfloat16).to(torch.float64)
+        return t.numpy()
+
+    W1 = q(get("w1")).reshape(H, 3)
+    b1 = get("b1")
+    W2 = q(get("w2")).reshape(H, H)
+    b2 = get("b2")
+    w3 = q(get("w3"))
+    b3 = get("b3")[0]
+    z1 = x @ W1.T + b1
+    h1 = z1 / (1.0 + np.exp(-z1))
+    h1q = q(h1)
+    z2 = h1q @ W2.T + b2
+    h2 = z2 / (1.0 + np.exp(-z2))
+    y = h2 @ w3 + b3
+    return y, (W1, W2, w3, z1, h1q, z2, h2)
+
+
+def _cpu_grad(params, x, t):
+    from pycles_b200.learned import H
+    y, (W1, W2, w3, z1, h1q, z2, h2) = _cpu_mlp(params, x, 0, 1, True)
+    sg = lambda z: (1 / (1 + np.exp(-z))) * (1 + z * (1 - 1 / (1 + np.exp(-z))))
+    dy = y - t
+    gw3 = h2.T @ dy
+    gb3 = dy.sum()
+    dz2 = dy[:, None] * w3[None, :] * sg(z2)
+    gW2 = dz2.T @ h1q
+    gb2 = dz2.sum(0)
+    dz1 = (dz2 @ W2) * sg(z1)
+    gW1 = dz1.T @ x
+    gb1 = dz1.sum(0)
+    return np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gw3, [gb3]])
+
+
+def test_mlp_forward_and_gradient_vs_cpu():
+    from pycles_b200.learned import SeedMLP
+    mlp = SeedMLP(seed=3)
+    rng = np.random.default_rng(0)
+    n = 1000
+    x = rng.uniform(-1, 1, size=(n, 3))
+    t = rng.standard_normal(n) * 0.5
+    xt = torch.tensor(x, dtype=torch.float32, device="cuda")
+    tt = torch.tensor(t, dtype=torch.float32, device="cuda")
+    mlp.grad_batch(xt, tt)
+    g_gpu = mlp.grad.cpu().numpy().astype(np.float64)
+    params = mlp.params.cpu().numpy()
+    g_cpu = _cpu_grad(params, xt.cpu().numpy().astype(np.float64), tt.cpu().numpy().astype(np.float64))
+    rel = np.linalg.norm(g_gpu - g_cpu) / np.linalg.norm(g_cpu)
+    print("gradient rel L2 vs FP64 CPU MLP:", rel)
+    assert rel < 3e-2
+    # forward through pb_mlp_forward on physical inputs
+    from pycles_b200.learned import IN_HI, IN_LO
+    phys = [lo + (x[:, i] + 1) * 0.5 * (hi - lo) for i, (lo, hi) in enumerate(zip(IN_LO, IN_HI))]
+    p0, s, qt = (torch.tensor(a, dtype=torch.float64, device="cuda") for a in phys)
+    y_gpu = mlp.forward(p0, s, qt).cpu().numpy()
+    y_cpu, _ = _cpu_mlp(params, mlp.normalise(p0, s, qt).cpu().numpy().astype(np.float64), 0, 1, True)
+    y_cpu = mlp.out_mean + mlp.out_scale * y_cpu
+    assert np.max(np.abs(y_gpu - y_cpu)) / mlp.out_scale < 3e-2
+
+
+def test_trained_seed_cuts_secant_iterations():
+    from pycles_b200 import learned
+    from pycles_b200.thermodynamics import ThermodynamicsSA
+    th = ThermodynamicsSA({})
+    g = torch.Generator(device="cuda").manual_seed(1)
+    n = 400_000
+    # saturated-range inputs: boundary-layer to cloud-layer pressures, entropies, moisture
+    p0 = 7.0e4 + 3.2e4 * torch.rand(n, device="cuda", dtype=torch.float64, generator=g)
+    s = 6850.0 + 200.0 * torch.rand(n, device="cuda", dtype=torch.float64, generator=g)
+    qt = 0.004 + 0.02 * torch.rand(n, device="cuda", dtype=torch.float64, generator=g)
+    P, S, Q, T, its = learned.training_pairs(th, p0, s, qt)
+    assert P.numel() > 10_000
+    ntr = P.numel() * 9 // 10
+    mlp = learned.SeedMLP(seed=0, out_mean=float(T.mean()), out_scale=float(T.std()) * 2)
+    hist = mlp.train(P[:ntr], S[:ntr], Q[:ntr], T[:ntr], epochs=6, batch=8192)
+    assert hist[-1] < hist[0]
+    # held-out points: iterations with and without the seed, same answer
+    Pt, St, Qt, Tt = P[ntr:], S[ntr:], Q[ntr:], T[ntr:]
+    seed = mlp.forward(Pt, St, Qt)
+    T_plain, it_plain = learned.secant_iterations(th, Pt, St, Qt)
+    T_seed, it_seed = learned.secant_iterations(th, Pt, St, Qt, seed=seed)
+    err = float((seed - Tt).abs().mean())
+    mp, ms = float(it_plain.double().mean()), float(it_seed.double().mean())
+    print(f"seed mean |error| {err:.3e} K; mean secant iterations plain {mp:.3f}, seeded {ms:.3f}")
+    assert ms < mp
+    assert float((T_seed - T_plain).abs().max()) < 2e-3

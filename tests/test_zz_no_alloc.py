@@ -55,7 +55,7 @@ def _solve(Gr, RS, vel, noalloc):
         nbytes = L.pb_pressure_workspace_bytes(ctypes.byref(Gr.dims))
         ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
         _capi.check(L.pb_pressure_init(ctypes.byref(Gr.dims), ws.data_ptr(), nbytes), "pb_pressure_init")
-        rc = L.pb_pressure_solve(*args, ws.data_ptr(), nbytes, 0, stream)
+        rc = L.pb_pressure_solve(*args, ws.data_ptr(), nbytes, 0, 0, stream)
     torch.cuda.synchronize()
     return rc, {n: t.cpu().numpy() for n, t in zip(("u", "v", "w", "div", "p"), (u, v, w, div, p))}
 
