@@ -1,7 +1,7 @@
 """Benchmark of the PyCLES hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config c5_dycoms]
-                    [--precision fp64|fp32] [--impl ours|reference]
+                    [--form both|fp64|fp32] [--impl ours|reference]
 
 A step is one time step (three SSP-RK3 stages) of the hot path --
 thermodynamics, scalar and momentum advection, RK update, ghost fill and the
@@ -169,42 +169,31 @@ def cpu_reference_run(cfg, nsteps, nwarm, backend="ref", cores=None):
 # ---------------------------------------------------------------------------
 # GPU side
 # ---------------------------------------------------------------------------
-def run_ours(args, rank, world, local_rank):
-    import numpy as np
+def _time_steps(sim, steps, local_rank, world):
+    """Device-resident timed region: `steps` time steps with CUDA events around
+    every component call on the launching stream."""
     import torch
     import torch.distributed as dist
 
     from pycles_b200 import _capi
-    from pycles_b200.simulation import CONFIGS, HotPathSimulation, namelist_for
-
-    cfg = dict(CONFIGS[args.config])
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    nl = namelist_for(**cfg, precision=args.precision)
-    sim = HotPathSimulation(nl, device=dev)
-    fields = sim.initialize(seed=rank)
+    dev = sim.device
     stream = torch.cuda.current_stream(dev)
-    sim.run(0)  # ghost fill + first thermodynamics update, as Simulation3d.run
-    _capi.clear_error()
-    for _ in range(args.warmup):
-        sim.step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-
-    # ---- device-resident timed region ---------------------------------------
     comp = ["thermo", "scalar_adv", "momentum_adv", "rk3+bcs", "pressure"]
     ev = []
     clocks = ClockSampler(local_rank)
     clocks.start()
     L = _capi.load()
     n_launch0 = L.pb_launch_count()
+    if sim.moist:
+        sim.Th.iter_stats.zero_()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     t_start.record(stream)
     Gr, PV, DV, RS = sim.Gr, sim.PV, sim.DV, sim.RS
-    for _ in range(args.steps):
+    for _ in range(steps):
         for rk in range(3):
             e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
             e[0].record(stream)
@@ -233,16 +222,104 @@ def run_ours(args, rank, world, local_rank):
     t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_ms = float(t.item())
-    err = _capi.get_error()
+    secant = None
+    if sim.moist:
+        st = sim.Th.iter_stats.cpu().tolist()
+        secant = {"mean_iterations_per_saturated_cell": (st[0] / st[1]) if st[1] else 0.0,
+                  "saturated_cells_per_stage": st[1] / (3 * steps)}
+    return float(t.item()), comp_ms, launches, clock_info, secant
 
+
+def _train_seed(sim, fields, log):
+    """Learned seed for the secant: pairs from the plain FP64 secant on the
+    saturated (p0, s, qt) of this state with a seeded jitter, trained with
+    the library's own tensor-core kernels (outside the timed region)."""
+    import torch
+
+    from pycles_b200 import learned
+    Gr = sim.Gr
+    n2 = Gr.dims.nlg[2]
+    s = torch.as_tensor(fields["s"], device=sim.device)
+    qt = torch.as_tensor(fields["qt"], device=sim.device)
+    p0 = sim.RS.d_p0_half.repeat(Gr.npg // n2)
+    n = 2_000_000
+    P, S, Q = learned.sample_inputs([(p0, s, qt)], n, rng_seed=1, device=sim.device)
+    P, S, Q, T, its = learned.training_pairs(sim.Th, P, S, Q)
+    if P.numel() < 1000:
+        return None
+    mlp = learned.SeedMLP(device=sim.device, seed=0, out_mean=float(T.mean()), out_scale=2.0 * float(T.std()))
+    t0 = time.time()
+    mlp.train(P, S, Q, T, epochs=4, batch=16384)
+    seed = mlp.forward(P[:200000], S[:200000], Q[:200000])
+    _, it_seed = learned.secant_iterations(sim.Th, P[:200000], S[:200000], Q[:200000], seed=seed)
+    info = {"training_pairs": int(P.numel()), "train_seconds": round(time.time() - t0, 1),
+            "seed_mean_abs_error_K": float((seed - T[:200000]).abs().mean()),
+            "pointwise_mean_iterations_plain": float(its[:200000].double().mean()),
+            "pointwise_mean_iterations_seeded": float(it_seed.double().mean())}
+    log(f"learned seed: {info}")
+    return mlp, info
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from pycles_b200 import _capi
+    from pycles_b200.simulation import CONFIGS, HotPathSimulation, namelist_for
+
+    cfg = dict(CONFIGS[args.config])
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    log = (lambda m: print(m, file=sys.stderr)) if rank == 0 else (lambda m: None)
+    forms = ["fp64"] if args.form == "fp64" else (["fp32"] if args.form == "fp32" else ["fp64", "fp32"])
+    results = {}
+    fields = None
+    rs = None
+    headline_sim = None
+    for form in forms:
+        nl = namelist_for(**cfg, precision=form)
+        sim = HotPathSimulation(nl, device=dev)
+        if fields is None:
+            fields = sim.initialize(seed=rank)
+            rs = sim.RS.profiles()
+        else:
+            sim.set_reference_state(rs)
+            sim.load_fields(fields)
+        seed_info = None
+        if form == "fp32" and sim.moist and not args.no_learned:
+            out = _train_seed(sim, fields, log)
+            if out is not None:
+                sim.Th.mlp, seed_info = out
+        sim.run(0)  # ghost fill + first thermodynamics update, as Simulation3d.run
+        _capi.clear_error()
+        for _ in range(args.warmup):
+            sim.step()
+        torch.cuda.synchronize()
+        elapsed_ms, comp_ms, launches, clock_info, secant = _time_steps(sim, args.steps, local_rank, world)
+        npl = sim.Gr.dims.npl
+        results[form] = {
+            "value": world * npl * 3 * args.steps / (elapsed_ms / 1e3),
+            "ms_per_step": elapsed_ms / args.steps,
+            "component_ms_per_step": {c: round(v / args.steps, 4) for c, v in comp_ms.items()},
+            "gpu_launches": launches, "clocks": clock_info, "secant": secant,
+            "device_error_word": _capi.get_error(),
+            "learned_seed": seed_info, "pressure_refine_sweeps": sim.Pr.refine_sweeps if form == "fp32" else None,
+        }
+        log(f"form {form}: {results[form]['ms_per_step']:.2f} ms/step")
+        if form == forms[-1]:
+            headline_sim = sim
+        else:
+            del sim
+            torch.cuda.empty_cache()
+    head = forms[-1]
+    sim = headline_sim
+    PV, Gr = sim.PV, sim.Gr
     npl = Gr.dims.npl
-    ms_per_step = elapsed_ms / args.steps
-    value = world * npl * 3 * args.steps / (elapsed_ms / 1e3)
 
     # ---- end to end through the public API with host buffers ---------------
     e2e = None
     if not args.no_e2e:
+        import torch.distributed as dist
+        stream = torch.cuda.current_stream(dev)
         host = torch.empty(PV.values.numel(), dtype=torch.float64, pin_memory=True)
         host.copy_(PV.values)
         torch.cuda.synchronize()
@@ -262,48 +339,55 @@ def run_ours(args, rank, world, local_rank):
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         nbytes = PV.values.numel() * 8
         e2e = {"value": world * npl * 3 * args.steps / (float(te.item()) / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "form": head, "what": "full prognostic state copied host->device before and device->host "
+                                     "after every step (the reference keeps it in host numpy arrays)"}
         del host
 
     # ---- roofline of the dominant kernel group (advection) -----------------
     peak, peak_kind = _peaks()
+    r = results[head]
     nv = PV.nv
-    adv_ms = (comp_ms["scalar_adv"] + comp_ms["momentum_adv"]) / (args.steps * 3)
+    cm = r["component_ms_per_step"]
+    adv_ms = (cm["scalar_adv"] + cm["momentum_adv"]) / 3.0
     adv_bytes = ADV_BYTES_PER_CELL.get(nv, 24 * nv) * npl
     achieved = adv_bytes / (adv_ms / 1e3) / 1e9
     flops_key = ("c5", 7) if cfg.get("scalar_order", 5) == 7 else (("moist", 5) if nv == 5 else ("dry", 5))
     adv_flops = ADV_FLOPS_PER_CELL[flops_key] * npl
-    traffic = _read_traffic(args.config, args.precision)
+    traffic = _read_traffic(args.config, head)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "advection (scalar + momentum, 6 launches per stage)",
+                "kernel": "advection (scalar + momentum launches of one RK stage)",
                 "algorithmic_bytes_per_cell_stage": ADV_BYTES_PER_CELL.get(nv, 24 * nv),
-                "fp64_flops_per_cell_stage": ADV_FLOPS_PER_CELL[flops_key],
-                "achieved_fp64_tflops": round(adv_flops / (adv_ms / 1e3) / 1e12, 2)}
+                "flops_per_cell_stage": ADV_FLOPS_PER_CELL[flops_key],
+                "achieved_tflops": round(adv_flops / (adv_ms / 1e3) / 1e12, 2),
+                "note": "the advection is FP-pipe bound, not HBM bound: see achieved_tflops"}
 
     out = None
     if rank == 0:
         out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64",
+            "dtype": "f64" if head == "fp64" else "f32 fluxes/FFT, f64 accumulation, TDMA, secant",
             "data": "synthetic (seeded DYCOMS-RF01-like state)" if cfg["case"] == "dycoms" else "synthetic (seeded)",
             "config": {"workload": f"{args.config}: {cfg['nx']}x{cfg['ny']}x{cfg['nz']} cells, "
                                    f"gw={cfg['gw']}, WENO{cfg.get('scalar_order', 5)} scalars / "
                                    f"WENO{cfg.get('momentum_order', 5)} momentum, case={cfg['case']}, "
-                                   f"dt={cfg['dt']}", "form": args.precision,
-                       "cells": npl, "state_bytes": int(PV.values.numel() * 8 * 4),
-                       "l2": "inputs larger than L2 (no flush needed)",
+                                   f"dt={cfg['dt']}",
+                       "form": "fp32+learned" if head == "fp32" else "fp64 plain",
+                       "cells": npl, "l2": "inputs larger than L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
-            "component_ms_per_step": {c: round(v / args.steps, 4) for c, v in comp_ms.items()},
+            "forms": results,
+            "speedup_fp32_learned_vs_fp64_plain": (results["fp32"]["value"] / results["fp64"]["value"]
+                                                   if "fp32" in results and "fp64" in results else None),
+            "component_ms_per_step": r["component_ms_per_step"],
             "roofline": roofline,
             "e2e": e2e,
-            "gpu_launches": launches,
-            "clocks": clock_info,
-            "device_error_word": err,
+            "gpu_launches": r["gpu_launches"],
+            "clocks": r["clocks"],
+            "device_error_word": r["device_error_word"],
         }
-    del fields
     return out, sim
 
 
@@ -329,7 +413,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c5_dycoms")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "fp32"],
+                    help="fp64: plain form; fp32: precision form + learned seed; both: headline fp32")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -177,9 +177,9 @@ int pb_eos_sa(const pb_table* table, const double* p0, const double* s, const do
  * Learned seed (no counterpart in the reference).  BF16 tensor-core
  * (mma.sync m16n8k16, FP32 accumulation) forward and backward passes of the
  * 3 -> 64 -> 64 -> 1 SiLU MLP of pb_mlp.  Packed FP32 parameter vector
- * (PB_MLP_NPARAM = 4417): W1[64][3], b1[64], W2[64][64], b2[64], w3[64], b3.
+ * (PB_MLP_NPARAM = 4481): W1[64][3], b1[64], W2[64][64], b2[64], w3[64], b3.
  * --------------------------------------------------------------------- */
-#define PB_MLP_NPARAM 4417
+#define PB_MLP_NPARAM 4481
 
 /* T_seed[i] = out_mean + out_scale * MLP(normalised p0[i], s[i], qt[i]). */
 int pb_mlp_forward(const pb_mlp* mlp, const double* p0, const double* s, const double* qt,

@@ -42,7 +42,7 @@ class PbMlp(ctypes.Structure):
 PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_UNSUPPORTED, PB_ERR_WORKSPACE = 0, 1, 2, 3, 4
 PB_FP64, PB_FP32 = 0, 1
 ERR_TABLE_RANGE, ERR_SECANT_CAP, ERR_NONFINITE = 0x1, 0x2, 0x4
-MLP_NPARAM = 4417
+MLP_NPARAM = 4481
 
 # name -> (restype, argtypes); every symbol include/pycles_b200.h declares
 _I, _LL, _D, _P = ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p

@@ -47,10 +47,11 @@ def nvcc() -> str:
     return "nvcc"
 
 
-# Translation units and their extra flags.  The thermodynamics are compiled
-# without FMA contraction so that the temperature follows the reference's
-# separately rounded arithmetic (see csrc/crmath.cuh).
-UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"])]
+# Translation units and their extra flags.  The thermodynamics and the FP64
+# plain-form advection are compiled without FMA contraction so that they
+# follow the reference's separately rounded arithmetic (see csrc/crmath.cuh
+# and csrc/advection_f64.cu).
+UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"]), ("advection_f64.cu", ["-fmad=false"])]
 
 
 def _run(cmd):
@@ -64,16 +65,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    objs = []
-    log = []
+    from concurrent.futures import ThreadPoolExecutor
+    objs, cmds = [], []
     for src, extra in UNITS:
         obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
         cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
         cmd.remove("-shared")
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        log.append(_run(cmd))
+        cmds.append(cmd)
         objs.append(obj)
+    with ThreadPoolExecutor(len(cmds)) as ex:
+        log = list(ex.map(_run, cmds))
     tmp = LIB + ".tmp"
     _run([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC"] + objs
          + ["-o", tmp])

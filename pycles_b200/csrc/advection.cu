@@ -1,349 +1,27 @@
-// WENO scalar and momentum advection with flux divergence.
-//
-// Direction-split, one launch per (direction, group): the x and y kernels
-// give each thread one (other-axis, k) column and march along the advection
-// axis, keeping the stencil in a register window and the previous face flux
-// in a register, so every face flux is computed once and each cell's
-// tendency is read-modified-written once per direction.  The z kernel puts
-// k on the lanes; lane L computes the flux of face f = k0-1+L and takes the
-// flux of face f-1 from lane L-1 by shuffle (31 cells per warp).
-//
-// Order of the tendency updates per variable is the reference's: d = 0, 1, 2
-// (ScalarAdvection.pyx:81, MomentumAdvection.pyx:56-60), each
-//   tend -= alpha(k) * (F[f] - F[f-1]) * dxi[d]      (Csrc/flux_divergence.h)
-#include "pb_common.cuh"
-#include "weno.cuh"
+// Advection entry points and the FP32 precision-form instantiations of the
+// kernels in advection_kernels.cuh (the FP64 plain form is instantiated in
+// advection_f64.cu, compiled without FMA contraction).
+#include "advection_kernels.cuh"
+
+namespace pbadv {
+
+cudaError_t scalar_fp32(int order, int ns, const Geo& g, ScalarArgs base, double* const* flux_dir[3],
+                        const double* const vel[3], cudaStream_t st) {
+  return order == 5 ? launch_scalar_ns<5, true>(ns, g, base, flux_dir, vel, st)
+                    : launch_scalar_ns<7, true>(ns, g, base, flux_dir, vel, st);
+}
+
+cudaError_t momentum_fp32(int order, const Geo& g, const MomArgs& a, cudaStream_t st) {
+  return order == 5 ? launch_momentum<5, true>(g, a, st) : launch_momentum<7, true>(g, a, st);
+}
+
+}  // namespace pbadv
 
 namespace {
 
-constexpr int kMaxScalars = 4;
-
-struct ScalarArgs {
-  const double* vel;           // advecting velocity of this direction
-  const double* rho0;
-  const double* rho0_half;
-  const double* alpha0_half;
-  const double* s[kMaxScalars];
-  double* t[kMaxScalars];
-  double* flux[kMaxScalars];   // this direction's flux slab or nullptr
-  int ns;
-};
-
-struct MomArgs {
-  const double* vel[3];        // u, v, w
-  double* tend[3];
-  const double* rho0;
-  const double* rho0_half;
-  const double* alpha0;
-  const double* alpha0_half;
-};
-
-template <int ORDER>
-struct St {
-  static constexpr int R = (ORDER + 1) / 2;  // half-width: faces read f-R+1 .. f+R
-  static constexpr int W = 2 * R;            // register window
-};
-
-// ---------------------------------------------------------------------------
-// scalars, x / y directions
-// ---------------------------------------------------------------------------
-template <int D, int ORDER, bool F32, int NS>
-__global__ void __launch_bounds__(128) scalar_march(Geo g, ScalarArgs a, int chunk) {
-  constexpr int R = St<ORDER>::R;
-  constexpr int W = St<ORDER>::W;
-  const long long k = g.gw + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long o = g.gw + (long long)blockIdx.y * blockDim.y + threadIdx.y;
-  const long long nD = (D == 0) ? g.n0 : g.n1;
-  const long long nO = (D == 0) ? g.n1 : g.n0;
-  if (k >= g.n2 - g.gw || o >= nO - g.gw) return;
-  const long long sD = (D == 0) ? g.is : g.js;
-  const long long sO = (D == 0) ? g.js : g.is;
-  const long long c0 = g.gw + (long long)blockIdx.z * chunk;
-  if (c0 >= nD - g.gw) return;
-  const long long c1 = min(c0 + (long long)chunk, nD - g.gw);
-  const long long base = o * sO + k;
-  const double rho = a.rho0_half[k];
-  const double alpha = a.alpha0_half[k];
-  const double dxi = (D == 0) ? g.dxi0 : g.dxi1;
-
-  double win[NS][W];
-  double fprev[NS];
-  double nxt[NS];
-#pragma unroll
-  for (int q = 0; q < NS; ++q) {
-#pragma unroll
-    for (int m = 0; m < W - 1; ++m) win[q][m] = a.s[q][(c0 - 1 - R + 1 + m) * sD + base];
-    nxt[q] = a.s[q][(c0 - 1 + R) * sD + base];
-    fprev[q] = 0.0;
-  }
-  double vnxt = a.vel[(c0 - 1) * sD + base];
-  for (long long f = c0 - 1; f < c1; ++f) {
-    const long long idx = f * sD + base;
-    const double vel = vnxt;
-    // software prefetch of the next face's loads, consumed one iteration later
-    const bool more = f + 1 < c1;
-    if (more) vnxt = a.vel[idx + sD];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) {
-      win[q][W - 1] = nxt[q];
-      if (more) nxt[q] = a.s[q][(f + 1 + R) * sD + base];
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(win[q][0], win[q][1], win[q][2], win[q][3], win[q][4]);
-        phim = weno_face<5, F32>(win[q][5], win[q][4], win[q][3], win[q][2], win[q][1]);
-      } else {
-        phip = weno_face<7, F32>(win[q][0], win[q][1], win[q][2], win[q][3], win[q][4], win[q][5], win[q][6]);
-        phim = weno_face<7, F32>(win[q][7], win[q][6], win[q][5], win[q][4], win[q][3], win[q][2], win[q][1]);
-      }
-      const double F = upwind_flux(vel, phip, phim, rho);
-      if (f >= c0) a.t[q][idx] -= alpha * (F - fprev[q]) * dxi;
-      if (a.flux[q] != nullptr) a.flux[q][idx] = F;
-      fprev[q] = F;
-#pragma unroll
-      for (int m = 0; m < W - 1; ++m) win[q][m] = win[q][m + 1];
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// scalars, z direction
-// ---------------------------------------------------------------------------
-template <int ORDER, bool F32, int NS>
-__global__ void __launch_bounds__(128) scalar_z(Geo g, ScalarArgs a, long long nwarps) {
-  constexpr int R = St<ORDER>::R;
-  const int lane = threadIdx.x & 31;
-  const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (wid >= nwarps) return;
-  const long long nl1 = g.n1 - 2 * g.gw;
-  const long long nl2 = g.n2 - 2 * g.gw;
-  const long long nseg = (nl2 + 30) / 31;
-  const long long seg = wid % nseg;
-  const long long rest = wid / nseg;
-  const long long j = g.gw + rest % nl1;
-  const long long i = g.gw + rest / nl1;
-  const long long f = g.gw + seg * 31 - 1 + lane;   // face of this lane = cell of this lane
-  const bool valid = f <= g.n2 - g.gw - 1;
-  const long long col = i * g.is + j * g.js;
-  const double dzi = g.dxi2;
-#pragma unroll
-  for (int q = 0; q < NS; ++q) {
-    double F = 0.0;
-    if (valid) {
-      const double* s = a.s[q] + col + f;
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(s[-2], s[-1], s[0], s[1], s[2]);
-        phim = weno_face<5, F32>(s[3], s[2], s[1], s[0], s[-1]);
-      } else {
-        phip = weno_face<7, F32>(s[-3], s[-2], s[-1], s[0], s[1], s[2], s[3]);
-        phim = weno_face<7, F32>(s[4], s[3], s[2], s[1], s[0], s[-1], s[-2]);
-      }
-      F = upwind_flux(a.vel[col + f], phip, phim, a.rho0[f]);
-      if (a.flux[q] != nullptr) a.flux[q][col + f] = F;
-    }
-    const double Fm = __shfl_up_sync(0xffffffffu, F, 1);
-    if (valid && lane > 0) a.t[q][col + f] -= a.alpha0_half[f] * (F - Fm) * dzi;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// momentum, x / y directions (advecting velocity = component D)
-// ---------------------------------------------------------------------------
-template <int D, int ORDER, bool F32>
-__global__ void __launch_bounds__(128) momentum_march(Geo g, MomArgs a, int chunk) {
-  constexpr int R = St<ORDER>::R;
-  constexpr int W = St<ORDER>::W;
-  constexpr int O = 1 - D;  // other horizontal axis
-  const long long k = g.gw + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long o = g.gw + (long long)blockIdx.y * blockDim.y + threadIdx.y;
-  const long long nD = (D == 0) ? g.n0 : g.n1;
-  const long long nO = (D == 0) ? g.n1 : g.n0;
-  if (k >= g.n2 - g.gw || o >= nO - g.gw) return;
-  const long long sD = (D == 0) ? g.is : g.js;
-  const long long sO = (D == 0) ? g.js : g.is;
-  const long long c0 = g.gw + (long long)blockIdx.z * chunk;
-  if (c0 >= nD - g.gw) return;
-  const long long c1 = min(c0 + (long long)chunk, nD - g.gw);
-  const long long base = o * sO + k;
-  const double dxi = (D == 0) ? g.dxi0 : g.dxi1;
-  const double* vD = a.vel[D];
-  // rho/alpha per advected component (momentum_advection_weno.h:145-236,
-  // flux_divergence.h:45-58): horizontal components use the half levels,
-  // w uses the full levels.
-  const double rho_h = a.rho0_half[k];
-  const double rho_f = a.rho0[k];
-  const double al_h = a.alpha0_half[k];
-  const double al_f = a.alpha0[k];
-
-  double win[3][W];
-  double fprev[3];
-  double nxt[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-#pragma unroll
-    for (int m = 0; m < W - 1; ++m) win[c][m] = a.vel[c][(c0 - 1 - R + 1 + m) * sD + base];
-    nxt[c] = a.vel[c][(c0 - 1 + R) * sD + base];
-    fprev[c] = 0.0;
-  }
-  for (long long f = c0 - 1; f < c1; ++f) {
-    const long long idx = f * sD + base;
-    const bool more = f + 1 < c1;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      win[c][W - 1] = nxt[c];
-      if (more) nxt[c] = a.vel[c][(f + 1 + R) * sD + base];
-    }
-    // window position of face f is R-1
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double vel_adv;
-      if (c == D) {
-        if constexpr (ORDER == 5)
-          vel_adv = interp_4<double>(win[D][R - 2], win[D][R - 1], win[D][R], win[D][R + 1]);
-        else
-          vel_adv = interp_6<double>(win[D][R - 3], win[D][R - 2], win[D][R - 1], win[D][R], win[D][R + 1],
-                                     win[D][R + 2]);
-      } else {
-        const long long st = (c == O) ? sO : 1;
-        const double* p = vD + idx;
-        if constexpr (ORDER == 5)
-          vel_adv = interp_4<double>(p[-st], p[0], p[st], p[2 * st]);
-        else
-          vel_adv = interp_6<double>(p[-2 * st], p[-st], p[0], p[st], p[2 * st], p[3 * st]);
-      }
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(win[c][0], win[c][1], win[c][2], win[c][3], win[c][4]);
-        phim = weno_face<5, F32>(win[c][5], win[c][4], win[c][3], win[c][2], win[c][1]);
-      } else {
-        phip = weno_face<7, F32>(win[c][0], win[c][1], win[c][2], win[c][3], win[c][4], win[c][5], win[c][6]);
-        phim = weno_face<7, F32>(win[c][7], win[c][6], win[c][5], win[c][4], win[c][3], win[c][2], win[c][1]);
-      }
-      const double F = upwind_flux(vel_adv, phip, phim, (c == 2) ? rho_f : rho_h);
-      if (f >= c0) a.tend[c][idx] -= ((c == 2) ? al_f : al_h) * (F - fprev[c]) * dxi;
-      fprev[c] = F;
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-#pragma unroll
-      for (int m = 0; m < W - 1; ++m) win[c][m] = win[c][m + 1];
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// momentum, z direction (advecting velocity = w)
-// ---------------------------------------------------------------------------
-template <int ORDER, bool F32>
-__global__ void __launch_bounds__(128) momentum_z(Geo g, MomArgs a, long long nwarps) {
-  const int lane = threadIdx.x & 31;
-  const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (wid >= nwarps) return;
-  const long long nl1 = g.n1 - 2 * g.gw;
-  const long long nl2 = g.n2 - 2 * g.gw;
-  const long long nseg = (nl2 + 30) / 31;
-  const long long seg = wid % nseg;
-  const long long rest = wid / nseg;
-  const long long j = g.gw + rest % nl1;
-  const long long i = g.gw + rest / nl1;
-  const long long f = g.gw + seg * 31 - 1 + lane;
-  const bool valid = f <= g.n2 - g.gw - 1;
-  const long long idx = i * g.is + j * g.js + f;
-  const double dzi = g.dxi2;
-  const double* wv = a.vel[2];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    double F = 0.0;
-    if (valid) {
-      const long long st = (c == 0) ? g.is : ((c == 1) ? g.js : 1);
-      const double* p = wv + idx;
-      double vel_adv;
-      if constexpr (ORDER == 5)
-        vel_adv = interp_4<double>(p[-st], p[0], p[st], p[2 * st]);
-      else
-        vel_adv = interp_6<double>(p[-2 * st], p[-st], p[0], p[st], p[2 * st], p[3 * st]);
-      const double* s = a.vel[c] + idx;
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(s[-2], s[-1], s[0], s[1], s[2]);
-        phim = weno_face<5, F32>(s[3], s[2], s[1], s[0], s[-1]);
-      } else {
-        phip = weno_face<7, F32>(s[-3], s[-2], s[-1], s[0], s[1], s[2], s[3]);
-        phim = weno_face<7, F32>(s[4], s[3], s[2], s[1], s[0], s[-1], s[-2]);
-      }
-      const double rho = (c == 2) ? a.rho0_half[f + 1] : a.rho0[f];
-      F = upwind_flux(vel_adv, phip, phim, rho);
-    }
-    const double Fm = __shfl_up_sync(0xffffffffu, F, 1);
-    if (valid && lane > 0) {
-      const double al = (c == 2) ? a.alpha0[f] : a.alpha0_half[f];
-      a.tend[c][idx] -= al * (F - Fm) * dzi;
-    }
-  }
-}
-
-constexpr int kChunk = 64;  // cells per marching thread along x / y
-
-template <int ORDER, bool F32, int NS>
-cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* flux_dir[3],
-                                const double* const vel[3], cudaStream_t st) {
-  const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
-  dim3 blk(32, 4);
-  {
-    ScalarArgs a = base;
-    a.vel = vel[0];
-    for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[0] ? flux_dir[0][q] : nullptr;
-    dim3 grd(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, kChunk));
-    scalar_march<0, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
-    pb_note_launch();
-  }
-  {
-    ScalarArgs a = base;
-    a.vel = vel[1];
-    for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[1] ? flux_dir[1][q] : nullptr;
-    dim3 grd(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, kChunk));
-    scalar_march<1, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
-    pb_note_launch();
-  }
-  {
-    ScalarArgs a = base;
-    a.vel = vel[2];
-    for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[2] ? flux_dir[2][q] : nullptr;
-    const long long nseg = (nl2 + 30) / 31;
-    const long long nwarps = nl0 * nl1 * nseg;
-    scalar_z<ORDER, F32, NS><<<ceil_div(nwarps, 4), 128, 0, st>>>(g, a, nwarps);
-    pb_note_launch();
-  }
-  return cudaGetLastError();
-}
-
-template <int ORDER, bool F32>
-cudaError_t launch_scalar_ns(int ns, const Geo& g, ScalarArgs base, double* const* flux_dir[3],
-                             const double* const vel[3], cudaStream_t st) {
-  switch (ns) {
-    case 1: return launch_scalar_group<ORDER, F32, 1>(g, base, flux_dir, vel, st);
-    case 2: return launch_scalar_group<ORDER, F32, 2>(g, base, flux_dir, vel, st);
-    case 3: return launch_scalar_group<ORDER, F32, 3>(g, base, flux_dir, vel, st);
-    default: return launch_scalar_group<ORDER, F32, 4>(g, base, flux_dir, vel, st);
-  }
-}
-
-template <int ORDER, bool F32>
-cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
-  const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
-  dim3 blk(32, 4);
-  momentum_march<0, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, kChunk)), blk, 0,
-                                  st>>>(g, a, kChunk);
-  pb_note_launch();
-  momentum_march<1, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, kChunk)), blk, 0,
-                                  st>>>(g, a, kChunk);
-  pb_note_launch();
-  const long long nseg = (nl2 + 30) / 31;
-  const long long nwarps = nl0 * nl1 * nseg;
-  momentum_z<ORDER, F32><<<ceil_div(nwarps, 4), 128, 0, st>>>(g, a, nwarps);
-  pb_note_launch();
-  return cudaGetLastError();
-}
+using pbadv::kMaxScalars;
+using pbadv::MomArgs;
+using pbadv::ScalarArgs;
 
 int check_order(const pb_dims* d, int order) {
   if (order != 5 && order != 7) return PB_ERR_UNSUPPORTED;
@@ -351,7 +29,6 @@ int check_order(const pb_dims* d, int order) {
   if (d->gw < R) return PB_ERR_UNSUPPORTED;
   return PB_OK;
 }
-
 }  // namespace
 
 extern "C" int pb_scalar_advection(const pb_dims* dims, const double* rho0, const double* rho0_half,
@@ -392,12 +69,8 @@ extern "C" int pb_scalar_advection(const pb_dims* dims, const double* rho0, cons
     }
     double* const* fdir[3] = {flux ? fx : nullptr, flux ? fy : nullptr, flux ? fz : nullptr};
     cudaError_t e;
-    if (order == 5)
-      e = precision == PB_FP64 ? launch_scalar_ns<5, false>(ns, g, a, fdir, vel, st)
-                               : launch_scalar_ns<5, true>(ns, g, a, fdir, vel, st);
-    else
-      e = precision == PB_FP64 ? launch_scalar_ns<7, false>(ns, g, a, fdir, vel, st)
-                               : launch_scalar_ns<7, true>(ns, g, a, fdir, vel, st);
+    e = precision == PB_FP64 ? pbadv::scalar_fp64(order, ns, g, a, fdir, vel, st)
+                             : pbadv::scalar_fp32(order, ns, g, a, fdir, vel, st);
     if (e != cudaSuccess) return PB_ERR_CUDA;
   }
   return PB_OK;
@@ -426,9 +99,6 @@ extern "C" int pb_momentum_advection(const pb_dims* dims, const double* rho0, co
   a.alpha0_half = alpha0_half;
   cudaStream_t st = as_stream(stream);
   cudaError_t e;
-  if (order == 5)
-    e = precision == PB_FP64 ? launch_momentum<5, false>(g, a, st) : launch_momentum<5, true>(g, a, st);
-  else
-    e = precision == PB_FP64 ? launch_momentum<7, false>(g, a, st) : launch_momentum<7, true>(g, a, st);
+  e = precision == PB_FP64 ? pbadv::momentum_fp64(order, g, a, st) : pbadv::momentum_fp32(order, g, a, st);
   return e == cudaSuccess ? PB_OK : PB_ERR_CUDA;
 }

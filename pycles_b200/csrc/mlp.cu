@@ -4,6 +4,8 @@
 #include "pb_common.cuh"
 #include "mlp.cuh"
 
+static_assert(mlpk::NPARAM == PB_MLP_NPARAM, "packed parameter count must match the public header");
+
 namespace mlpk {
 
 struct FwdArgs {

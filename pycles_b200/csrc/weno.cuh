@@ -1,8 +1,14 @@
 // WENO and central interpolants, Csrc/advection_interpolation.h.
 //
-// The FP64 forms keep the reference's term order (the compiler may contract
-// a*b+c into FMAs, which moves results by at most a few ulp).  The FP32
-// forms are used by the precision path through weno5_mixed / weno7_mixed:
+// The templates keep the reference's operations and their order.  The FP64
+// plain form instantiates them with double in a translation unit compiled
+// without FMA contraction (advection_f64.cu), which reproduces the
+// reference's roundings exactly: the WENO7 smoothness indicators are
+// quadratic forms whose ~1e4 phi^2 terms cancel down to (dphi)^2, and the
+// face values enter flux differences that cancel further, so any other
+// rounding (a contracted FMA, a rearranged weight formula) moves tendencies
+// of slow velocity components by ~1e-12 relative.  The FP32 forms are used
+// by the precision path through weno_face<ORDER, true>:
 // the stencil is shifted by its centre value in FP64, the WENO arithmetic
 // (candidate polynomials, smoothness indicators, weights) runs in FP32 on
 // the differences, and the centre is added back in FP64.  WENO is exactly
@@ -91,77 +97,6 @@ __device__ __forceinline__ R weno7(R phim3, R phim2, R phim1, R phi, R phip1, R 
   return w0 * p0 + w1 * p1 + w2 * p2 + w3 * p3;
 }
 
-// The same WENO5/WENO7 interpolants with a single division.  The normalised
-// weights w_k = (d_k/q_k) / sum_j (d_j/q_j), q_k = (beta_k + eps)^2, equal
-// n_k / sum_j n_j with n_k = d_k * prod_{j != k} q_j, so one reciprocal of
-// the sum replaces the reference's 4 (WENO5) or 5 (WENO7) divisions.  In
-// FP64 the products stay far from the range limits (q >= 1e-20, and q <= 1e10
-// for any physical jump), and the result differs from the reference's
-// formula by rounding only.  Used by the FP64 form: FP64 division is a
-// multi-instruction sequence, and the advection is FP64-pipe bound.
-__device__ __forceinline__ double weno5_1div(double phim2, double phim1, double phi, double phip1, double phip2) {
-  const double p0 = (1.0 / 3.0) * phim2 - (7.0 / 6.0) * phim1 + (11.0 / 6.0) * phi;
-  const double p1 = (-1.0 / 6.0) * phim1 + (5.0 / 6.0) * phi + (1.0 / 3.0) * phip1;
-  const double p2 = (1.0 / 3.0) * phi + (5.0 / 6.0) * phip1 - (1.0 / 6.0) * phip2;
-  const double a2 = phi - 2.0 * phip1 + phip2;
-  const double b2 = 3.0 * phi - 4.0 * phip1 + phip2;
-  const double a1 = phim1 - 2.0 * phi + phip1;
-  const double b1 = phim1 - phip1;
-  const double a0 = phim2 - 2.0 * phim1 + phi;
-  const double b0 = phim2 - 4.0 * phim1 + 3.0 * phi;
-  const double e0 = (13.0 / 12.0) * a0 * a0 + 0.25 * b0 * b0 + 1e-10;
-  const double e1 = (13.0 / 12.0) * a1 * a1 + 0.25 * b1 * b1 + 1e-10;
-  const double e2 = (13.0 / 12.0) * a2 * a2 + 0.25 * b2 * b2 + 1e-10;
-  const double q0 = e0 * e0, q1 = e1 * e1, q2 = e2 * e2;
-  const double n0 = 0.1 * (q1 * q2);
-  const double n1 = 0.6 * (q0 * q2);
-  const double n2 = 0.3 * (q0 * q1);
-  return (n0 * p0 + n1 * p1 + n2 * p2) / (n0 + n1 + n2);
-}
-
-// a*(c0 a + c1 b + c2 c + c3 d) + b*(c4 b + c5 c + c6 d) + c*(c7 c + c8 d) + c9 d d,
-// every product and sum rounded separately, left to right, as the C source
-// of advection_interpolation.h:116-131 evaluates it.
-__device__ __forceinline__ double w7_beta(double a, double b, double c, double d, double c0, double c1, double c2,
-                                          double c3, double c4, double c5, double c6, double c7, double c8,
-                                          double c9) {
-  const double i1 = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(c0, a), __dmul_rn(c1, b)), __dmul_rn(c2, c)),
-                              __dmul_rn(c3, d));
-  const double i2 = __dadd_rn(__dadd_rn(__dmul_rn(c4, b), __dmul_rn(c5, c)), __dmul_rn(c6, d));
-  const double i3 = __dadd_rn(__dmul_rn(c7, c), __dmul_rn(c8, d));
-  const double g4 = __dmul_rn(__dmul_rn(c9, d), d);
-  return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, i1), __dmul_rn(b, i2)), __dmul_rn(c, i3)), g4);
-}
-
-__device__ __forceinline__ double weno7_1div(double phim3, double phim2, double phim1, double phi, double phip1,
-                                             double phip2, double phip3) {
-  const double p0 = (-1.0 / 4.0) * phim3 + (13.0 / 12.0) * phim2 + (-23.0 / 12.0) * phim1 + (25.0 / 12.0) * phi;
-  const double p1 = (1.0 / 12.0) * phim2 + (-5.0 / 12.0) * phim1 + (13.0 / 12.0) * phi + (1.0 / 4.0) * phip1;
-  const double p2 = (-1.0 / 12.0) * phim1 + (7.0 / 12.0) * phi + (7.0 / 12.0) * phip1 + (-1.0 / 12.0) * phip2;
-  const double p3 = (1.0 / 4.0) * phi + (13.0 / 12.0) * phip1 + (-5.0 / 12.0) * phip2 + (1.0 / 12.0) * phip3;
-  // The WENO7 smoothness indicators are quadratic forms in the stencil
-  // values themselves, whose terms (~1e4 phi^2) cancel down to (dphi)^2: a
-  // contracted FMA moves beta by ~1e-10 relative, which reaches the weights.
-  // They are therefore evaluated with the reference's separately rounded
-  // operations in its order.
-  const double beta0 = w7_beta(phim3, phim2, phim1, phi, 547.0, -3882.0, 4642.0, -1854.0, 7043.0, -17246.0, 7042.0,
-                               11003.0, -9402.0, 2107.0);
-  const double beta1 = w7_beta(phim2, phim1, phi, phip1, 267.0, -1642.0, 1602.0, -494.0, 2843.0, -5966.0, 1922.0,
-                               3443.0, -2522.0, 547.0);
-  const double beta2 = w7_beta(phim1, phi, phip1, phip2, 547.0, -2522.0, 1922.0, -494.0, 3443.0, -5966.0, 1602.0,
-                               2843.0, -1642.0, 267.0);
-  const double beta3 = w7_beta(phi, phip1, phip2, phip3, 2107.0, -9402.0, 7042.0, -1854.0, 11003.0, -17246.0,
-                               4642.0, 7043.0, -3882.0, 547.0);
-  const double e0 = beta0 + 1e-10, e1 = beta1 + 1e-10, e2 = beta2 + 1e-10, e3 = beta3 + 1e-10;
-  const double q0 = e0 * e0, q1 = e1 * e1, q2 = e2 * e2, q3 = e3 * e3;
-  const double q01 = q0 * q1, q23 = q2 * q3;
-  const double n0 = (1.0 / 35.0) * (q1 * q23);
-  const double n1 = (12.0 / 35.0) * (q0 * q23);
-  const double n2 = (18.0 / 35.0) * (q3 * q01);
-  const double n3 = (4.0 / 35.0) * (q2 * q01);
-  return (n0 * p0 + n1 * p1 + n2 * p2 + n3 * p3) / (n0 + n1 + n2 + n3);
-}
-
 // FP32 value type whose division is the fast approximate one (__fdividef,
 // ~2 ulp): the precision form's WENO weights are ratios of smoothness
 // indicators and need no correctly rounded division.
@@ -184,7 +119,7 @@ __device__ __forceinline__ double weno_face(double a0, double a1, double a2, dou
                                             double a5 = 0.0, double a6 = 0.0) {
   if constexpr (ORDER == 5) {
     if constexpr (!F32) {
-      return weno5_1div(a0, a1, a2, a3, a4);
+      return weno5<double>(a0, a1, a2, a3, a4);
     } else {
       const float r = weno5<FastF>(FastF((float)(a0 - a2)), FastF((float)(a1 - a2)), FastF(0.0f),
                                    FastF((float)(a3 - a2)), FastF((float)(a4 - a2))).v;
@@ -192,7 +127,7 @@ __device__ __forceinline__ double weno_face(double a0, double a1, double a2, dou
     }
   } else {
     if constexpr (!F32) {
-      return weno7_1div(a0, a1, a2, a3, a4, a5, a6);
+      return weno7<double>(a0, a1, a2, a3, a4, a5, a6);
     } else {
       const float r = weno7<FastF>(FastF((float)(a0 - a3)), FastF((float)(a1 - a3)), FastF((float)(a2 - a3)),
                                    FastF(0.0f), FastF((float)(a4 - a3)), FastF((float)(a5 - a3)),

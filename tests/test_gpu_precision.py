@@ -4,8 +4,9 @@ solves and FP64-residual iterative refinement) against the FP64 oracle.
 
 Tolerances (relative L2):
   * advection tendencies: 1e-5 (FP32 weights and candidate polynomials)
-  * pressure without refinement: 1e-5; each refinement sweep must shrink the
-    difference to the FP64 solve by >= 1e4, two sweeps reach 1e-11
+  * pressure without refinement: 1e-5; with the per-level horizontal mean
+    (the mode the solver projects out) removed, one refinement sweep shrinks
+    the difference to the FP64 solve by >= 1e4 and two reach 1e-12
   * prognostic fields after 5 steps of the whole hot path: 1e-6 (the north
     star's budget is 1e-5 after 1000 steps)
 """
@@ -43,24 +44,44 @@ def test_fp32_advection_tendencies():
         assert rel_l2(gt[n], o.tend(n)) < 1e-5, n
 
 
+def _levels_demeaned(p, d):
+    """Interior of a ghosted field with its horizontal mean removed per level."""
+    P = p.reshape(d.shape)[d.interior()]
+    return P - P.mean(axis=(0, 1), keepdims=True)
+
+
 def test_fp32_pressure_refinement_converges():
+    """Refinement computes the residual div - A p in FP64 and solves for the
+    correction with the FP32 transforms.  The solver projects out the (0,0)
+    horizontal mode (the reference zeroes it), so refinement cannot correct
+    the per-level horizontal mean that the first FP32 inverse transform leaves
+    in p (~1e-8 relative); that mean has no horizontal gradient and its
+    vertical part only reaches the horizontal mean of w, which the next
+    solve's remove_mean_u3 removes.  Everything else must converge to the FP64
+    solution."""
+    from helpers import oracle_dims
     nl, rs, f = host_case(**MOIST)
     f = _stir(f)
     o = oracle_sim(nl, rs, f)
     o.update_all_bcs()
     o.pr_update()
-    errs = []
+    d = oracle_dims(nl)
+    ref = o.dv["dynamic_pressure"]
+    ref_dm = _levels_demeaned(ref, d)
+    raw, demeaned = [], []
     for sweeps in (0, 1, 2):
         g = gpu_sim(nl, rs, f, precision="fp32")
         g.Pr.refine_sweeps = sweeps
         g.PV.Update_all_bcs(g.Gr)
         g.Pr.update(g.Gr, g.RS, g.DV, g.PV)
-        gd = gpu_dv(g)
-        errs.append(rel_l2(gd["dynamic_pressure"], o.dv["dynamic_pressure"]))
-    print("pressure rel L2 vs FP64 by refinement sweeps:", errs)
-    assert errs[0] < 1e-5
-    assert errs[1] < errs[0] * 1e-4
-    assert errs[2] < 1e-11
+        p = gpu_dv(g)["dynamic_pressure"]
+        raw.append(rel_l2(p, ref))
+        demeaned.append(np.linalg.norm(_levels_demeaned(p, d) - ref_dm) / np.linalg.norm(ref_dm))
+    print("pressure vs FP64 by refinement sweeps: raw", raw, "level means removed", demeaned)
+    assert demeaned[0] < 1e-5
+    assert demeaned[1] < demeaned[0] * 1e-4
+    assert demeaned[2] < 1e-12
+    assert max(raw) < 1e-5 and raw[2] < 1e-7
 
 
 def test_fp32_form_five_steps():
