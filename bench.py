@@ -169,6 +169,18 @@ def cpu_reference_run(cfg, nsteps, nwarm, backend="ref", cores=None):
 # ---------------------------------------------------------------------------
 # GPU side
 # ---------------------------------------------------------------------------
+def max_over_ranks(ms: float, device, world: int) -> float:
+    """The job's time: the slowest rank's device-timed region (the ranks are
+    independent replicas; this is their only collective)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _time_steps(sim, steps, local_rank, world):
     """Device-resident timed region: `steps` time steps with CUDA events around
     every component call on the launching stream."""
@@ -219,15 +231,13 @@ def _time_steps(sim, steps, local_rank, world):
     for e in ev:
         for i, c in enumerate(comp):
             comp_ms[c] += e[i].elapsed_time(e[i + 1])
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms = max_over_ranks(elapsed_ms, dev, world)
     secant = None
     if sim.moist:
         st = sim.Th.iter_stats.cpu().tolist()
         secant = {"mean_iterations_per_saturated_cell": (st[0] / st[1]) if st[1] else 0.0,
                   "saturated_cells_per_stage": st[1] / (3 * steps)}
-    return float(t.item()), comp_ms, launches, clock_info, secant
+    return elapsed_ms, comp_ms, launches, clock_info, secant
 
 
 def _train_seed(sim, fields, log):
@@ -334,11 +344,9 @@ def run_ours(args, rank, world, local_rank):
             host.copy_(PV.values, non_blocking=True)
         b.record(stream)
         torch.cuda.synchronize()
-        te = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te_ms = max_over_ranks(a.elapsed_time(b), dev, world)
         nbytes = PV.values.numel() * 8
-        e2e = {"value": world * npl * 3 * args.steps / (float(te.item()) / 1e3), "unit": UNIT,
+        e2e = {"value": world * npl * 3 * args.steps / (te_ms / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "form": head, "what": "full prognostic state copied host->device before and device->host "
                                      "after every step (the reference keeps it in host numpy arrays)"}
@@ -420,6 +428,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cores", type=int, default=None)
+    ap.add_argument("--grid", default=None, metavar="NXxNYxNZ",
+                    help="override the configuration's cell counts (orders, gw, case and spacing kept), "
+                         "e.g. a reduced case for profiler captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -428,6 +439,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
     from pycles_b200.simulation import CONFIGS
+    if args.grid:
+        nx, ny, nz = (int(t) for t in args.grid.lower().split("x"))
+        CONFIGS[args.config] = dict(CONFIGS[args.config], nx=nx, ny=ny, nz=nz)
     cfg = dict(CONFIGS[args.config])
 
     if args.impl == "reference":
