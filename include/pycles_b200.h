@@ -75,7 +75,8 @@ typedef struct pb_table {
 /*
  * Learned saturation-adjustment seed: a 3->64->64->1 SiLU MLP with BF16
  * weights (device pointers), inputs (p0, s, qt) mapped affinely to [-1,1]
- * by in_lo/in_hi, output T = out_mean + out_scale * y.
+ * by in_lo/in_hi; the seed is T = T_1 + out_mean + out_scale * y with T_1
+ * the secant's first point (the network learns the correction to it).
  * Weight layouts: w1 [64][3], w2 [64][64], w3 [64] (row = output unit),
  * biases FP32.
  */
@@ -140,38 +141,47 @@ int pb_momentum_advection(const pb_dims* dims, const double* rho0, const double*
  * (:98-132, adds to w_tend), bvf_sa (:134-182), thetali_update (:185-211).
  * Latent heat: latent_heat_variable, lambda = 1 (Microphysics.pxd:65-75).
  *   mlp (nullable)        : learned seed for the secant's second point
- *                           (no counterpart in the reference); the seeds of
- *                           the saturated cells are evaluated first into
- *                           seed_scratch (npg doubles, required with mlp).
+ *                           (no counterpart in the reference; precision
+ *                           PB_FP32 only): evaluated inside the kernel for
+ *                           the saturated cells, T_2 = T_1 + out_mean +
+ *                           out_scale * MLP(p0, s, qt), T_1 the secant's
+ *                           first point (:22-24).
  *   secant_iters (nullable): device long long[2]; receives
  *                           {sum of secant iterations, saturated cells}.
  *   max_iter              : secant iteration cap (the reference has none);
  *                           reaching it sets PB_ERR_SECANT_CAP in the error word.
+ *   precision             : PB_FP64 (plain form: correctly rounded exp/log,
+ *                           no FMA contraction, the reference's roundings) or
+ *                           PB_FP32 (precision form: FP64 arithmetic with
+ *                           CUDA's exp/log and FMA, optional learned seed).
  */
 int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const double* alpha0_half,
                  const pb_table* table, const double* s, double* qt, double* T, double* qv,
                  double* ql, double* qi, double* alpha, double* buoyancy, double* theta_rho,
                  double* bvf, double* thetali, double* w_tend, int clip_qt, const pb_mlp* mlp,
-                 double* seed_scratch, long long* secant_iters, int max_iter, void* stream);
+                 long long* secant_iters, int max_iter, int precision, void* stream);
 
 /*
  * ThermodynamicsDry.update (ThermodynamicsDry.pyx:105-120): eos_update
  * (Csrc/thermodynamics_dry.h:12-37), buoyancy_update (:39-73, adds to
  * w_tend), bvf_dry (:75-110).  pd is RS.p0_half as the reference passes it.
+ * precision as for pb_thermo_sa (without a seed).
  */
 int pb_thermo_dry(const pb_dims* dims, const double* p0_half, const double* alpha0_half,
                   const double* s, double* T, double* alpha, double* buoyancy, double* theta,
-                  double* bvf, double* w_tend, void* stream);
+                  double* bvf, double* w_tend, int precision, void* stream);
 
 /*
  * ThermodynamicsSA.eos (ThermodynamicsSA.pyx:169-174) for n points: eos_c
- * (Csrc/thermodynamics_sa.h:17-66) on (p0[i], s[i], qt[i]) -> T[i], ql[i],
- * qi[i] (ql, qi nullable), iters[i] = secant iterations (nullable; 0 for
- * unsaturated points).  seed (nullable) replaces the secant's second point.
+ * (Csrc/thermodynamics_sa.h:17-66, FP64 plain form) on (p0[i], s[i], qt[i])
+ * -> T[i], ql[i], qi[i] (ql, qi nullable), T_first[i] = the secant's first
+ * point T_1 (:22-24; nullable), iters[i] = secant iterations (nullable; 0
+ * for unsaturated points).  seed (nullable) replaces the secant's second
+ * point.
  */
 int pb_eos_sa(const pb_table* table, const double* p0, const double* s, const double* qt,
-              const double* seed, double* T, double* ql, double* qi, int* iters, long long n,
-              int max_iter, void* stream);
+              const double* seed, double* T, double* ql, double* qi, double* T_first, int* iters,
+              long long n, int max_iter, void* stream);
 
 /* ------------------------------------------------------------------------
  * Learned seed (no counterpart in the reference).  BF16 tensor-core
@@ -181,7 +191,11 @@ int pb_eos_sa(const pb_table* table, const double* p0, const double* s, const do
  * --------------------------------------------------------------------- */
 #define PB_MLP_NPARAM 4481
 
-/* T_seed[i] = out_mean + out_scale * MLP(normalised p0[i], s[i], qt[i]). */
+/*
+ * T_seed[i] = T_1 + out_mean + out_scale * MLP(normalised p0[i], s[i], qt[i]),
+ * T_1 the secant's first point (Csrc/thermodynamics_sa.h:22-24, evaluated
+ * with the precision form's arithmetic): the seed pb_thermo_sa uses.
+ */
 int pb_mlp_forward(const pb_mlp* mlp, const double* p0, const double* s, const double* qt,
                    double* T_seed, long long n, void* stream);
 

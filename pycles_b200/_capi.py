@@ -41,6 +41,13 @@ class PbMlp(ctypes.Structure):
 
 PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_UNSUPPORTED, PB_ERR_WORKSPACE = 0, 1, 2, 3, 4
 PB_FP64, PB_FP32 = 0, 1
+
+
+def precision_of(namelist) -> int:
+    """The namelist's gpu.precision: "fp64" (plain form, default) or "fp32"
+    (precision form)."""
+    p = str((namelist or {}).get("gpu", {}).get("precision", "fp64")).lower()
+    return PB_FP32 if p in ("fp32", "mixed", "precision") else PB_FP64
 ERR_TABLE_RANGE, ERR_SECANT_CAP, ERR_NONFINITE = 0x1, 0x2, 0x4
 MLP_NPARAM = 4481
 
@@ -51,13 +58,13 @@ SIGNATURES = {
     "pb_scalar_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _I, _I, _P]),
     "pb_momentum_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P]),
     "pb_thermo_sa": (_I, [_DIMS, _P, _P, ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
-                          _P, _I, ctypes.POINTER(PbMlp), _P, _P, _I, _P]),
-    "pb_eos_sa": (_I, [ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
+                          _P, _I, ctypes.POINTER(PbMlp), _P, _I, _I, _P]),
+    "pb_eos_sa": (_I, [ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
     "pb_mlp_forward": (_I, [ctypes.POINTER(PbMlp), _P, _P, _P, _P, _LL, _P]),
     "pb_mlp_grad": (_I, [ctypes.POINTER(PbMlp), _P, _P, _LL, _P, _P, _P]),
     "pb_mlp_adam": (_I, [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                          ctypes.c_float, _P, _P, _P, _P, _P, _P, _P]),
-    "pb_thermo_dry": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pb_thermo_dry": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "pb_rk3_update": (_I, [_P, _P, _P, _LL, _D, _I, _P]),
     "pb_update_all_bcs": (_I, [_DIMS, _P, _P, _I, _P]),
     "pb_pressure_workspace_bytes": (_LL, [_DIMS]),

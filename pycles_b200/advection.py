@@ -13,8 +13,7 @@ from . import _capi
 
 
 def _precision(namelist):
-    p = str(namelist.get("gpu", {}).get("precision", "fp64")).lower()
-    return _capi.PB_FP32 if p in ("fp32", "mixed", "precision") else _capi.PB_FP64
+    return _capi.precision_of(namelist)
 
 
 class ScalarAdvection:

@@ -51,7 +51,8 @@ def nvcc() -> str:
 # plain-form advection are compiled without FMA contraction so that they
 # follow the reference's separately rounded arithmetic (see csrc/crmath.cuh
 # and csrc/advection_f64.cu).
-UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"]), ("advection_f64.cu", ["-fmad=false"])]
+UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"]), ("advection_f64.cu", ["-fmad=false"]),
+         ("thermo_fast.cu", [])]
 
 
 def _run(cmd):

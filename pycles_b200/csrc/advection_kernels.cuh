@@ -94,15 +94,8 @@ __global__ void __launch_bounds__(128) scalar_march(Geo g, ScalarArgs a, int chu
     for (int q = 0; q < NS; ++q) {
       win[q][W - 1] = nxt[q];
       if (more) nxt[q] = a.s[q][(f + 1 + R) * sD + base];
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(win[q][0], win[q][1], win[q][2], win[q][3], win[q][4]);
-        phim = weno_face<5, F32>(win[q][5], win[q][4], win[q][3], win[q][2], win[q][1]);
-      } else {
-        phip = weno_face<7, F32>(win[q][0], win[q][1], win[q][2], win[q][3], win[q][4], win[q][5], win[q][6]);
-        phim = weno_face<7, F32>(win[q][7], win[q][6], win[q][5], win[q][4], win[q][3], win[q][2], win[q][1]);
-      }
-      const double F = upwind_flux(vel, phip, phim, rho);
+      const double phi = weno_upwind<ORDER, F32>(vel >= 0.0, win[q]);
+      const double F = upwind_flux1(vel, phi, rho);
       if (f >= c0) a.t[q][idx] -= alpha * (F - fprev[q]) * dxi;
       if (a.flux[q] != nullptr) a.flux[q][idx] = F;
       fprev[q] = F;
@@ -136,16 +129,12 @@ __global__ void __launch_bounds__(128) scalar_z(Geo g, ScalarArgs a, long long n
   for (int q = 0; q < NS; ++q) {
     double F = 0.0;
     if (valid) {
-      const double* s = a.s[q] + col + f;
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(s[-2], s[-1], s[0], s[1], s[2]);
-        phim = weno_face<5, F32>(s[3], s[2], s[1], s[0], s[-1]);
-      } else {
-        phip = weno_face<7, F32>(s[-3], s[-2], s[-1], s[0], s[1], s[2], s[3]);
-        phim = weno_face<7, F32>(s[4], s[3], s[2], s[1], s[0], s[-1], s[-2]);
-      }
-      F = upwind_flux(a.vel[col + f], phip, phim, a.rho0[f]);
+      const double* s = a.s[q] + col + f - (R - 1);
+      double v[2 * R];
+#pragma unroll
+      for (int m = 0; m < 2 * R; ++m) v[m] = s[m];
+      const double vel = a.vel[col + f];
+      F = upwind_flux1(vel, weno_upwind<ORDER, F32>(vel >= 0.0, v), a.rho0[f]);
       if (a.flux[q] != nullptr) a.flux[q][col + f] = F;
     }
     const double Fm = __shfl_up_sync(0xffffffffu, F, 1);
@@ -218,15 +207,8 @@ __global__ void __launch_bounds__(128) momentum_march(Geo g, MomArgs a, int chun
         else
           vel_adv = interp_6<double>(p[-2 * st], p[-st], p[0], p[st], p[2 * st], p[3 * st]);
       }
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(win[c][0], win[c][1], win[c][2], win[c][3], win[c][4]);
-        phim = weno_face<5, F32>(win[c][5], win[c][4], win[c][3], win[c][2], win[c][1]);
-      } else {
-        phip = weno_face<7, F32>(win[c][0], win[c][1], win[c][2], win[c][3], win[c][4], win[c][5], win[c][6]);
-        phim = weno_face<7, F32>(win[c][7], win[c][6], win[c][5], win[c][4], win[c][3], win[c][2], win[c][1]);
-      }
-      const double F = upwind_flux(vel_adv, phip, phim, (c == 2) ? rho_f : rho_h);
+      const double phi = weno_upwind<ORDER, F32>(vel_adv >= 0.0, win[c]);
+      const double F = upwind_flux1(vel_adv, phi, (c == 2) ? rho_f : rho_h);
       if (f >= c0) a.tend[c][idx] -= ((c == 2) ? al_f : al_h) * (F - fprev[c]) * dxi;
       fprev[c] = F;
     }
@@ -269,17 +251,13 @@ __global__ void __launch_bounds__(128) momentum_z(Geo g, MomArgs a, long long nw
         vel_adv = interp_4<double>(p[-st], p[0], p[st], p[2 * st]);
       else
         vel_adv = interp_6<double>(p[-2 * st], p[-st], p[0], p[st], p[2 * st], p[3 * st]);
-      const double* s = a.vel[c] + idx;
-      double phip, phim;
-      if constexpr (ORDER == 5) {
-        phip = weno_face<5, F32>(s[-2], s[-1], s[0], s[1], s[2]);
-        phim = weno_face<5, F32>(s[3], s[2], s[1], s[0], s[-1]);
-      } else {
-        phip = weno_face<7, F32>(s[-3], s[-2], s[-1], s[0], s[1], s[2], s[3]);
-        phim = weno_face<7, F32>(s[4], s[3], s[2], s[1], s[0], s[-1], s[-2]);
-      }
+      constexpr int R = St<ORDER>::R;
+      const double* s = a.vel[c] + idx - (R - 1);
+      double v[2 * R];
+#pragma unroll
+      for (int m = 0; m < 2 * R; ++m) v[m] = s[m];
       const double rho = (c == 2) ? a.rho0_half[f + 1] : a.rho0[f];
-      F = upwind_flux(vel_adv, phip, phim, rho);
+      F = upwind_flux1(vel_adv, weno_upwind<ORDER, F32>(vel_adv >= 0.0, v), rho);
     }
     const double Fm = __shfl_up_sync(0xffffffffu, F, 1);
     if (valid && lane > 0) {

@@ -3,6 +3,7 @@
 // fragment layouts.)
 #include "pb_common.cuh"
 #include "mlp.cuh"
+#include "thermo_funcs.cuh"
 
 static_assert(mlpk::NPARAM == PB_MLP_NPARAM, "packed parameter count must match the public header");
 
@@ -26,7 +27,7 @@ struct FwdArgs {
 
 __global__ void __launch_bounds__(128) mlp_forward_kernel(FwdArgs a) {
   __shared__ Smem sm;
-  stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3);
+  stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3, threadIdx.x, blockDim.x);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -49,8 +50,13 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(FwdArgs a) {
     float y0, y1;
     forward_tile(sm, x0, x1, y0, y1, nullptr);
     if (t == 0) {
-      if (r0 < a.n) a.T[r0] = (double)a.out_mean + (double)a.out_scale * (double)y0;
-      if (r1 < a.n) a.T[r1] = (double)a.out_mean + (double)a.out_scale * (double)y1;
+      using thermo_f::FastMath;
+      if (r0 < a.n)
+        a.T[r0] = thermo_f::first_point<FastMath>(a.p0[r0], a.s[r0], a.qt[r0]) + (double)a.out_mean +
+                  (double)a.out_scale * (double)y0;
+      if (r1 < a.n)
+        a.T[r1] = thermo_f::first_point<FastMath>(a.p0[r1], a.s[r1], a.qt[r1]) + (double)a.out_mean +
+                  (double)a.out_scale * (double)y1;
     }
   }
 }
@@ -79,7 +85,7 @@ __global__ void __launch_bounds__(64) mlp_grad_kernel(GradArgs a) {
   __shared__ float dz2_s[kGradWarps][16][H];
   __shared__ float h1_s[kGradWarps][16][H];
   __shared__ float loss_s;
-  stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3);
+  stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3, threadIdx.x, blockDim.x);
   for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) acc[i] = 0.0f;
   if (threadIdx.x == 0) loss_s = 0.0f;
   __syncthreads();

@@ -57,18 +57,19 @@ struct Smem {
   float b3;
 };
 
-// Loads BF16 weights + FP32 biases into shared memory (whole block).
+// Loads BF16 weights + FP32 biases into shared memory (whole block; tid and
+// nthreads are the thread's linear index and the block size).
 __device__ __forceinline__ void stage_weights(Smem& sm, const __nv_bfloat16* w1, const float* b1,
                                               const __nv_bfloat16* w2, const float* b2, const __nv_bfloat16* w3,
-                                              const float* b3) {
-  for (int i = threadIdx.x; i < H * H; i += blockDim.x) sm.w2[i] = w2[i];
-  for (int i = threadIdx.x; i < H * 3; i += blockDim.x) sm.w1[i] = __bfloat162float(w1[i]);
-  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+                                              const float* b3, int tid, int nthreads) {
+  for (int i = tid; i < H * H; i += nthreads) sm.w2[i] = w2[i];
+  for (int i = tid; i < H * 3; i += nthreads) sm.w1[i] = __bfloat162float(w1[i]);
+  for (int i = tid; i < H; i += nthreads) {
     sm.b1[i] = b1[i];
     sm.b2[i] = b2[i];
     sm.w3[i] = __bfloat162float(w3[i]);
   }
-  if (threadIdx.x == 0) sm.b3 = b3[0];
+  if (tid == 0) sm.b3 = b3[0];
 }
 
 // Forward pass of one 16-row tile.  xr0/xr1: the 3 normalised inputs of the

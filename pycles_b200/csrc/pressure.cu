@@ -27,8 +27,8 @@
 
 namespace {
 
-constexpr int kPartials = 296;  // 2 x 148 SMs
-constexpr int kFftThreads = 256;
+constexpr int kPartials = 1184;  // 8 x 148 SMs
+constexpr int kFftThreads = 512;  // stockham_pass: nlines * N <= 16 * kFftThreads
 
 struct PLayout {
   long long partial, mean, twx, twy, twxf, twyf, kx2, ky2, spec, scr, total;
@@ -75,56 +75,162 @@ template <class C> __device__ __forceinline__ C creal(double x);
 template <> __device__ __forceinline__ double2 creal<double2>(double x) { return make_double2(x, 0.0); }
 template <> __device__ __forceinline__ float2 creal<float2>(double x) { return make_float2((float)x, 0.0f); }
 
-// In-place radix-2 DIT over `nlines` lines of length N (power of two) held
-// in shared memory in bit-reversed order.  tw[m] = exp(-2 pi i m / N).
+// ---- line FFTs in shared memory --------------------------------------------
+// A block transforms `nlines` lines of length N held in shared memory.  Line l
+// element x lives at l*line_ld(N) + swz(x): the swizzle (one pad element per
+// 8) and the odd line stride keep the strided accesses of the passes and of
+// the global loads/stores (consecutive threads on consecutive lines) free of
+// bank conflicts.
+__host__ __device__ __forceinline__ int line_ld(int N) { return N + N / 8 + 1; }
+__device__ __forceinline__ int swz(int x) { return x + (x >> 3); }
+
 template <class C>
-__device__ void fft_pow2_lines(C* buf, int nlines, int N, int logN, const C* __restrict__ tw, bool inverse) {
-  const int halfN = N >> 1;
-  for (int s = 1; s <= logN; ++s) {
-    const int half = 1 << (s - 1);
-    const int twstride = N >> s;
-    for (int b = threadIdx.x; b < nlines * halfN; b += blockDim.x) {
-      const int line = b / halfN;
-      const int bb = b - line * halfN;
-      const int group = bb >> (s - 1);
-      const int pos = bb & (half - 1);
-      const int i0 = line * N + group * 2 * half + pos;
-      const int i1 = i0 + half;
-      C w = tw[pos * twstride];
-      if (inverse) w.y = -w.y;
-      const C x0 = buf[i0];
-      const C t = cmul(w, buf[i1]);
-      buf[i0] = cadd(x0, t);
-      buf[i1] = csub(x0, t);
-    }
-    __syncthreads();
-  }
+__device__ __forceinline__ C mul_mi(C a, bool inverse) {  // a * (-i), or a * (+i) for the inverse
+  C r;
+  if (!inverse) { r.x = a.y; r.y = -a.x; } else { r.x = -a.y; r.y = a.x; }
+  return r;
 }
 
-// Direct DFT for lengths that are not powers of two: out = DFT(in).
+// 2-, 4- and 8-point DFTs in registers, y_k = sum_n x_n exp(-+2 pi i n k / R).
 template <class C>
-__device__ void dft_lines(const C* in, C* out, int nlines, int N, const C* __restrict__ tw, bool inverse) {
-  for (int e = threadIdx.x; e < nlines * N; e += blockDim.x) {
-    const int line = e / N;
-    const int m = e - line * N;
-    C acc = czero<C>();
-    const C* x = in + line * N;
-    int idx = 0;
-    for (int n = 0; n < N; ++n) {
-      C w = tw[idx];
-      if (inverse) w.y = -w.y;
-      acc = cadd(acc, cmul(w, x[n]));
-      idx += m;
-      if (idx >= N) idx -= N;
+__device__ __forceinline__ void dft2(C* v) {
+  const C t = v[0];
+  v[0] = cadd(t, v[1]);
+  v[1] = csub(t, v[1]);
+}
+template <class C>
+__device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3, bool inverse) {
+  const C a0 = cadd(x0, x2), a1 = csub(x0, x2);
+  const C b0 = cadd(x1, x3), b1 = mul_mi(csub(x1, x3), inverse);
+  x0 = cadd(a0, b0);
+  x2 = csub(a0, b0);
+  x1 = cadd(a1, b1);
+  x3 = csub(a1, b1);
+}
+template <class C>
+__device__ __forceinline__ void dft8(C* v, bool inverse) {
+  // radix-2 decimation in time over two 4-point DFTs
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4(e0, e1, e2, e3, inverse);
+  dft4(o0, o1, o2, o3, inverse);
+  using R = decltype(o1.x);
+  const R h = (R)0.70710678118654752440;  // 1/sqrt(2)
+  C t1, t3;
+  if (!inverse) {  // W8 = (1-i)/sqrt2, W8^3 = (-1-i)/sqrt2
+    t1.x = (o1.x + o1.y) * h; t1.y = (o1.y - o1.x) * h;
+    t3.x = (o3.y - o3.x) * h; t3.y = -(o3.x + o3.y) * h;
+  } else {         // conjugates
+    t1.x = (o1.x - o1.y) * h; t1.y = (o1.x + o1.y) * h;
+    t3.x = -(o3.x + o3.y) * h; t3.y = (o3.x - o3.y) * h;
+  }
+  const C t2 = mul_mi(o2, inverse);
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, t1); v[5] = csub(e1, t1);
+  v[2] = cadd(e2, t2); v[6] = csub(e2, t2);
+  v[3] = cadd(e3, t3); v[7] = csub(e3, t3);
+}
+
+// One radix-R pass of the Stockham autosort FFT over all lines, in place:
+// every thread reads its items (R values each, stride N/R), twiddles them by
+// exp(-+2 pi i (j mod Ns) r / (Ns R)), transforms, and after a barrier
+// writes them to (j div Ns) Ns R + (j mod Ns) + r Ns.  Input and output are
+// in natural order.  Needs nlines * N <= 16 * blockDim.x.
+template <class C, int R>
+__device__ __forceinline__ void stockham_pass(C* buf, int nlines, int N, int Ns, const C* __restrict__ tw,
+                                              bool inverse) {
+  constexpr int MAXI = 16 / R;
+  const int per_line = N / R;
+  const int total = nlines * per_line;
+  const int ld = line_ld(N);
+  const int twstep = N / (Ns * R);
+  C v[MAXI][R];
+#pragma unroll
+  for (int it = 0; it < MAXI; ++it) {
+    const int b = threadIdx.x + it * blockDim.x;
+    if (b < total) {
+      const int l = b / per_line;
+      const int j = b - l * per_line;
+      const C* line = buf + l * ld;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[it][r] = line[swz(j + r * per_line)];
+      if (Ns > 1) {
+        const int k = j % Ns;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = tw[k * r * twstep];
+          if (inverse) w.y = -w.y;
+          v[it][r] = cmul(v[it][r], w);
+        }
+      }
+      if constexpr (R == 8) dft8(v[it], inverse);
+      else if constexpr (R == 4) dft4(v[it][0], v[it][1], v[it][2], v[it][3], inverse);
+      else dft2(v[it]);
     }
-    out[e] = acc;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < MAXI; ++it) {
+    const int b = threadIdx.x + it * blockDim.x;
+    if (b < total) {
+      const int l = b / per_line;
+      const int j = b - l * per_line;
+      const int k = j % Ns;
+      const int base = (j - k) * R + k;
+      C* line = buf + l * ld;
+#pragma unroll
+      for (int r = 0; r < R; ++r) line[swz(base + r * Ns)] = v[it][r];
+    }
   }
   __syncthreads();
 }
 
-__device__ __forceinline__ int slot(int idx, int N, int logN) {
-  if (!is_pow2(N)) return idx;
-  return logN == 0 ? 0 : (int)(__brev((unsigned)idx) >> (32 - logN));
+// Power-of-two N: radix-8 passes, then one radix-4 or radix-2 pass.
+template <class C>
+__device__ void fft_lines_pow2(C* buf, int nlines, int N, const C* __restrict__ tw, bool inverse) {
+  int Ns = 1;
+  while (Ns * 8 <= N) {
+    stockham_pass<C, 8>(buf, nlines, N, Ns, tw, inverse);
+    Ns *= 8;
+  }
+  if (Ns * 4 == N) stockham_pass<C, 4>(buf, nlines, N, Ns, tw, inverse);
+  else if (Ns * 2 == N) stockham_pass<C, 2>(buf, nlines, N, Ns, tw, inverse);
+}
+
+// Direct DFT for lengths that are not powers of two: out = DFT(in), both in
+// the swizzled line layout.
+template <class C>
+__device__ void dft_lines(const C* in, C* out, int nlines, int N, const C* __restrict__ tw, bool inverse) {
+  const int ld = line_ld(N);
+  for (int e = threadIdx.x; e < nlines * N; e += blockDim.x) {
+    const int line = e / N;
+    const int m = e - line * N;
+    C acc = czero<C>();
+    const C* x = in + line * ld;
+    int idx = 0;
+    for (int n = 0; n < N; ++n) {
+      C w = tw[idx];
+      if (inverse) w.y = -w.y;
+      acc = cadd(acc, cmul(w, x[swz(n)]));
+      idx += m;
+      if (idx >= N) idx -= N;
+    }
+    out[line * ld + swz(m)] = acc;
+  }
+  __syncthreads();
+}
+
+// Transform the lines in `in`; returns where the result is.
+template <class C>
+__device__ __forceinline__ C* fft_lines(C* in, int nlines, int maxlines, int N, const C* __restrict__ tw,
+                                        bool inverse) {
+  if (is_pow2(N)) {
+    fft_lines_pow2<C>(in, nlines, N, tw, inverse);
+    return in;
+  }
+  C* out = in + (size_t)maxlines * line_ld(N);
+  dft_lines<C>(in, out, nlines, N, tw, inverse);
+  return out;
 }
 
 struct PArgs {
@@ -147,7 +253,6 @@ struct PArgs {
   const double* ky2;
   void* spec;     // double2 (plain form) or float2 (precision form) W[k][j][i]
   double* scr;
-  int log0, log1;
 };
 
 template <class C> __device__ __forceinline__ const C* twx_of(const PArgs& a);
@@ -158,17 +263,32 @@ template <> __device__ __forceinline__ const double2* twy_of<double2>(const PArg
 template <> __device__ __forceinline__ const float2* twy_of<float2>(const PArgs& a) { return a.twyf; }
 
 // ---- HorizontalMean (ParallelMPI.pyx:196-241) ------------------------------
+// Block b sums a contiguous chunk of interior columns for every level (one
+// thread per level, four interleaved accumulators for memory-level
+// parallelism); the partition and the order of the sums are fixed, so the
+// mean is deterministic.
 __global__ void hmean_partial(Geo g, const double* __restrict__ w, double* __restrict__ partial) {
   const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw;
   const long long ncol = nl0 * nl1;
+  const long long per = (ncol + gridDim.x - 1) / gridDim.x;
+  const long long c0 = (long long)blockIdx.x * per;
+  const long long c1 = min(ncol, c0 + per);
   for (long long k = threadIdx.x; k < g.n2; k += blockDim.x) {
-    double s = 0.0;
-    for (long long c = blockIdx.x; c < ncol; c += gridDim.x) {
-      const long long i = g.gw + c / nl1;
-      const long long j = g.gw + c % nl1;
-      s += w[i * g.is + j * g.js + k];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    long long c = c0;
+    auto at = [&](long long cc) {
+      const long long i = g.gw + cc / nl1;
+      const long long j = g.gw + cc % nl1;
+      return w[i * g.is + j * g.js + k];
+    };
+    for (; c + 3 < c1; c += 4) {
+      s0 += at(c);
+      s1 += at(c + 1);
+      s2 += at(c + 2);
+      s3 += at(c + 3);
     }
-    partial[(long long)blockIdx.x * g.n2 + k] = s;
+    for (; c < c1; ++c) s0 += at(c);
+    partial[(long long)blockIdx.x * g.n2 + k] = (s0 + s1) + (s2 + s3);
   }
 }
 
@@ -246,7 +366,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
   const int k0 = blockIdx.y * KC;
   const int kc = min(KC, nz - k0);
   const long long j = g.gw + jl;
-  const bool p2 = is_pow2(N);
+  const int ld = line_ld(N);
   const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
   for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
     const int kl = e % KC;
@@ -273,22 +393,16 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
       if (kk > 0) vert -= a.rho0[k - 1] * (pc - p[ijk - 1]);
       d = a.div[ijk] - (lap_h + vert * (dxi2 * dxi2));
     }
-    in[kl * N + slot(il, N, a.log0)] = creal<C>(d);
+    in[kl * ld + swz(il)] = creal<C>(d);
   }
   __syncthreads();
-  C* res = in;
-  if (p2) {
-    fft_pow2_lines<C>(in, kc, N, a.log0, twx_of<C>(a), false);
-  } else {
-    res = in + N * KC;
-    dft_lines<C>(in, res, kc, N, twx_of<C>(a), false);
-  }
+  const C* res = fft_lines<C>(in, kc, KC, N, twx_of<C>(a), false);
   C* spec = reinterpret_cast<C*>(a.spec);
   const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
   for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
     const int il = e % N;
     const int kl = e / N;
-    spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il] = res[kl * N + il];
+    spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il] = res[kl * ld + swz(il)];
   }
 }
 
@@ -302,28 +416,22 @@ __global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, boo
   const int kk = blockIdx.y;
   const int i0 = blockIdx.x * IC;
   const int ic = min(IC, Nx - i0);
-  const bool p2 = is_pow2(N);
+  const int ld = line_ld(N);
   C* plane = reinterpret_cast<C*>(a.spec) + (long long)kk * N * Nx;
   for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
     const int il = e % IC;
     const int jl = e / IC;
     if (il >= ic) continue;
-    in[il * N + slot(jl, N, a.log1)] = plane[(long long)jl * Nx + i0 + il];
+    in[il * ld + swz(jl)] = plane[(long long)jl * Nx + i0 + il];
   }
   __syncthreads();
-  C* res = in;
-  if (p2) {
-    fft_pow2_lines<C>(in, ic, N, a.log1, twy_of<C>(a), inverse);
-  } else {
-    res = in + N * IC;
-    dft_lines<C>(in, res, ic, N, twy_of<C>(a), inverse);
-  }
+  const C* res = fft_lines<C>(in, ic, IC, N, twy_of<C>(a), inverse);
   const double sc = inverse ? 1.0 / (double)N : 1.0;
   for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
     const int il = e % IC;
     const int jl = e / IC;
     if (il >= ic) continue;
-    C r = res[il * N + jl];
+    C r = res[il * ld + swz(jl)];
     if (inverse) {
       r.x *= sc;
       r.y *= sc;
@@ -426,22 +534,16 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
   const int jl = blockIdx.x;
   const int k0 = blockIdx.y * KC;
   const int kc = min(KC, nz - k0);
-  const bool p2 = is_pow2(N);
+  const int ld = line_ld(N);
   const C* spec = reinterpret_cast<const C*>(a.spec);
   const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
   for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
     const int il = e % N;
     const int kl = e / N;
-    in[kl * N + slot(il, N, a.log0)] = spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il];
+    in[kl * ld + swz(il)] = spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il];
   }
   __syncthreads();
-  C* res = in;
-  if (p2) {
-    fft_pow2_lines<C>(in, kc, N, a.log0, twx_of<C>(a), true);
-  } else {
-    res = in + N * KC;
-    dft_lines<C>(in, res, kc, N, twx_of<C>(a), true);
-  }
+  const C* res = fft_lines<C>(in, kc, KC, N, twx_of<C>(a), true);
   const double sc = 1.0 / (double)N;
   const long long j = g.gw + jl;
   for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
@@ -449,7 +551,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
     const int il = e / KC;
     if (kl >= kc) continue;
     const long long ijk = (g.gw + il) * g.is + j * g.js + g.gw + k0 + kl;
-    const double val = (double)res[kl * N + il].x * sc;
+    const double val = (double)res[kl * ld + swz(il)].x * sc;
     if (ACC) a.p[ijk] += val;
     else a.p[ijk] = val;
   }
@@ -489,12 +591,6 @@ __global__ void correction(Geo g, const double* __restrict__ p, double* __restri
   }
 }
 
-int ilog2_exact(long long n) {
-  int l = 0;
-  while ((1LL << l) < n) ++l;
-  return l;
-}
-
 int stream_blocks(long long work) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -506,16 +602,19 @@ int stream_blocks(long long work) {
 bool pow2(long long n) { return (n & (n - 1)) == 0; }
 
 size_t fft_smem(long long N, int lines, size_t elem) {
-  return (size_t)(pow2(N) ? 1 : 2) * (size_t)N * lines * elem;
+  return (size_t)(pow2(N) ? 1 : 2) * (size_t)line_ld((int)N) * lines * elem;
 }
 
-int lines_for(long long N) {
-  // keep one FFT block's shared memory at or below 64 KiB when possible
-  long long per = (pow2(N) ? 1 : 2) * N * 16;
-  int L = (int)(65536 / per);
-  if (L > 8) L = 8;
+// Lines per FFT block: up to 16 (128-byte runs of FP64 levels / FP32
+// complex columns in the global accesses) within ~80 KiB of shared memory,
+// and nlines * N <= 16 * kFftThreads for the Stockham passes.
+int lines_for(long long N, size_t elem) {
+  const long long per = (pow2(N) ? 1 : 2) * (long long)line_ld((int)N) * (long long)elem;
+  long long L = 81920 / per;
+  if (L > 16) L = 16;
+  if (pow2(N) && L * N > 16LL * kFftThreads) L = 16LL * kFftThreads / N;
   if (L < 1) L = 1;
-  return L;
+  return (int)L;
 }
 
 }  // namespace
@@ -566,9 +665,9 @@ extern "C" int pb_pressure_init(const pb_dims* dims, void* workspace, long long 
 template <class C>
 static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t st) {
   const long long Nx = g.n0 - 2 * g.gw, Ny = g.n1 - 2 * g.gw, nz = g.n2 - 2 * g.gw;
-  const int KC = lines_for(Nx);
+  const int KC = lines_for(Nx, sizeof(C));
   const size_t smx = fft_smem(Nx, KC, sizeof(C));
-  const int IC = lines_for(Ny);
+  const int IC = lines_for(Ny, sizeof(C));
   const size_t smy = fft_smem(Ny, IC, sizeof(C));
   if (smx > 48 * 1024) {
     PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
@@ -631,11 +730,10 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
   a.spec = base + L.spec;
   a.scr = reinterpret_cast<double*>(base + L.scr);
   const long long Nx = dims->n[0], Ny = dims->n[1], nz = dims->n[2];
-  a.log0 = ilog2_exact(Nx);
-  a.log1 = ilog2_exact(Ny);
   const long long nghost = g.npg - Nx * Ny * nz;
 
-  hmean_partial<<<kPartials, 256, 0, st>>>(g, w, a.partial);
+  const int kpad = (int)((g.n2 + 31) / 32 * 32);
+  hmean_partial<<<kPartials, kpad < 1024 ? kpad : 1024, 0, st>>>(g, w, a.partial);
   pb_note_launch();
   hmean_final<<<1, 256, 0, st>>>(g, a.partial, a.mean, kPartials, 1.0 / (double)(Ny * Nx));
   pb_note_launch();

@@ -1,0 +1,186 @@
+// Thermodynamic functions of the saturation adjustment, templated on the
+// exp/log implementation M:
+//   * ExactMath (crmath.cuh, correctly rounded) for the FP64 plain form,
+//     instantiated only in thermo.cu, compiled with -fmad=false so the
+//     temperature follows the reference's separately rounded C arithmetic;
+//   * FastMath (CUDA's exp/log, FMA contraction on) for the precision form,
+//     instantiated only in thermo_fast.cu and mlp.cu.
+// Everything here has internal linkage: each translation unit gets its own
+// copy compiled with its own flags.
+#pragma once
+
+#include "pb_common.cuh"
+
+namespace {
+namespace thermo_f {
+
+using namespace pbc;
+
+struct FastMath {
+  static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+  static __device__ __forceinline__ double log(double x) { return ::log(x); }
+};
+
+// ---- Csrc/thermodynamic_functions.h, Csrc/entropies.h
+__device__ __forceinline__ double pd_c(double p0, double qt, double qv) {
+  return p0 * (1.0 - qt) / (1.0 - qt + eps_vi * qv);
+}
+__device__ __forceinline__ double pv_c(double p0, double qt, double qv) {
+  return p0 * eps_vi * qv / (1.0 - qt + eps_vi * qv);
+}
+__device__ __forceinline__ double qv_star_c(double p0, double qt, double pv) {
+  return eps_v * (1.0 - qt) * pv / (p0 - pv);
+}
+// alpha and buoyancy: buoyancy cancels ~3 digits of alpha, so both keep the
+// reference's separately rounded operations in either form.
+__device__ __forceinline__ double alpha_c(double p0, double T, double qt, double qv) {
+  return mul_rn((Rd * T) / p0, add_rn(sub_rn(1.0, qt), mul_rn(eps_vi, qv)));
+}
+__device__ __forceinline__ double buoyancy_c(double alpha0, double alpha) {
+  return mul_rn(g, sub_rn(alpha, alpha0)) / alpha0;
+}
+__device__ __forceinline__ double cpm_c(double qt) { return (1.0 - qt) * cpd + qt * cpv; }
+template <class M>
+__device__ __forceinline__ double sd_c(double pd, double T) {
+  return sd_tilde + cpd * M::log(T / T_tilde) - Rd * M::log(pd / p_tilde);
+}
+template <class M>
+__device__ __forceinline__ double sv_c(double pv, double T) {
+  return sv_tilde + cpv * M::log(T / T_tilde) - Rv * M::log(pv / p_tilde);
+}
+__device__ __forceinline__ double sc_c(double L, double T) { return -L / T; }
+__device__ __forceinline__ double interp_2(double a, double b) { return 0.5 * (a + b); }
+
+// latent_heat_variable with lambda_constant (Microphysics.pxd:65-75)
+__device__ __forceinline__ double latent_heat(double T) {
+  const double TC = T - 273.15;
+  return (2500.8 - 2.36 * TC + 0.0016 * TC * TC - 0.00006 * TC * TC * TC) * 1000.0;
+}
+
+// lookup (Csrc/lookup.h:48-54) with a range check the reference lacks:
+// out-of-table arguments flag PB_ERR_TABLE_RANGE and are clamped.
+__device__ __forceinline__ double table_lookup(const pb_table& t, double x, unsigned int* err) {
+  const double fi = floor((x - t.x_min) * t.dxi);
+  long long indx;
+  if (!(fi >= 0.0 && fi <= (double)(t.n - 2))) {
+    pb_flag_at(err, PB_ERR_TABLE_RANGE);
+    indx = (fi >= 0.0) ? t.n - 2 : 0;
+  } else {
+    indx = (long long)fi;
+  }
+  const double y1 = __ldg(t.y + indx);
+  const double y2 = __ldg(t.y + indx + 1);
+  const double x1 = t.x_min + t.dx * indx;
+  return y1 + (x - x1) * (y2 - y1) * t.dxi;
+}
+
+// temperature_no_ql (Csrc/thermodynamics_sa.h:10-15)
+template <class M>
+__device__ __forceinline__ double temperature_no_ql(double pd, double pv, double s, double qt) {
+  return T_tilde * M::exp((s - (1.0 - qt) * (sd_tilde - Rd * M::log(pd / p_tilde)) -
+                           qt * (sv_tilde - Rv * M::log(pv / p_tilde))) /
+                          ((1.0 - qt) * cpd + qt * cpv));
+}
+
+// The secant's first point (Csrc/thermodynamics_sa.h:22-24): the temperature
+// with all water as vapour.  The learned seed is a correction to it.
+template <class M>
+__device__ __forceinline__ double first_point(double p0, double s, double qt) {
+  const double pv_1 = pv_c(p0, qt, qt);
+  const double pd_1 = p0 - pv_1;
+  return temperature_no_ql<M>(pd_1, pv_1, s, qt);
+}
+
+struct EosOut {
+  double T, qv, ql, qi;
+  int iters;
+  bool sat;
+};
+
+// eos_c (Csrc/thermodynamics_sa.h:17-66) in two parts, so that a caller can
+// evaluate learned seeds for the saturated cells between them.
+struct EosStart {
+  double pd_1, pv_1, T_1, qv_star_1;
+  bool sat;
+};
+
+template <class M>
+__device__ __forceinline__ EosStart eos_start(const pb_table& LT, double p0, double s, double qt,
+                                              unsigned int* err) {
+  EosStart e;
+  e.pv_1 = pv_c(p0, qt, qt);
+  e.pd_1 = p0 - e.pv_1;
+  e.T_1 = temperature_no_ql<M>(e.pd_1, e.pv_1, s, qt);
+  const double pv_star_1 = table_lookup(LT, e.T_1, err);
+  e.qv_star_1 = qv_star_c(p0, qt, pv_star_1);
+  e.sat = !(qt <= e.qv_star_1);
+  return e;
+}
+
+// The saturated branch (:33-64).  The secant loop is the reference's; it is
+// capped at max_iter (the reference loops without a cap), reaching the cap
+// sets PB_ERR_SECANT_CAP.  use_seed replaces the second secant point T_2
+// (:39) by a learned guess; the loop and its stopping test stay the
+// reference's.
+template <class M>
+__device__ __forceinline__ EosOut eos_finish(const pb_table& LT, const EosStart& e, double p0, double s, double qt,
+                                             int max_iter, bool use_seed, double seed, unsigned int* err) {
+  EosOut o;
+  o.qv = qt;
+  o.ql = 0.0;
+  o.qi = 0.0;
+  o.iters = 0;
+  double T_1 = e.T_1;
+  if (!e.sat) {
+    o.T = T_1;
+    o.sat = false;
+    return o;
+  }
+  o.sat = true;
+  const double sigma_1 = qt - e.qv_star_1;
+  const double L_1 = latent_heat(T_1);
+  const double s_1 =
+      sd_c<M>(e.pd_1, T_1) * (1.0 - qt) + sv_c<M>(e.pv_1, T_1) * qt + sc_c(L_1, T_1) * sigma_1;
+  double f_1 = s - s_1;
+  double T_2 = T_1 + sigma_1 * L_1 / ((1.0 - qt) * cpd + e.qv_star_1 * cpv);
+  if (use_seed) T_2 = seed;
+  double delta_T;
+  double qv_star_2, sigma_2;
+  int it = 0;
+  do {
+    const double pv_star_2 = table_lookup(LT, T_2, err);
+    qv_star_2 = qv_star_c(p0, qt, pv_star_2);
+    const double pv_2 = pv_c(p0, qt, qv_star_2);
+    const double pd_2 = p0 - pv_2;
+    sigma_2 = qt - qv_star_2;
+    const double L_2 = latent_heat(T_2);
+    const double s_2 = sd_c<M>(pd_2, T_2) * (1.0 - qt) + sv_c<M>(pv_2, T_2) * qt + sc_c(L_2, T_2) * sigma_2;
+    const double f_2 = s - s_2;
+    const double T_n = T_2 - f_2 * (T_2 - T_1) / (f_2 - f_1);
+    T_1 = T_2;
+    T_2 = T_n;
+    f_1 = f_2;
+    delta_T = fabs(T_2 - T_1);
+    ++it;
+    if (it >= max_iter) {
+      if (delta_T >= 1.0e-3 || sigma_2 < 0.0) pb_flag_at(err, PB_ERR_SECANT_CAP);
+      break;
+    }
+  } while (delta_T >= 1.0e-3 || sigma_2 < 0.0);
+  o.T = T_2;
+  o.qv = qv_star_2;
+  o.ql = 1.0 * sigma_2;  // lambda = 1
+  o.qi = (1.0 - 1.0) * sigma_2;
+  o.iters = it;
+  return o;
+}
+
+template <class M>
+__device__ __forceinline__ EosOut eos_sa(const pb_table& LT, double p0, double s, double qt, int max_iter,
+                                         bool use_seed, double seed, unsigned int* err) {
+  const EosStart e = eos_start<M>(LT, p0, s, qt, err);
+  return eos_finish<M>(LT, e, p0, s, qt, max_iter, use_seed, seed, err);
+}
+
+}  // namespace thermo_f
+}  // namespace

@@ -1,0 +1,331 @@
+// Saturation-adjustment and dry thermodynamics kernels, templated on the
+// exp/log implementation (thermo_funcs.cuh) and instantiated by
+// thermo.cu (FP64 plain form, correctly rounded exp/log, no FMA) and
+// thermo_fast.cu (precision form: CUDA exp/log, FMA, optional learned seed).
+//
+// One thread block owns whole (i,j) columns, one thread per level k, so the
+// vertical neighbours that buoyancy_update_sa / bvf_sa need come from shared
+// memory and every cell's state is computed exactly once.
+#pragma once
+
+#include "pb_common.cuh"
+#include "thermo_funcs.cuh"
+#include "mlp.cuh"
+
+namespace thermo_k {
+
+struct SeedNet {             // learned seed (precision form), see pb_mlp
+  const __nv_bfloat16* w1;
+  const float* b1;
+  const __nv_bfloat16* w2;
+  const float* b2;
+  const __nv_bfloat16* w3;
+  const float* b3;
+  float lo[3], hi[3];
+  float out_mean, out_scale;
+};
+
+struct SaArgs {
+  const double* p0;          // RS.p0_half
+  const double* alpha0;      // RS.alpha0_half
+  pb_table LT;
+  const double* s;
+  double* qt;
+  double* T;
+  double* qv;
+  double* ql;
+  double* qi;
+  double* alpha;
+  double* buoy;
+  double* theta_rho;
+  double* bvf;
+  double* thetali;
+  double* wt;
+  unsigned long long* stats; // {iterations, saturated cells} (nullable)
+  unsigned int* err;         // device error word
+  SeedNet net;
+  int clip;
+  int max_iter;
+};
+
+struct DryArgs {
+  const double* pd;       // RS.p0_half
+  const double* alpha0;   // RS.alpha0_half
+  const double* s;
+  double* T;
+  double* alpha;
+  double* buoy;
+  double* theta;
+  double* bvf;
+  double* wt;
+};
+
+// Launch shape: blocks of (kpad, cols) threads, kpad = n2 rounded up to a
+// warp, cols columns per block; dynamic shared memory for the per-column
+// arrays (and the network and its per-warp slots when seeded).
+void column_launch_shape(long long n2, int per_col_arrays, dim3* blk, size_t* smem);
+unsigned int column_grid(long long ncols, dim3 blk);
+constexpr size_t kSeedSlotFloats = 32 * 4;  // per warp: 3 inputs + 1 output per lane
+size_t seed_smem_bytes(dim3 blk);
+
+// Per-translation-unit launchers.
+cudaError_t launch_sa_exact(const Geo& geo, const SaArgs& a, cudaStream_t st);
+cudaError_t launch_dry_exact(const Geo& geo, const DryArgs& a, cudaStream_t st);
+cudaError_t launch_sa_fast(const Geo& geo, const SaArgs& a, bool seeded, cudaStream_t st);
+cudaError_t launch_dry_fast(const Geo& geo, const DryArgs& a, cudaStream_t st);
+
+}  // namespace thermo_k
+
+namespace {
+namespace thermo_kk {
+
+using namespace pbc;
+using namespace thermo_f;
+using thermo_k::DryArgs;
+using thermo_k::SaArgs;
+
+// ThermodynamicsSA.update (ThermodynamicsSA.pyx:176-213): clip_qt, eos_update,
+// buoyancy_update_sa, bvf_sa, thetali_update.  Shared memory per column: T,
+// qt, theta_rho, buoyancy; with SEED, the network's weights and 32 slots per
+// warp follow.  Each block walks a uniform number of column groups
+// (grid-stride), so the per-level constants (p0, alpha0, the Exner function)
+// are evaluated once per thread.
+//
+// SEED: after the first secant point, each warp compacts its saturated cells
+// into its slots, evaluates the network on them 16 at a time on the tensor
+// cores, and each saturated cell starts the secant from
+//   T_2 = T_1 + out_mean + out_scale * y.
+template <class M, bool SEED>
+__global__ void thermo_sa_kernel(Geo geo, SaArgs a, long long ncols) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* sm = reinterpret_cast<double*>(smraw);
+  const int kpad = blockDim.x;
+  const int k = threadIdx.x;
+  const long long n2 = geo.n2;
+  double* sT = sm + (size_t)threadIdx.y * 4 * kpad;
+  double* sQ = sT + kpad;
+  double* sR = sQ + kpad;
+  double* sB = sR + kpad;
+  mlpk::Smem* net = nullptr;
+  float* slots = nullptr;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = tid & 31;
+  if constexpr (SEED) {
+    net = reinterpret_cast<mlpk::Smem*>(smraw + (size_t)4 * kpad * blockDim.y * sizeof(double));
+    slots = reinterpret_cast<float*>(net + 1) + (size_t)(tid >> 5) * thermo_k::kSeedSlotFloats;
+    mlpk::stage_weights(*net, a.net.w1, a.net.b1, a.net.w2, a.net.b2, a.net.w3, a.net.b3, tid,
+                        blockDim.x * blockDim.y);
+    __syncthreads();
+  }
+  const bool kin = k < n2;
+  const double p0 = kin ? a.p0[k] : 1.0;
+  const double a0 = kin ? a.alpha0[k] : 1.0;
+  const double exner = pow(p0 / p_tilde, kappa);
+  const double dzi = 1.0 / geo.dx2;
+  unsigned long long my_it = 0, my_sat = 0;
+  for (long long cbase = (long long)blockIdx.x * blockDim.y; cbase < ncols; cbase += (long long)gridDim.x * blockDim.y) {
+    const long long col = cbase + threadIdx.y;
+    const bool active = (col < ncols) && kin;
+    const long long idx = col * n2 + k;  // columns are contiguous: (i*n1 + j)*n2
+    double qt = 0.0, qv = 0.0, T = 0.0, s = 0.0;
+    EosStart st{};
+    if (active) {
+      qt = a.qt[idx];
+      if (a.clip) {  // clip_qt (Csrc/thermodynamics_sa.h:213-219)
+        qt = fmax(qt, 1e-11);
+        a.qt[idx] = qt;
+      }
+      s = a.s[idx];
+      st = eos_start<M>(a.LT, p0, s, qt, a.err);
+    }
+    double seed = 0.0;
+    if constexpr (SEED) {
+      const bool sat = active && st.sat;
+      const unsigned mask = __ballot_sync(0xffffffffu, sat);
+      if (mask) {  // warp-uniform
+        const int pos = __popc(mask & ((1u << lane) - 1u));
+        const int count = __popc(mask);
+        if (sat) {
+          slots[pos * 4 + 0] = mlpk::norm_in(p0, a.net.lo[0], a.net.hi[0]);
+          slots[pos * 4 + 1] = mlpk::norm_in(s, a.net.lo[1], a.net.hi[1]);
+          slots[pos * 4 + 2] = mlpk::norm_in(qt, a.net.lo[2], a.net.hi[2]);
+        }
+        __syncwarp();
+        const int g = lane >> 2, t = lane & 3;
+        for (int t0 = 0; t0 < count; t0 += 16) {
+          const int r0 = t0 + g, r1 = t0 + g + 8;
+          float x0[3] = {0.f, 0.f, 0.f}, x1[3] = {0.f, 0.f, 0.f};
+          if (r0 < count)
+            for (int i = 0; i < 3; ++i) x0[i] = slots[r0 * 4 + i];
+          if (r1 < count)
+            for (int i = 0; i < 3; ++i) x1[i] = slots[r1 * 4 + i];
+          float y0, y1;
+          mlpk::forward_tile(*net, x0, x1, y0, y1, nullptr);
+          if (t == 0) {
+            if (r0 < count) slots[r0 * 4 + 3] = y0;
+            if (r1 < count) slots[r1 * 4 + 3] = y1;
+          }
+        }
+        __syncwarp();
+        if (sat) seed = st.T_1 + (double)a.net.out_mean + (double)a.net.out_scale * (double)slots[pos * 4 + 3];
+        __syncwarp();  // the slots are reused by the next column group
+      }
+    }
+    if (active) {
+      const EosOut e = eos_finish<M>(a.LT, st, p0, s, qt, a.max_iter, SEED && st.sat, seed, a.err);
+      T = e.T;
+      qv = e.qv;
+      if (!isfinite(T)) pb_flag_at(a.err, PB_ERR_NONFINITE);
+      my_it += (unsigned long long)e.iters;
+      my_sat += e.sat ? 1ull : 0ull;
+      a.T[idx] = T;
+      a.qv[idx] = qv;
+      a.ql[idx] = e.ql;
+      a.qi[idx] = e.qi;
+      const double al = alpha_c(p0, T, qt, qv);
+      a.alpha[idx] = al;
+      // thetali_update (:185-211) with thetali_c (thermodynamic_functions.h:15-18);
+      // without condensate the exponential is exp(-0) = 1 exactly
+      const double theta = T / exner;
+      if (e.ql == 0.0 && e.qi == 0.0) {
+        a.thetali[idx] = theta * 1.0;
+      } else {
+        const double Lv = latent_heat(T);
+        a.thetali[idx] = theta * M::exp(-Lv * (e.ql / (1.0 - qt) + e.qi / (1.0 - qt)) / (T * cpd));
+      }
+      // bvf_sa first loop (:147-157): theta_rho on k in [1, n2-1)
+      double thr = 0.0;
+      if (k >= 1 && k < n2 - 1) {
+        thr = T * (1.0 - qt + eps_vi * qv) / exner;
+        a.theta_rho[idx] = thr;
+      }
+      // buoyancy_update_sa first loop (:110-119): k in [0, n2-1)
+      double b = 0.0;
+      if (k < n2 - 1) {
+        b = buoyancy_c(a0, al);
+        a.buoy[idx] = b;
+      }
+      sT[k] = T;
+      sQ[k] = qt;
+      sR[k] = thr;
+      sB[k] = b;
+    }
+    __syncthreads();
+    if (active) {
+      // buoyancy_update_sa second loop (:121-130): k in [1, n2-3)
+      if (k >= 1 && k < n2 - 3) a.wt[idx] = a.wt[idx] + interp_2(sB[k], sB[k + 1]);
+      // bvf_sa second loop (:159-180): k in [2, n2-2)
+      if (k >= 2 && k < n2 - 2) {
+        double bv;
+        if (qv < qt) {
+          const double Lv = latent_heat(T);
+          const double pv_star = table_lookup(a.LT, T, a.err);
+          const double rsl = eps_v * pv_star / (p0 - pv_star);
+          const double gamma_w = g / cpd * (1.0 / (1.0 - qt)) * (1.0 + Lv * rsl / (Rd * T)) /
+                                 (cpm_c(qt) / cpd + Lv * Lv * (eps_v + rsl) * rsl / (cpd * Rd * T * T));
+          const double dTdz = (interp_2(sT[k], sT[k + 1]) - interp_2(sT[k - 1], sT[k])) * dzi;
+          const double dqtdz = (interp_2(sQ[k], sQ[k + 1]) - interp_2(sQ[k - 1], sQ[k])) * dzi;
+          bv = g / T * (dTdz + gamma_w) * (1.0 + Lv * rsl / (Rd * T)) - dqtdz / (1.0 - qt);
+        } else {
+          bv = g / sR[k] * (interp_2(sR[k], sR[k + 1]) - interp_2(sR[k - 1], sR[k])) * dzi;
+        }
+        a.bvf[idx] = bv;
+      }
+    }
+    __syncthreads();  // shared memory is reused by the next column group
+  }
+  if (a.stats) {
+    // warp-aggregated secant statistics
+    for (int off = 16; off > 0; off >>= 1) {
+      my_it += __shfl_down_sync(0xffffffffu, my_it, off);
+      my_sat += __shfl_down_sync(0xffffffffu, my_sat, off);
+    }
+    if (lane == 0 && (my_it | my_sat)) {
+      atomicAdd(a.stats, my_it);
+      atomicAdd(a.stats + 1, my_sat);
+    }
+  }
+}
+
+// ThermodynamicsDry.update (ThermodynamicsDry.pyx:105-120).
+template <class M>
+__global__ void thermo_dry_kernel(Geo geo, DryArgs a, long long ncols) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* sm = reinterpret_cast<double*>(smraw);
+  const int kpad = blockDim.x;
+  const long long col = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const int k = threadIdx.x;
+  const long long n2 = geo.n2;
+  double* sTh = sm + (size_t)threadIdx.y * 2 * kpad;
+  double* sB = sTh + kpad;
+  const bool active = (col < ncols) && (k < n2);
+  const long long i = col / geo.n1;
+  const long long j = col - i * geo.n1;
+  long long idx = 0;
+  double T = 0.0;
+  if (active) {
+    idx = col * n2 + k;
+    const double pd = a.pd[k];
+    // eos_c (Csrc/thermodynamics_dry.h:8-10), eos_update (:12-37)
+    T = T_tilde * (M::exp((a.s[idx] - sd_tilde + Rd * M::log(pd / p_tilde)) / cpd));
+    a.T[idx] = T;
+    const double al = mul_rn((Rd * T) / pd, 1.0);
+    a.alpha[idx] = al;
+    // buoyancy_update (:39-73): i < n0-1, j < n1-1, k < n2-1
+    const bool bij = (i < geo.n0 - 1) && (j < geo.n1 - 1);
+    double b = 0.0;
+    if (bij && k < n2 - 1) {
+      b = buoyancy_c(a.alpha0[k], al);
+      a.buoy[idx] = b;
+    } else if (bij) {
+      b = a.buoy[idx];  // level n2-1 keeps the field's current value
+    }
+    sB[k] = b;
+    // bvf_dry (:75-110): theta on k in [1, n2)
+    double th = 0.0;
+    if (k >= 1) {
+      th = T / pow(pd / p_tilde, kappa);
+      a.theta[idx] = th;
+    }
+    sTh[k] = th;
+  }
+  __syncthreads();
+  if (active) {
+    if ((i < geo.n0 - 1) && (j < geo.n1 - 1) && k < n2 - 1) a.wt[idx] += interp_2(sB[k], sB[k + 1]);
+    if (k >= 2 && k < n2 - 1) {
+      const double dzi = 1.0 / geo.dx2;
+      a.bvf[idx] = g / sTh[k] * (interp_2(sTh[k], sTh[k + 1]) - interp_2(sTh[k - 1], sTh[k])) * dzi;
+    }
+  }
+}
+
+template <class M, bool SEED>
+cudaError_t launch_sa(const Geo& geo, const SaArgs& a, cudaStream_t st) {
+  dim3 blk;
+  size_t smem;
+  thermo_k::column_launch_shape(geo.n2, 4, &blk, &smem);
+  if (SEED) smem += thermo_k::seed_smem_bytes(blk);
+  if (smem > 48 * 1024) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(thermo_sa_kernel<M, SEED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const long long ncols = geo.n0 * geo.n1;
+  thermo_sa_kernel<M, SEED><<<thermo_k::column_grid(ncols, blk), blk, smem, st>>>(geo, a, ncols);
+  pb_note_launch();
+  return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t launch_dry(const Geo& geo, const DryArgs& a, cudaStream_t st) {
+  dim3 blk;
+  size_t smem;
+  thermo_k::column_launch_shape(geo.n2, 2, &blk, &smem);
+  const long long ncols = geo.n0 * geo.n1;
+  thermo_dry_kernel<M><<<ceil_div(ncols, blk.y), blk, smem, st>>>(geo, a, ncols);
+  pb_note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace thermo_kk
+}  // namespace

@@ -142,3 +142,29 @@ __device__ __forceinline__ double weno_face(double a0, double a1, double a2, dou
 __device__ __forceinline__ double upwind_flux(double vel, double phip, double phim, double rho) {
   return 0.5 * ((vel + fabs(vel)) * phip + (vel - fabs(vel)) * phim) * rho;
 }
+
+// Upwind-only evaluation.  Of the reference's two biased interpolants one is
+// always multiplied by an exact zero ((u-|u|) for u >= 0, (u+|u|) for
+// u <= 0), so only the upwind one is computed: from a window v[0..W-1]
+// (W = ORDER+1; the face lies between v[W/2-1] and v[W/2]) the stencil is
+// v[0..ORDER-1] for u >= 0 and v[W-1..1] for u < 0, picked element by
+// element so lanes of one warp that see both signs do not diverge.  With
+// phi the upwind value,
+//   0.5*((u+|u|)*phi + (u-|u|)*phi)*rho
+// equals the reference's flux for every finite input (the zero term adds
+// +-0), rounding included, so the FP64 form stays bit-identical.
+template <int ORDER, bool F32>
+__device__ __forceinline__ double weno_upwind(bool pos, const double* v) {
+  constexpr int W = ORDER + 1;
+  double st[ORDER];
+#pragma unroll
+  for (int m = 0; m < ORDER; ++m) st[m] = pos ? v[m] : v[W - 1 - m];
+  if constexpr (ORDER == 5)
+    return weno_face<5, F32>(st[0], st[1], st[2], st[3], st[4]);
+  else
+    return weno_face<7, F32>(st[0], st[1], st[2], st[3], st[4], st[5], st[6]);
+}
+
+__device__ __forceinline__ double upwind_flux1(double vel, double phi, double rho) {
+  return 0.5 * ((vel + fabs(vel)) * phi + (vel - fabs(vel)) * phi) * rho;
+}

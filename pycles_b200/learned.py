@@ -2,10 +2,14 @@
 
 A 3 -> 64 -> 64 -> 1 SiLU MLP maps (p0, s, qt), each normalised to [-1, 1]
 over p0 in [5e4, 1.02e5] Pa, s in [6800, 7100] J/kg/K, qt in [0, 0.025],
-to the temperature that seeds the secant of eos_c in place of its
-linearised second point (Csrc/thermodynamics_sa.h:39).  The secant loop
-itself is unchanged and still runs to the reference tolerance, so the
-network can only change how many iterations a cell takes.
+to the correction T - T_1 between the converged temperature and the
+secant's first point T_1 (the all-vapour temperature of
+Csrc/thermodynamics_sa.h:22-24).  The seed T_1 + correction replaces the
+secant's linearised second point (:39).  The secant loop itself is
+unchanged and still runs to the reference tolerance, so the network can only
+change how many iterations a cell takes.  Learning the correction rather
+than T itself keeps the target's scale at ~1 K, so the BF16 network's
+relative error costs millikelvins.
 
 Training pairs come from the plain FP64 secant (pb_eos_sa) on saturated
 (p0, s, qt) samples; training runs on the GPU with this library's own BF16
@@ -30,7 +34,7 @@ OFF = {"w1": (0, H * 3), "b1": (H * 3, H), "w2": (H * 3 + H, H * H), "b2": (H * 
 
 
 class SeedMLP:
-    def __init__(self, device="cuda", seed=0, out_mean=285.0, out_scale=15.0):
+    def __init__(self, device="cuda", seed=0, out_mean=0.5, out_scale=1.0):
         self.device = torch.device(device)
         g = torch.Generator().manual_seed(seed)
         p = torch.zeros(_capi.MLP_NPARAM, dtype=torch.float32)
@@ -100,10 +104,11 @@ class SeedMLP:
             lr, beta1, beta2, eps, 1.0 / float(n), self.w1.data_ptr(), self.b1.data_ptr(), self.w2.data_ptr(),
             self.b2.data_ptr(), self.w3.data_ptr(), self.b3.data_ptr(), _capi.stream_handle(stream)), "pb_mlp_adam")
 
-    def train(self, p0, s, qt, T, epochs=3, batch=16384, lr=3e-3, lr_final=1e-4, seed=0, log=None):
-        """Mini-batch Adam on (p0, s, qt) -> T pairs (CUDA float64 tensors)."""
+    def train(self, p0, s, qt, T, T1, epochs=3, batch=16384, lr=3e-3, lr_final=1e-4, seed=0, log=None):
+        """Mini-batch Adam on (p0, s, qt) -> T - T1 pairs (CUDA float64
+        tensors; T1 the secant's first point); cosine learning-rate decay."""
         x = self.normalise(p0, s, qt)
-        y = ((T - self.out_mean) / self.out_scale).to(torch.float32).contiguous()
+        y = ((T - T1 - self.out_mean) / self.out_scale).to(torch.float32).contiguous()
         n = x.shape[0]
         g = torch.Generator(device=x.device).manual_seed(seed)
         nb = max(1, n // batch)
@@ -127,16 +132,17 @@ class SeedMLP:
 
 
 def training_pairs(thermo, p0, s, qt, max_iter=100):
-    """(p0, s, qt) -> (T, secant iterations) from the plain FP64 secant
+    """(p0, s, qt) -> (T, T_1, secant iterations) from the plain FP64 secant
     (pb_eos_sa); keeps the saturated points (iterations > 0)."""
     table = thermo.CC.device_table(p0.device)
     T = torch.empty_like(p0)
+    T1 = torch.empty_like(p0)
     its = torch.empty(p0.numel(), dtype=torch.int32, device=p0.device)
     _capi.check(_capi.load().pb_eos_sa(ctypes.byref(table), p0.data_ptr(), s.data_ptr(), qt.data_ptr(), None,
-                                       T.data_ptr(), None, None, its.data_ptr(), p0.numel(), max_iter,
-                                       _capi.stream_handle(None)), "pb_eos_sa")
+                                       T.data_ptr(), None, None, T1.data_ptr(), its.data_ptr(), p0.numel(),
+                                       max_iter, _capi.stream_handle(None)), "pb_eos_sa")
     keep = its > 0
-    return p0[keep], s[keep], qt[keep], T[keep], its[keep]
+    return p0[keep], s[keep], qt[keep], T[keep], T1[keep], its[keep]
 
 
 def secant_iterations(thermo, p0, s, qt, seed=None, max_iter=100):
@@ -146,7 +152,7 @@ def secant_iterations(thermo, p0, s, qt, seed=None, max_iter=100):
     its = torch.empty(p0.numel(), dtype=torch.int32, device=p0.device)
     _capi.check(_capi.load().pb_eos_sa(ctypes.byref(table), p0.data_ptr(), s.data_ptr(), qt.data_ptr(),
                                        seed.data_ptr() if seed is not None else None, T.data_ptr(), None, None,
-                                       its.data_ptr(), p0.numel(), max_iter, _capi.stream_handle(None)),
+                                       None, its.data_ptr(), p0.numel(), max_iter, _capi.stream_handle(None)),
                 "pb_eos_sa")
     return T, its
 

@@ -204,7 +204,8 @@ class ThermodynamicsSA:
         th = namelist.get("thermodynamics", {})
         self.do_qt_clipping = bool(th.get("do_qt_clipping", True))
         self.max_secant_iter = int(namelist.get("gpu", {}).get("secant_max_iter", 100))
-        self.mlp = None          # learned seed (pycles_b200.learned.SeedMLP) or None
+        self.precision = _capi.precision_of(namelist)
+        self.mlp = None          # learned seed (pycles_b200.learned.SeedMLP, precision form) or None
         self.iter_stats = None   # device int64[2]: secant iterations, saturated cells
 
     def initialize(self, Gr, PV, DV, NS=None, Pa=None):
@@ -235,15 +236,13 @@ class ThermodynamicsSA:
         if self.iter_stats is None or self.iter_stats.device != PV.values.device:
             self.iter_stats = torch.zeros(2, dtype=torch.int64, device=PV.values.device)
         mlp_struct = None
-        seed_scratch = None
         if self.mlp is not None:
-            # learned path: seeds of the saturated cells first (no counterpart
-            # in the reference), then the unchanged secant
-            if getattr(self, "_seed_scratch", None) is None or self._seed_scratch.numel() != Gr.dims.npg:
-                self._seed_scratch = torch.empty(Gr.dims.npg, dtype=torch.float64, device=PV.values.device)
+            # learned seed for the secant's second point (no counterpart in the
+            # reference; precision form only), evaluated inside the kernel
+            if self.precision != _capi.PB_FP32:
+                raise ValueError("the learned seed belongs to the precision form (gpu.precision = 'fp32')")
             self._mlp_struct = self.mlp.struct()
             mlp_struct = ctypes.byref(self._mlp_struct)
-            seed_scratch = _capi.ptr(self._seed_scratch)
         table = self.CC.device_table(PV.values.device)
         rc = L.pb_thermo_sa(ctypes.byref(Gr.dims), _capi.ptr(RS.d_p0_half), _capi.ptr(RS.d_alpha0_half),
                             ctypes.byref(table), _capi.ptr(PV.field("s", Gr)), _capi.ptr(PV.field("qt", Gr)),
@@ -251,8 +250,8 @@ class ThermodynamicsSA:
                             _capi.ptr(f("qi", Gr)), _capi.ptr(f("alpha", Gr)), _capi.ptr(f("buoyancy", Gr)),
                             _capi.ptr(f("theta_rho", Gr)), _capi.ptr(f("buoyancy_frequency", Gr)),
                             _capi.ptr(f("thetali", Gr)), _capi.ptr(PV.tendency("w", Gr)),
-                            1 if self.do_qt_clipping else 0, mlp_struct, seed_scratch, _capi.ptr(self.iter_stats),
-                            self.max_secant_iter, _capi.stream_handle(stream))
+                            1 if self.do_qt_clipping else 0, mlp_struct, _capi.ptr(self.iter_stats),
+                            self.max_secant_iter, self.precision, _capi.stream_handle(stream))
         _capi.check(rc, "pb_thermo_sa")
 
 
@@ -263,6 +262,7 @@ class ThermodynamicsDry:
 
     def __init__(self, namelist=None, LH=None, Par=None):
         self.CC = ClausiusClapeyron(namelist)
+        self.precision = _capi.precision_of(namelist)
 
     def initialize(self, Gr, PV, DV, NS=None, Pa=None):
         PV.add_variable("s", "J kg^-1 K^-1", "s", "specific entropy", "sym", "scalar", Pa)
@@ -286,5 +286,5 @@ class ThermodynamicsDry:
                              _capi.ptr(PV.field("s", Gr)), _capi.ptr(f("temperature", Gr)),
                              _capi.ptr(f("alpha", Gr)), _capi.ptr(f("buoyancy", Gr)), _capi.ptr(f("theta", Gr)),
                              _capi.ptr(f("buoyancy_frequency", Gr)), _capi.ptr(PV.tendency("w", Gr)),
-                             _capi.stream_handle(stream))
+                             self.precision, _capi.stream_handle(stream))
         _capi.check(rc, "pb_thermo_dry")

@@ -82,7 +82,12 @@ def test_mlp_forward_and_gradient_vs_cpu():
     p0, s, qt = (torch.tensor(a, dtype=torch.float64, device="cuda") for a in phys)
     y_gpu = mlp.forward(p0, s, qt).cpu().numpy()
     y_cpu, _ = _cpu_mlp(params, mlp.normalise(p0, s, qt).cpu().numpy().astype(np.float64), 0, 1, True)
-    y_cpu = mlp.out_mean + mlp.out_scale * y_cpu
+    # the seed is the secant's first point plus the network's correction
+    from oracle import port
+    P, S, Q = phys
+    pv1 = port.pv_c(P, Q, Q)
+    T1 = port.temperature_no_ql(P - pv1, pv1, S, Q)
+    y_cpu = T1 + mlp.out_mean + mlp.out_scale * y_cpu
     assert np.max(np.abs(y_gpu - y_cpu)) / mlp.out_scale < 3e-2
 
 
@@ -96,11 +101,12 @@ def test_trained_seed_cuts_secant_iterations():
     p0 = 7.0e4 + 3.2e4 * torch.rand(n, device="cuda", dtype=torch.float64, generator=g)
     s = 6850.0 + 200.0 * torch.rand(n, device="cuda", dtype=torch.float64, generator=g)
     qt = 0.004 + 0.02 * torch.rand(n, device="cuda", dtype=torch.float64, generator=g)
-    P, S, Q, T, its = learned.training_pairs(th, p0, s, qt)
+    P, S, Q, T, T1, its = learned.training_pairs(th, p0, s, qt)
     assert P.numel() > 10_000
     ntr = P.numel() * 9 // 10
-    mlp = learned.SeedMLP(seed=0, out_mean=float(T.mean()), out_scale=float(T.std()) * 2)
-    hist = mlp.train(P[:ntr], S[:ntr], Q[:ntr], T[:ntr], epochs=6, batch=8192)
+    r = T - T1
+    mlp = learned.SeedMLP(seed=0, out_mean=float(r.mean()), out_scale=float(r.std()) * 2)
+    hist = mlp.train(P[:ntr], S[:ntr], Q[:ntr], T[:ntr], T1[:ntr], epochs=6, batch=8192)
     assert hist[-1] < hist[0]
     # held-out points: iterations with and without the seed, same answer
     Pt, St, Qt, Tt = P[ntr:], S[ntr:], Q[ntr:], T[ntr:]
@@ -112,3 +118,39 @@ def test_trained_seed_cuts_secant_iterations():
     print(f"seed mean |error| {err:.3e} K; mean secant iterations plain {mp:.3f}, seeded {ms:.3f}")
     assert ms < mp
     assert float((T_seed - T_plain).abs().max()) < 2e-3
+
+
+def test_fused_seed_in_thermodynamics():
+    """The seed evaluated inside the precision-form thermodynamics kernel:
+    same temperatures as the plain form to the secant's tolerance, fewer
+    secant iterations than the precision form without the seed."""
+    from helpers import gpu_dv, gpu_sim, host_case
+    from pycles_b200 import learned
+    nl, rs, f = host_case(case="dycoms", nx=16, ny=16, nz=256, dx=35.0, dy=35.0, dz=5.0, gw=4, dt=0.25,
+                          scalar_order=7, momentum_order=5)
+    plain = gpu_sim(nl, rs, f)
+    fast = gpu_sim(nl, rs, f, precision="fp32")
+    seeded = gpu_sim(nl, rs, f, precision="fp32")
+    n2 = plain.Gr.dims.nlg[2]
+    s = torch.as_tensor(f["s"], device="cuda")
+    qt = torch.as_tensor(f["qt"], device="cuda")
+    p0 = seeded.RS.d_p0_half.repeat(s.numel() // n2)
+    P, S, Q = learned.sample_inputs([(p0, s, qt)], 600_000, rng_seed=1)
+    P, S, Q, T, T1, _ = learned.training_pairs(seeded.Th, P, S, Q)
+    r = T - T1
+    mlp = learned.SeedMLP(seed=0, out_mean=float(r.mean()), out_scale=2.0 * float(r.std()))
+    mlp.train(P, S, Q, T, T1, epochs=8, batch=8192)
+    seeded.Th.mlp = mlp
+    stats = {}
+    for name, g in (("plain", plain), ("fast", fast), ("seeded", seeded)):
+        g.PV.Update_all_bcs(g.Gr)
+        g.Th.iter_stats = None
+        g.Th.update(g.Gr, g.RS, g.PV, g.DV)
+        it, nsat = g.Th.iter_stats.cpu().tolist()
+        stats[name] = (it / max(nsat, 1), nsat, gpu_dv(g))
+    print({k: v[:2] for k, v in stats.items()})
+    assert stats["plain"][1] == stats["fast"][1] == stats["seeded"][1] > 1000
+    Tp, Tf, Ts = (stats[k][2]["temperature"] for k in ("plain", "fast", "seeded"))
+    assert np.max(np.abs(Tf - Tp)) < 1e-6
+    assert np.max(np.abs(Ts - Tp)) < 2e-3
+    assert stats["seeded"][0] < stats["fast"][0]
