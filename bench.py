@@ -45,6 +45,40 @@ ADV_BYTES_PER_CELL = {5: 120, 4: 96}
 ADV_FLOPS_PER_CELL = {("c5", 7): 3252, ("moist", 5): 2340, ("dry", 5): 1881}
 
 
+def _ghost_bytes(nv, cfg):
+    """Ghost fill: 16 B per ghost cell and variable, per interior cell."""
+    gw, n = cfg["gw"], (cfg["nx"], cfg["ny"], cfg["nz"])
+    npl = n[0] * n[1] * n[2]
+    npg = (n[0] + 2 * gw) * (n[1] + 2 * gw) * (n[2] + 2 * gw)
+    return 16.0 * nv * (npg - npl) / npl
+
+
+# Compulsory (algorithmic) bytes per interior cell per RK stage of each timed
+# component, FP64 storage: every array it must read once and write once.
+COMPONENT_BYTES_PER_CELL = {
+    # moist: read s, qt, w-tendency; write qt, T, qv, ql, qi, alpha,
+    # buoyancy, theta_rho, bvf, thetali, w-tendency.  dry: read s,
+    # w-tendency; write T, alpha, buoyancy, theta, bvf, w-tendency.
+    "thermo": lambda nv, cfg: 112.0 if cfg["case"] != "dry_cbl" else 64.0,
+    # read u, v, w and the scalars, read-modify-write the scalar tendencies
+    "scalar_adv": lambda nv, cfg: 8.0 * nv + 16.0 * (nv - 3),
+    # read u, v, w, read-modify-write the three momentum tendencies
+    "momentum_adv": lambda nv, cfg: 72.0,
+    # SSP-RK3 stage (read value, tendency, copy; write value, copy,
+    # zeroed tendency: 40 B per variable) + ghost fill
+    "rk3+bcs": lambda nv, cfg: 40.0 * nv + _ghost_bytes(nv, cfg),
+    # read u, v, w; write u, v, w, divergence, pressure
+    "pressure": lambda nv, cfg: 64.0,
+}
+COMPONENT_KERNELS = {
+    "thermo": "thermo_sa_kernel (saturation adjustment, buoyancy, bvf, thetali; one launch per stage)",
+    "scalar_adv": "scalar_march x, y + scalar_z (WENO fluxes + divergence, 3 launches per stage)",
+    "momentum_adv": "momentum_march x, y + momentum_z (3 launches per stage)",
+    "rk3+bcs": "rk3_kernel + ghost_fill_kernel",
+    "pressure": "hmean, fft_x_fwd, fft_y, tdma, fft_x_inv (+ refinement), ghost_sym, correction",
+}
+
+
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -287,13 +321,21 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     log = (lambda m: print(m, file=sys.stderr)) if rank == 0 else (lambda m: None)
-    forms = ["fp64"] if args.form == "fp64" else (["fp32"] if args.form == "fp32" else ["fp64", "fp32"])
+    # (name, precision, learned seed); the last one is the headline
+    forms = []
+    if args.form in ("all", "fp64"):
+        forms.append(("fp64", "fp64", False))
+    if args.form in ("all", "fp32"):
+        forms.append(("fp32", "fp32", False))
+        if cfg["case"] != "dry_cbl" and not args.no_learned:
+            forms.append(("fp32+learned", "fp32", True))
     results = {}
     fields = None
     rs = None
     headline_sim = None
-    for form in forms:
-        nl = namelist_for(**cfg, precision=form)
+    trained = None
+    for form, precision, learned in forms:
+        nl = namelist_for(**cfg, precision=precision)
         sim = HotPathSimulation(nl, device=dev)
         if fields is None:
             fields = sim.initialize(seed=rank)
@@ -302,10 +344,11 @@ def run_ours(args, rank, world, local_rank):
             sim.set_reference_state(rs)
             sim.load_fields(fields)
         seed_info = None
-        if form == "fp32" and sim.moist and not args.no_learned:
-            out = _train_seed(sim, fields, log)
-            if out is not None:
-                sim.Th.mlp, seed_info = out
+        if learned:
+            if trained is None:
+                trained = _train_seed(sim, fields, log)
+            if trained is not None:
+                sim.Th.mlp, seed_info = trained
         sim.run(0)  # ghost fill + first thermodynamics update, as Simulation3d.run
         _capi.clear_error()
         for _ in range(args.warmup):
@@ -319,15 +362,16 @@ def run_ours(args, rank, world, local_rank):
             "component_ms_per_step": {c: round(v / args.steps, 4) for c, v in comp_ms.items()},
             "gpu_launches": launches, "clocks": clock_info, "secant": secant,
             "device_error_word": _capi.get_error(),
-            "learned_seed": seed_info, "pressure_refine_sweeps": sim.Pr.refine_sweeps if form == "fp32" else None,
+            "learned_seed": seed_info,
+            "pressure_refine_sweeps": sim.Pr.refine_sweeps if precision == "fp32" else None,
         }
         log(f"form {form}: {results[form]['ms_per_step']:.2f} ms/step")
-        if form == forms[-1]:
+        if form == forms[-1][0]:
             headline_sim = sim
         else:
             del sim
             torch.cuda.empty_cache()
-    head = forms[-1]
+    head = forms[-1][0]
     sim = headline_sim
     PV, Gr = sim.PV, sim.Gr
     npl = Gr.dims.npl
@@ -359,24 +403,29 @@ def run_ours(args, rank, world, local_rank):
                                      "after every step (the reference keeps it in host numpy arrays)"}
         del host
 
-    # ---- roofline of the dominant kernel group (advection) -----------------
+    # ---- roofline per component; the headline is the largest one ----------
     peak, peak_kind = _peaks()
     r = results[head]
     nv = PV.nv
-    cm = r["component_ms_per_step"]
-    adv_ms = (cm["scalar_adv"] + cm["momentum_adv"]) / 3.0
-    adv_bytes = ADV_BYTES_PER_CELL.get(nv, 24 * nv) * npl
-    achieved = adv_bytes / (adv_ms / 1e3) / 1e9
+    comps = {}
+    for comp, ms_step in r["component_ms_per_step"].items():
+        ms = ms_step / 3.0  # per RK stage
+        nbytes = COMPONENT_BYTES_PER_CELL[comp](nv, cfg)
+        ach = nbytes * npl / (ms / 1e3) / 1e9
+        comps[comp] = {"ms_per_stage": round(ms, 4), "algorithmic_bytes_per_cell_stage": nbytes,
+                       "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4),
+                       "traffic_bytes_per_stage": _read_traffic(args.config, head, comp)}
     flops_key = ("c5", 7) if cfg.get("scalar_order", 5) == 7 else (("moist", 5) if nv == 5 else ("dry", 5))
-    adv_flops = ADV_FLOPS_PER_CELL[flops_key] * npl
-    traffic = _read_traffic(args.config, head)
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "advection (scalar + momentum launches of one RK stage)",
-                "algorithmic_bytes_per_cell_stage": ADV_BYTES_PER_CELL.get(nv, 24 * nv),
-                "flops_per_cell_stage": ADV_FLOPS_PER_CELL[flops_key],
-                "achieved_tflops": round(adv_flops / (adv_ms / 1e3) / 1e12, 2),
-                "note": "the advection is FP-pipe bound, not HBM bound: see achieved_tflops"}
+    adv_ms = comps["scalar_adv"]["ms_per_stage"] + comps["momentum_adv"]["ms_per_stage"]
+    comps["scalar_adv+momentum_adv"] = {
+        "flops_per_cell_stage": ADV_FLOPS_PER_CELL[flops_key],
+        "achieved_tflops": round(ADV_FLOPS_PER_CELL[flops_key] * npl / (adv_ms / 1e3) / 1e12, 2)}
+    top = max(r["component_ms_per_step"], key=lambda c: r["component_ms_per_step"][c])
+    roofline = {"bound": "hbm", "achieved": comps[top]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                "frac": comps[top]["frac"], "traffic": comps[top]["traffic_bytes_per_stage"],
+                "peak_source": peak_kind, "kernel": COMPONENT_KERNELS[top],
+                "algorithmic_bytes_per_cell_stage": comps[top]["algorithmic_bytes_per_cell_stage"],
+                "components": comps}
 
     out = None
     if rank == 0:
@@ -390,13 +439,12 @@ def run_ours(args, rank, world, local_rank):
                                    f"gw={cfg['gw']}, WENO{cfg.get('scalar_order', 5)} scalars / "
                                    f"WENO{cfg.get('momentum_order', 5)} momentum, case={cfg['case']}, "
                                    f"dt={cfg['dt']}",
-                       "form": (("fp32+learned" if r["learned_seed"] else "fp32") if head == "fp32"
-                                else "fp64 plain"),
+                       "form": head,
                        "cells": npl, "l2": "inputs larger than L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "forms": results,
-            "speedup_fp32_learned_vs_fp64_plain": (results["fp32"]["value"] / results["fp64"]["value"]
-                                                   if "fp32" in results and "fp64" in results else None),
+            "speedup_vs_fp64_plain": ({f: results[f]["value"] / results["fp64"]["value"] for f in results}
+                                      if "fp64" in results else None),
             "component_ms_per_step": r["component_ms_per_step"],
             "roofline": roofline,
             "e2e": e2e,
@@ -407,17 +455,19 @@ def run_ours(args, rank, world, local_rank):
     return out, sim
 
 
-def _read_traffic(config, precision):
-    """DRAM bytes per launch of the dominant kernels, from the committed ncu
-    summary (profiles/advection_*.md: a line 'traffic_bytes_per_stage: N')."""
+def _read_traffic(config, form, component):
+    """DRAM bytes per RK stage of a component's kernels, from the committed
+    ncu summaries (profiles/*.md lines
+    'traffic_bytes_per_stage[<config>,<form>,<component>]: N'), or None."""
     import glob
     import re
-    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "advection_*.md"))):
+    key = rf"traffic_bytes_per_stage\[{re.escape(config)},{re.escape(form)},{re.escape(component)}\]:\s*([0-9.eE+]+)"
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         try:
             txt = open(p).read()
         except OSError:
             continue
-        m = re.search(rf"traffic_bytes_per_stage\[{re.escape(config)},{precision}\]:\s*([0-9.eE+]+)", txt)
+        m = re.search(key, txt)
         if m:
             return float(m.group(1))
     return None
@@ -429,8 +479,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c5_dycoms")
-    ap.add_argument("--form", default="both", choices=["both", "fp64", "fp32"],
-                    help="fp64: plain form; fp32: precision form + learned seed; both: headline fp32")
+    ap.add_argument("--form", default="all", choices=["all", "fp64", "fp32"],
+                    help="fp64: plain form; fp32: precision form without and with the learned seed; "
+                         "all: every form, headline the last (fp32+learned)")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")

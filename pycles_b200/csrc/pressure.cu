@@ -7,7 +7,8 @@
 // to each (kx,ky) column with consecutive threads on consecutive i.
 //
 //   hmean_partial/hmean_final  HorizontalMean(w), deterministic two-pass sum
-//   remove_mean                w -= mean[k] on every cell (remove_mean_u3)
+//   (remove_mean_u3)           w -= mean[k] on every cell, applied where w is
+//                              read: in the divergence and in the correction
 //   zero_ghosts                divergence ghosts = 0 (the reference zeroes the
 //                              whole array before adding the interior terms)
 //   fft_x_fwd                  second_order_divergence (d = 0,1,2 in order)
@@ -137,28 +138,32 @@ __device__ __forceinline__ void dft8(C* v, bool inverse) {
 // writes them to (j div Ns) Ns R + (j mod Ns) + r Ns.  Input and output are
 // in natural order.  Needs nlines * N <= 16 * blockDim.x.
 template <class C, int R>
-__device__ __forceinline__ void stockham_pass(C* buf, int nlines, int N, int Ns, const C* __restrict__ tw,
+__device__ __forceinline__ void stockham_pass(C* buf, int nlines, int lgN, int lgNs, const C* __restrict__ tw,
                                               bool inverse) {
   constexpr int MAXI = 16 / R;
-  const int per_line = N / R;
-  const int total = nlines * per_line;
+  constexpr int lgR = R == 8 ? 3 : (R == 4 ? 2 : 1);
+  const int N = 1 << lgN;
+  const int lg_per = lgN - lgR;              // per_line = N / R
+  const int per_line = 1 << lg_per;
+  const int total = nlines << lg_per;
   const int ld = line_ld(N);
-  const int twstep = N / (Ns * R);
+  const int lg_tw = lgN - lgNs - lgR;        // twiddle step N / (Ns R)
+  const int ns_mask = (1 << lgNs) - 1;
   C v[MAXI][R];
 #pragma unroll
   for (int it = 0; it < MAXI; ++it) {
     const int b = threadIdx.x + it * blockDim.x;
     if (b < total) {
-      const int l = b / per_line;
-      const int j = b - l * per_line;
+      const int l = b >> lg_per;
+      const int j = b & (per_line - 1);
       const C* line = buf + l * ld;
 #pragma unroll
       for (int r = 0; r < R; ++r) v[it][r] = line[swz(j + r * per_line)];
-      if (Ns > 1) {
-        const int k = j % Ns;
+      if (lgNs > 0) {
+        const int k = j & ns_mask;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          C w = tw[k * r * twstep];
+          C w = tw[(k * r) << lg_tw];
           if (inverse) w.y = -w.y;
           v[it][r] = cmul(v[it][r], w);
         }
@@ -173,13 +178,13 @@ __device__ __forceinline__ void stockham_pass(C* buf, int nlines, int N, int Ns,
   for (int it = 0; it < MAXI; ++it) {
     const int b = threadIdx.x + it * blockDim.x;
     if (b < total) {
-      const int l = b / per_line;
-      const int j = b - l * per_line;
-      const int k = j % Ns;
-      const int base = (j - k) * R + k;
+      const int l = b >> lg_per;
+      const int j = b & (per_line - 1);
+      const int k = j & ns_mask;
+      const int base = ((j - k) << lgR) + k;
       C* line = buf + l * ld;
 #pragma unroll
-      for (int r = 0; r < R; ++r) line[swz(base + r * Ns)] = v[it][r];
+      for (int r = 0; r < R; ++r) line[swz(base + (r << lgNs))] = v[it][r];
     }
   }
   __syncthreads();
@@ -188,13 +193,27 @@ __device__ __forceinline__ void stockham_pass(C* buf, int nlines, int N, int Ns,
 // Power-of-two N: radix-8 passes, then one radix-4 or radix-2 pass.
 template <class C>
 __device__ void fft_lines_pow2(C* buf, int nlines, int N, const C* __restrict__ tw, bool inverse) {
-  int Ns = 1;
-  while (Ns * 8 <= N) {
-    stockham_pass<C, 8>(buf, nlines, N, Ns, tw, inverse);
-    Ns *= 8;
+  const int lgN = __ffs(N) - 1;
+  int lgNs = 0;
+  while (lgNs + 3 <= lgN) {
+    stockham_pass<C, 8>(buf, nlines, lgN, lgNs, tw, inverse);
+    lgNs += 3;
   }
-  if (Ns * 4 == N) stockham_pass<C, 4>(buf, nlines, N, Ns, tw, inverse);
-  else if (Ns * 2 == N) stockham_pass<C, 2>(buf, nlines, N, Ns, tw, inverse);
+  if (lgNs + 2 == lgN) stockham_pass<C, 4>(buf, nlines, lgN, lgNs, tw, inverse);
+  else if (lgNs + 1 == lgN) stockham_pass<C, 2>(buf, nlines, lgN, lgNs, tw, inverse);
+}
+
+// e -> (e / d, e % d) with a shift and a mask when d is a power of two
+// (the usual case: line counts are powers of two, and so are most N).
+__device__ __forceinline__ void split_idx(int e, int d, int& q, int& r) {
+  if ((d & (d - 1)) == 0) {
+    const int lg = __ffs(d) - 1;
+    q = e >> lg;
+    r = e & (d - 1);
+  } else {
+    q = e / d;
+    r = e - q * d;
+  }
 }
 
 // Direct DFT for lengths that are not powers of two: out = DFT(in), both in
@@ -292,20 +311,21 @@ __global__ void hmean_partial(Geo g, const double* __restrict__ w, double* __res
   }
 }
 
+// One block per level: each thread sums a fixed strided subset of the
+// partials, then a fixed-order tree in shared memory (deterministic).
 __global__ void hmean_final(Geo g, const double* __restrict__ partial, double* __restrict__ mean, int np,
                             double n_horizontal_i) {
-  for (long long k = threadIdx.x; k < g.n2; k += blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < np; ++b) s += partial[(long long)b * g.n2 + k];
-    mean[k] = s * n_horizontal_i;
+  __shared__ double red[256];
+  const long long k = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < np; b += blockDim.x) s += partial[(long long)b * g.n2 + k];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
   }
-}
-
-// remove_mean_u3 (PressureSolver.pyx:113-136): every cell
-__global__ void remove_mean(Geo g, double* __restrict__ w, const double* __restrict__ mean) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < g.npg; t += stride)
-    w[t] = w[t] - mean[t % g.n2];
+  if (threadIdx.x == 0) mean[k] = red[0] * n_horizontal_i;
 }
 
 __device__ __forceinline__ void ghost_decode(const Geo& g, long long t, long long& i, long long& j, long long& k) {
@@ -369,8 +389,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
   const int ld = line_ld(N);
   const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
   for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
-    const int kl = e % KC;
-    const int il = e / KC;
+    int kl, il;
+    split_idx(e, KC, il, kl);
     if (kl >= kc) continue;
     const long long k = g.gw + k0 + kl;
     const long long ijk = (g.gw + il) * g.is + j * g.js + k;
@@ -380,7 +400,10 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
       d = 0.0;
       d = add_rn(d, mul_rn(sub_rn(a.u[ijk] / ah, a.u[ijk - g.is] / ah), dxi0));
       d = add_rn(d, mul_rn(sub_rn(a.v[ijk] / ah, a.v[ijk - g.js] / ah), dxi1));
-      d = add_rn(d, mul_rn(sub_rn((a.w[ijk]) / a.alpha0[k], (a.w[ijk - 1]) / a.alpha0[k - 1]), dxi2));
+      // w after remove_mean_u3 (PressureSolver.pyx:113-136), w - mean[k]
+      const double wc = sub_rn(a.w[ijk], a.mean[k]);
+      const double wm = sub_rn(a.w[ijk - 1], a.mean[k - 1]);
+      d = add_rn(d, mul_rn(sub_rn(wc / a.alpha0[k], wm / a.alpha0[k - 1]), dxi2));
       a.div[ijk] = d;
     } else {
       const double* p = a.p;
@@ -400,8 +423,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
   C* spec = reinterpret_cast<C*>(a.spec);
   const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
   for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
-    const int il = e % N;
-    const int kl = e / N;
+    int kl, il;
+    split_idx(e, N, kl, il);
     spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il] = res[kl * ld + swz(il)];
   }
 }
@@ -419,8 +442,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, boo
   const int ld = line_ld(N);
   C* plane = reinterpret_cast<C*>(a.spec) + (long long)kk * N * Nx;
   for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
-    const int il = e % IC;
-    const int jl = e / IC;
+    int il, jl;
+    split_idx(e, IC, jl, il);
     if (il >= ic) continue;
     in[il * ld + swz(jl)] = plane[(long long)jl * Nx + i0 + il];
   }
@@ -428,8 +451,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, boo
   const C* res = fft_lines<C>(in, ic, IC, N, twy_of<C>(a), inverse);
   const double sc = inverse ? 1.0 / (double)N : 1.0;
   for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
-    const int il = e % IC;
-    const int jl = e / IC;
+    int il, jl;
+    split_idx(e, IC, jl, il);
     if (il >= ic) continue;
     C r = res[il * ld + swz(jl)];
     if (inverse) {
@@ -489,7 +512,13 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
   xpy = xpy / b;
   x[0] = from_d<C>(xpx, xpy);
   scr[0] = s_prev;
+  // loads run two levels ahead of the recurrence
+  C xa = nz > 1 ? x[ncol] : from_d<C>(0.0, 0.0);
+  C xb = nz > 2 ? x[2 * ncol] : from_d<C>(0.0, 0.0);
   for (int k = 1; k < nz; ++k) {
+    const C xin = xa;
+    xa = xb;
+    if (k + 2 < nz) xb = x[(long long)(k + 2) * ncol];
     const double ak = mul_rn(mul_rn(dzi, dzi), rho0[k + gw - 1]);
     double ck, bk;
     if (k < nz - 1) {
@@ -503,7 +532,7 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
     s_prev = mul_rn(ck, m);
     scr[(long long)k * ncol] = s_prev;
     double xkx, xky;
-    to_d(x[(long long)k * ncol], xkx, xky);
+    to_d(xin, xkx, xky);
     xkx = mul_rn(sub_rn(xkx, mul_rn(ak, xpx)), m);
     xky = mul_rn(sub_rn(xky, mul_rn(ak, xpy)), m);
     // keep the FP64 forward-sweep values for the back substitution
@@ -512,10 +541,22 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
     xpy = xky;
   }
   // back substitution from the last value, reading the stored sweep values
+  // (two levels ahead, like the forward sweep)
+  double sa = nz > 1 ? scr[(long long)(nz - 2) * ncol] : 0.0;
+  double sb = nz > 2 ? scr[(long long)(nz - 3) * ncol] : 0.0;
+  xa = nz > 1 ? x[(long long)(nz - 2) * ncol] : from_d<C>(0.0, 0.0);
+  xb = nz > 2 ? x[(long long)(nz - 3) * ncol] : from_d<C>(0.0, 0.0);
   for (int k = nz - 2; k >= 0; --k) {
-    const double sk = scr[(long long)k * ncol];
+    const double sk = sa;
+    const C xin = xa;
+    sa = sb;
+    xa = xb;
+    if (k - 2 >= 0) {
+      sb = scr[(long long)(k - 2) * ncol];
+      xb = x[(long long)(k - 2) * ncol];
+    }
     double xkx, xky;
-    to_d(x[(long long)k * ncol], xkx, xky);
+    to_d(xin, xkx, xky);
     xkx = sub_rn(xkx, mul_rn(sk, xpx));
     xky = sub_rn(xky, mul_rn(sk, xpy));
     x[(long long)k * ncol] = from_d<C>(xkx, xky);
@@ -538,8 +579,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
   const C* spec = reinterpret_cast<const C*>(a.spec);
   const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
   for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
-    const int il = e % N;
-    const int kl = e / N;
+    int kl, il;
+    split_idx(e, N, kl, il);
     in[kl * ld + swz(il)] = spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il];
   }
   __syncthreads();
@@ -547,8 +588,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
   const double sc = 1.0 / (double)N;
   const long long j = g.gw + jl;
   for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
-    const int kl = e % KC;
-    const int il = e / KC;
+    int kl, il;
+    split_idx(e, KC, il, kl);
     if (kl >= kc) continue;
     const long long ijk = (g.gw + il) * g.is + j * g.js + g.gw + k0 + kl;
     const double val = (double)res[kl * ld + swz(il)].x * sc;
@@ -575,19 +616,26 @@ __global__ void ghost_sym(Geo g, double* __restrict__ f, long long nghost) {
 }
 
 // ---- second_order_pressure_correction (PressureSolver.pyx:83-110) ---------
+// w enters as it was before remove_mean_u3; every cell first gets w - mean[k]
+// (the reference's remove_mean_u3 over all cells), then the correction on
+// [0, nlg-1) in every dimension.
 __global__ void correction(Geo g, const double* __restrict__ p, double* __restrict__ u, double* __restrict__ v,
-                           double* __restrict__ w) {
+                           double* __restrict__ w, const double* __restrict__ mean) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < g.npg; t += stride) {
     const long long k = t % g.n2;
     const long long r = t / g.n2;
     const long long j = r % g.n1;
     const long long i = r / g.n1;
-    if (i >= g.n0 - 1 || j >= g.n1 - 1 || k >= g.n2 - 1) continue;
+    const double wt = sub_rn(w[t], mean[k]);
+    if (i >= g.n0 - 1 || j >= g.n1 - 1 || k >= g.n2 - 1) {
+      w[t] = wt;
+      continue;
+    }
     const double pc = p[t];
     u[t] = sub_rn(u[t], mul_rn(sub_rn(p[t + g.is], pc), g.dxi0));
     v[t] = sub_rn(v[t], mul_rn(sub_rn(p[t + g.js], pc), g.dxi1));
-    w[t] = sub_rn(w[t], mul_rn(sub_rn(p[t + 1], pc), g.dxi2));
+    w[t] = sub_rn(wt, mul_rn(sub_rn(p[t + 1], pc), g.dxi2));
   }
 }
 
@@ -614,6 +662,7 @@ int lines_for(long long N, size_t elem) {
   if (L > 16) L = 16;
   if (pow2(N) && L * N > 16LL * kFftThreads) L = 16LL * kFftThreads / N;
   if (L < 1) L = 1;
+  while (L & (L - 1)) L &= L - 1;  // a power of two: shifts in the index arithmetic
   return (int)L;
 }
 
@@ -735,9 +784,7 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
   const int kpad = (int)((g.n2 + 31) / 32 * 32);
   hmean_partial<<<kPartials, kpad < 1024 ? kpad : 1024, 0, st>>>(g, w, a.partial);
   pb_note_launch();
-  hmean_final<<<1, 256, 0, st>>>(g, a.partial, a.mean, kPartials, 1.0 / (double)(Ny * Nx));
-  pb_note_launch();
-  remove_mean<<<stream_blocks(g.npg), 256, 0, st>>>(g, w, a.mean);
+  hmean_final<<<(unsigned)g.n2, 256, 0, st>>>(g, a.partial, a.mean, kPartials, 1.0 / (double)(Ny * Nx));
   pb_note_launch();
   if (nghost > 0) {
     zero_ghosts<<<stream_blocks(nghost), 256, 0, st>>>(g, divergence, nghost);
@@ -764,7 +811,7 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
     ghost_sym<<<stream_blocks(nghost), 256, 0, st>>>(g, dynamic_pressure, nghost);
     pb_note_launch();
   }
-  correction<<<stream_blocks(g.npg), 256, 0, st>>>(g, dynamic_pressure, u, v, w);
+  correction<<<stream_blocks(g.npg), 256, 0, st>>>(g, dynamic_pressure, u, v, w, a.mean);
   pb_note_launch();
   PB_LAUNCH_CHECK();
   return PB_OK;

@@ -18,16 +18,6 @@ struct ExactMath {
 
 namespace thermo_k {
 
-// Column-group grid: enough blocks to fill the GPU several times over, each
-// looping over its share of columns.
-unsigned int column_grid(long long ncols, dim3 blk) {
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long groups = (ncols + blk.y - 1) / blk.y;
-  const long long cap = (long long)sms * 16;
-  return (unsigned int)(groups < cap ? groups : cap);
-}
-
 void column_launch_shape(long long n2, int per_col_arrays, dim3* blk, size_t* smem) {
   const int kpad = (int)((n2 + 31) / 32 * 32);
   int cols = 256 / kpad;

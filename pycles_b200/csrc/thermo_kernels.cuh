@@ -3,9 +3,9 @@
 // thermo.cu (FP64 plain form, correctly rounded exp/log, no FMA) and
 // thermo_fast.cu (precision form: CUDA exp/log, FMA, optional learned seed).
 //
-// One thread block owns whole (i,j) columns, one thread per level k, so the
-// vertical neighbours that buoyancy_update_sa / bvf_sa need come from shared
-// memory and every cell's state is computed exactly once.
+// Saturation adjustment: warps own vertical segments of columns (see
+// thermo_sa_kernel).  Dry thermodynamics: one thread block owns whole (i,j)
+// columns, one thread per level, neighbours through shared memory.
 #pragma once
 
 #include "pb_common.cuh"
@@ -60,11 +60,10 @@ struct DryArgs {
   double* wt;
 };
 
-// Launch shape: blocks of (kpad, cols) threads, kpad = n2 rounded up to a
-// warp, cols columns per block; dynamic shared memory for the per-column
-// arrays (and the network and its per-warp slots when seeded).
+// Launch shape of the dry kernel: blocks of (kpad, cols) threads, kpad = n2
+// rounded up to a warp, cols columns per block; dynamic shared memory for the
+// per-column arrays.  seed_smem_bytes: the network and its per-warp slots.
 void column_launch_shape(long long n2, int per_col_arrays, dim3* blk, size_t* smem);
-unsigned int column_grid(long long ncols, dim3 blk);
 constexpr size_t kSeedSlotFloats = 32 * 4;  // per warp: 3 inputs + 1 output per lane
 size_t seed_smem_bytes(dim3 blk);
 
@@ -85,62 +84,67 @@ using thermo_k::DryArgs;
 using thermo_k::SaArgs;
 
 // ThermodynamicsSA.update (ThermodynamicsSA.pyx:176-213): clip_qt, eos_update,
-// buoyancy_update_sa, bvf_sa, thetali_update.  Shared memory per column: T,
-// qt, theta_rho, buoyancy; with SEED, the network's weights and 32 slots per
-// warp follow.  Each block walks a uniform number of column groups
-// (grid-stride), so the per-level constants (p0, alpha0, the Exner function)
-// are evaluated once per thread.
+// buoyancy_update_sa, bvf_sa, thetali_update.
+//
+// Each warp owns one segment of kSeg levels of a column at a time: lane L
+// holds level k = kSeg*seg - 1 + L, lanes 1..kSeg are the segment's cells and
+// lanes 0 and kSeg+1 recompute the neighbouring levels (same code, same
+// inputs, same result as the warp that owns them), so the vertical
+// neighbours that buoyancy_update_sa / bvf_sa need come by shuffle and no
+// block barrier is needed: warps in the cloud layer, whose secant iterates,
+// do not hold up the others.  A warp keeps its segment and walks the
+// columns, so the per-level constants (p0, alpha0, the Exner function) are
+// evaluated once per lane.
 //
 // SEED: after the first secant point, each warp compacts its saturated cells
 // into its slots, evaluates the network on them 16 at a time on the tensor
 // cores, and each saturated cell starts the secant from
 //   T_2 = T_1 + out_mean + out_scale * y.
+constexpr int kSeg = 30;
+constexpr int kSaThreads = 256;
+
 template <class M, bool SEED>
-__global__ void thermo_sa_kernel(Geo geo, SaArgs a, long long ncols) {
+__global__ void __launch_bounds__(kSaThreads) thermo_sa_kernel(Geo geo, SaArgs a, long long ncols, int nseg,
+                                                               long long nstreams) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  double* sm = reinterpret_cast<double*>(smraw);
-  const int kpad = blockDim.x;
-  const int k = threadIdx.x;
-  const long long n2 = geo.n2;
-  double* sT = sm + (size_t)threadIdx.y * 4 * kpad;
-  double* sQ = sT + kpad;
-  double* sR = sQ + kpad;
-  double* sB = sR + kpad;
+  const int lane = threadIdx.x & 31;
   mlpk::Smem* net = nullptr;
   float* slots = nullptr;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int lane = tid & 31;
   if constexpr (SEED) {
-    net = reinterpret_cast<mlpk::Smem*>(smraw + (size_t)4 * kpad * blockDim.y * sizeof(double));
-    slots = reinterpret_cast<float*>(net + 1) + (size_t)(tid >> 5) * thermo_k::kSeedSlotFloats;
-    mlpk::stage_weights(*net, a.net.w1, a.net.b1, a.net.w2, a.net.b2, a.net.w3, a.net.b3, tid,
-                        blockDim.x * blockDim.y);
+    net = reinterpret_cast<mlpk::Smem*>(smraw);
+    slots = reinterpret_cast<float*>(net + 1) + (size_t)(threadIdx.x >> 5) * thermo_k::kSeedSlotFloats;
+    mlpk::stage_weights(*net, a.net.w1, a.net.b1, a.net.w2, a.net.b2, a.net.w3, a.net.b3, threadIdx.x,
+                        blockDim.x);
     __syncthreads();
   }
-  const bool kin = k < n2;
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (gwarp >= nstreams * nseg) return;  // whole warps
+  const int seg = (int)(gwarp % nseg);
+  const long long n2 = geo.n2;
+  const long long k = (long long)seg * kSeg - 1 + lane;
+  const bool kin = k >= 0 && k < n2;
+  const bool own = kin && lane >= 1 && lane <= kSeg;
   const double p0 = kin ? a.p0[k] : 1.0;
   const double a0 = kin ? a.alpha0[k] : 1.0;
   const double exner = pow(p0 / p_tilde, kappa);
   const double dzi = 1.0 / geo.dx2;
   unsigned long long my_it = 0, my_sat = 0;
-  for (long long cbase = (long long)blockIdx.x * blockDim.y; cbase < ncols; cbase += (long long)gridDim.x * blockDim.y) {
-    const long long col = cbase + threadIdx.y;
-    const bool active = (col < ncols) && kin;
+  for (long long col = gwarp / nseg; col < ncols; col += nstreams) {
     const long long idx = col * n2 + k;  // columns are contiguous: (i*n1 + j)*n2
-    double qt = 0.0, qv = 0.0, T = 0.0, s = 0.0;
+    double qt = 0.0, s = 0.0;
     EosStart st{};
-    if (active) {
+    if (kin) {
       qt = a.qt[idx];
       if (a.clip) {  // clip_qt (Csrc/thermodynamics_sa.h:213-219)
         qt = fmax(qt, 1e-11);
-        a.qt[idx] = qt;
+        if (own) a.qt[idx] = qt;
       }
       s = a.s[idx];
       st = eos_start<M>(a.LT, p0, s, qt, a.err);
     }
     double seed = 0.0;
     if constexpr (SEED) {
-      const bool sat = active && st.sat;
+      const bool sat = kin && st.sat;
       const unsigned mask = __ballot_sync(0xffffffffu, sat);
       if (mask) {  // warp-uniform
         const int pos = __popc(mask & ((1u << lane) - 1u));
@@ -168,52 +172,49 @@ __global__ void thermo_sa_kernel(Geo geo, SaArgs a, long long ncols) {
         }
         __syncwarp();
         if (sat) seed = st.T_1 + (double)a.net.out_mean + (double)a.net.out_scale * (double)slots[pos * 4 + 3];
-        __syncwarp();  // the slots are reused by the next column group
+        __syncwarp();  // the slots are reused by the next column
       }
     }
-    if (active) {
+    double T = 0.0, qv = 0.0, thr = 0.0, b = 0.0;
+    if (kin) {
       const EosOut e = eos_finish<M>(a.LT, st, p0, s, qt, a.max_iter, SEED && st.sat, seed, a.err);
       T = e.T;
       qv = e.qv;
-      if (!isfinite(T)) pb_flag_at(a.err, PB_ERR_NONFINITE);
-      my_it += (unsigned long long)e.iters;
-      my_sat += e.sat ? 1ull : 0ull;
-      a.T[idx] = T;
-      a.qv[idx] = qv;
-      a.ql[idx] = e.ql;
-      a.qi[idx] = e.qi;
       const double al = alpha_c(p0, T, qt, qv);
-      a.alpha[idx] = al;
-      // thetali_update (:185-211) with thetali_c (thermodynamic_functions.h:15-18);
-      // without condensate the exponential is exp(-0) = 1 exactly
-      const double theta = T / exner;
-      if (e.ql == 0.0 && e.qi == 0.0) {
-        a.thetali[idx] = theta * 1.0;
-      } else {
-        const double Lv = latent_heat(T);
-        a.thetali[idx] = theta * M::exp(-Lv * (e.ql / (1.0 - qt) + e.qi / (1.0 - qt)) / (T * cpd));
-      }
       // bvf_sa first loop (:147-157): theta_rho on k in [1, n2-1)
-      double thr = 0.0;
-      if (k >= 1 && k < n2 - 1) {
-        thr = T * (1.0 - qt + eps_vi * qv) / exner;
-        a.theta_rho[idx] = thr;
-      }
+      if (k >= 1 && k < n2 - 1) thr = T * (1.0 - qt + eps_vi * qv) / exner;
       // buoyancy_update_sa first loop (:110-119): k in [0, n2-1)
-      double b = 0.0;
-      if (k < n2 - 1) {
-        b = buoyancy_c(a0, al);
-        a.buoy[idx] = b;
+      if (k < n2 - 1) b = buoyancy_c(a0, al);
+      if (own) {
+        if (!isfinite(T)) pb_flag_at(a.err, PB_ERR_NONFINITE);
+        my_it += (unsigned long long)e.iters;
+        my_sat += e.sat ? 1ull : 0ull;
+        a.T[idx] = T;
+        a.qv[idx] = qv;
+        a.ql[idx] = e.ql;
+        a.qi[idx] = e.qi;
+        a.alpha[idx] = al;
+        // thetali_update (:185-211) with thetali_c (thermodynamic_functions.h:15-18);
+        // without condensate the exponential is exp(-0) = 1 exactly
+        const double theta = T / exner;
+        if (e.ql == 0.0 && e.qi == 0.0) {
+          a.thetali[idx] = theta * 1.0;
+        } else {
+          const double Lv = latent_heat(T);
+          a.thetali[idx] = theta * M::exp(-Lv * (e.ql / (1.0 - qt) + e.qi / (1.0 - qt)) / (T * cpd));
+        }
+        if (k >= 1 && k < n2 - 1) a.theta_rho[idx] = thr;
+        if (k < n2 - 1) a.buoy[idx] = b;
       }
-      sT[k] = T;
-      sQ[k] = qt;
-      sR[k] = thr;
-      sB[k] = b;
     }
-    __syncthreads();
-    if (active) {
+    // vertical neighbours from the adjacent lanes
+    const double T_dn = __shfl_up_sync(0xffffffffu, T, 1), T_up = __shfl_down_sync(0xffffffffu, T, 1);
+    const double q_dn = __shfl_up_sync(0xffffffffu, qt, 1), q_up = __shfl_down_sync(0xffffffffu, qt, 1);
+    const double r_dn = __shfl_up_sync(0xffffffffu, thr, 1), r_up = __shfl_down_sync(0xffffffffu, thr, 1);
+    const double b_up = __shfl_down_sync(0xffffffffu, b, 1);
+    if (own) {
       // buoyancy_update_sa second loop (:121-130): k in [1, n2-3)
-      if (k >= 1 && k < n2 - 3) a.wt[idx] = a.wt[idx] + interp_2(sB[k], sB[k + 1]);
+      if (k >= 1 && k < n2 - 3) a.wt[idx] = a.wt[idx] + interp_2(b, b_up);
       // bvf_sa second loop (:159-180): k in [2, n2-2)
       if (k >= 2 && k < n2 - 2) {
         double bv;
@@ -223,16 +224,15 @@ __global__ void thermo_sa_kernel(Geo geo, SaArgs a, long long ncols) {
           const double rsl = eps_v * pv_star / (p0 - pv_star);
           const double gamma_w = g / cpd * (1.0 / (1.0 - qt)) * (1.0 + Lv * rsl / (Rd * T)) /
                                  (cpm_c(qt) / cpd + Lv * Lv * (eps_v + rsl) * rsl / (cpd * Rd * T * T));
-          const double dTdz = (interp_2(sT[k], sT[k + 1]) - interp_2(sT[k - 1], sT[k])) * dzi;
-          const double dqtdz = (interp_2(sQ[k], sQ[k + 1]) - interp_2(sQ[k - 1], sQ[k])) * dzi;
+          const double dTdz = (interp_2(T, T_up) - interp_2(T_dn, T)) * dzi;
+          const double dqtdz = (interp_2(qt, q_up) - interp_2(q_dn, qt)) * dzi;
           bv = g / T * (dTdz + gamma_w) * (1.0 + Lv * rsl / (Rd * T)) - dqtdz / (1.0 - qt);
         } else {
-          bv = g / sR[k] * (interp_2(sR[k], sR[k + 1]) - interp_2(sR[k - 1], sR[k])) * dzi;
+          bv = g / thr * (interp_2(thr, r_up) - interp_2(r_dn, thr)) * dzi;
         }
         a.bvf[idx] = bv;
       }
     }
-    __syncthreads();  // shared memory is reused by the next column group
   }
   if (a.stats) {
     // warp-aggregated secant statistics
@@ -301,17 +301,25 @@ __global__ void thermo_dry_kernel(Geo geo, DryArgs a, long long ncols) {
 
 template <class M, bool SEED>
 cudaError_t launch_sa(const Geo& geo, const SaArgs& a, cudaStream_t st) {
-  dim3 blk;
-  size_t smem;
-  thermo_k::column_launch_shape(geo.n2, 4, &blk, &smem);
-  if (SEED) smem += thermo_k::seed_smem_bytes(blk);
+  const size_t smem = SEED ? thermo_k::seed_smem_bytes(dim3(kSaThreads, 1)) : 0;
   if (smem > 48 * 1024) {
     const cudaError_t e =
         cudaFuncSetAttribute(thermo_sa_kernel<M, SEED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
   const long long ncols = geo.n0 * geo.n1;
-  thermo_sa_kernel<M, SEED><<<thermo_k::column_grid(ncols, blk), blk, smem, st>>>(geo, a, ncols);
+  const int nseg = (int)((geo.n2 + kSeg - 1) / kSeg);
+  // resident blocks only; each warp walks its column stream
+  int dev = 0, sms = 148, per_sm = 1;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, thermo_sa_kernel<M, SEED>, kSaThreads, smem);
+  if (per_sm < 1) per_sm = 1;
+  const long long warps = (long long)sms * per_sm * (kSaThreads / 32);
+  long long nstreams = warps / nseg;
+  if (nstreams < 1) nstreams = 1;
+  if (nstreams > ncols) nstreams = ncols;
+  const long long blocks = (nstreams * nseg + kSaThreads / 32 - 1) / (kSaThreads / 32);
+  thermo_sa_kernel<M, SEED><<<(unsigned)blocks, kSaThreads, smem, st>>>(geo, a, ncols, nseg, nstreams);
   pb_note_launch();
   return cudaGetLastError();
 }
