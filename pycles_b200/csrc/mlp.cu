@@ -77,11 +77,13 @@ struct GradArgs {
   long long n;
 };
 
-constexpr int kGradWarps = 2;  // 64-thread blocks keep the static shared memory under 48 KiB
+constexpr int kGradWarps = 2;
+// dynamic shared memory of mlp_grad_kernel: the FP32 gradient accumulator
+constexpr size_t kGradSmem = NPARAM * sizeof(float);
 
 __global__ void __launch_bounds__(64) mlp_grad_kernel(GradArgs a) {
   __shared__ Smem sm;
-  __shared__ float acc[NPARAM];
+  extern __shared__ float acc[];  // [NPARAM]
   __shared__ float dz2_s[kGradWarps][16][H];
   __shared__ float h1_s[kGradWarps][16][H];
   __shared__ float loss_s;
@@ -316,7 +318,17 @@ extern "C" int pb_mlp_grad(const pb_mlp* mlp, const float* x, const float* targe
   a.grad = grad;
   a.loss = loss;
   a.n = n;
-  mlpk::mlp_grad_kernel<<<mlp_blocks((n + 15) / 16, mlpk::kGradWarps), 32 * mlpk::kGradWarps, 0, as_stream(stream)>>>(a);
+  // the shared-memory opt-in is set on each device's copy of the kernel
+  static bool attr_set[64] = {};
+  int dev = 0;
+  PB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    PB_CUDA_TRY(cudaFuncSetAttribute(mlpk::mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)mlpk::kGradSmem));
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
+  mlpk::mlp_grad_kernel<<<mlp_blocks((n + 15) / 16, mlpk::kGradWarps), 32 * mlpk::kGradWarps, mlpk::kGradSmem,
+                          as_stream(stream)>>>(a);
   pb_note_launch();
   PB_LAUNCH_CHECK();
   return PB_OK;

@@ -28,9 +28,19 @@ constexpr int OFF_W3 = OFF_B2 + H;       // [64]
 constexpr int OFF_B3 = OFF_W3 + H;       // [1]
 constexpr int NPARAM = OFF_B3 + 1;
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU(z) = z sigmoid(z), sigmoid(z) = (1 + tanh(z/2)) / 2, with the
+// hardware tanh approximation (tanh.approx.f32, one special-function
+// instruction; relative error ~2^-11, below the BF16 rounding of the
+// activations).  Training and inference use the same function.
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
+__device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 __device__ __forceinline__ float silu_grad(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = sigmoid(z);
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -47,11 +57,16 @@ __device__ __forceinline__ void mma_bf16_16816(float c[4], const uint32_t a[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// Weights staged in shared memory by the block.
+// Weights staged in shared memory by the block.  w1b packs layer 1's three
+// weights and bias per unit (one 16-byte load); w2f holds layer 2 in B
+// fragment order, [ntile][ktile][lane] -> {b0, b1}, so each lane's fragment
+// is one conflict-free 8-byte load.
 struct Smem {
   float w1[H * 3];
   float b1[H];
+  float4 w1b[H];
   __nv_bfloat16 w2[H * H];  // [n][k]
+  uint2 w2f[8 * 4 * 32];
   float b2[H];
   float w3[H];
   float b3;
@@ -68,6 +83,16 @@ __device__ __forceinline__ void stage_weights(Smem& sm, const __nv_bfloat16* w1,
     sm.b1[i] = b1[i];
     sm.b2[i] = b2[i];
     sm.w3[i] = __bfloat162float(w3[i]);
+    sm.w1b[i] = make_float4(__bfloat162float(w1[i * 3 + 0]), __bfloat162float(w1[i * 3 + 1]),
+                            __bfloat162float(w1[i * 3 + 2]), b1[i]);
+  }
+  for (int i = tid; i < 8 * 4 * 32; i += nthreads) {
+    const int lane = i & 31, kt = (i >> 5) & 3, nt = i >> 7;
+    const int n = nt * 8 + (lane >> 2), k = kt * 16 + 2 * (lane & 3);
+    uint2 b;
+    b.x = *reinterpret_cast<const uint32_t*>(w2 + n * H + k);
+    b.y = *reinterpret_cast<const uint32_t*>(w2 + n * H + k + 8);
+    sm.w2f[i] = b;
   }
   if (tid == 0) sm.b3 = b3[0];
 }
@@ -97,8 +122,8 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
       float h[2];
 #pragma unroll
       for (int p = 0; p < 2; ++p) {
-        const int c = col + p;
-        const float z = sm.b1[c] + sm.w1[c * 3 + 0] * x[0] + sm.w1[c * 3 + 1] * x[1] + sm.w1[c * 3 + 2] * x[2];
+        const float4 wb = sm.w1b[col + p];
+        const float z = wb.w + wb.x * x[0] + wb.y * x[1] + wb.z * x[2];
         if (keep) keep->z1[kt][r][p] = z;
         h[p] = silu(z);
       }
@@ -117,11 +142,8 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
     float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int kt = 0; kt < 4; ++kt) {
-      const int n = nt * 8 + g;
-      const int k = kt * 16 + 2 * t;
-      uint32_t b[2];
-      b[0] = *reinterpret_cast<const uint32_t*>(&sm.w2[n * H + k]);
-      b[1] = *reinterpret_cast<const uint32_t*>(&sm.w2[n * H + k + 8]);
+      const uint2 bf = sm.w2f[(nt * 4 + kt) * 32 + lane];
+      const uint32_t b[2] = {bf.x, bf.y};
       mma_bf16_16816(c, a1[kt], b);
     }
 #pragma unroll

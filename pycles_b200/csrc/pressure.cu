@@ -29,7 +29,7 @@
 namespace {
 
 constexpr int kPartials = 1184;  // 8 x 148 SMs
-constexpr int kFftThreads = 512;  // stockham_pass: nlines * N <= 16 * kFftThreads
+constexpr int kFftThreads = 256;  // stockham_pass: nlines * N <= 16 * kFftThreads
 
 struct PLayout {
   long long partial, mean, twx, twy, twxf, twyf, kx2, ky2, spec, scr, total;
@@ -512,56 +512,81 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
   xpy = xpy / b;
   x[0] = from_d<C>(xpx, xpy);
   scr[0] = s_prev;
-  // loads run two levels ahead of the recurrence
-  C xa = nz > 1 ? x[ncol] : from_d<C>(0.0, 0.0);
-  C xb = nz > 2 ? x[2 * ncol] : from_d<C>(0.0, 0.0);
-  for (int k = 1; k < nz; ++k) {
-    const C xin = xa;
-    xa = xb;
-    if (k + 2 < nz) xb = x[(long long)(k + 2) * ncol];
-    const double ak = mul_rn(mul_rn(dzi, dzi), rho0[k + gw - 1]);
-    double ck, bk;
-    if (k < nz - 1) {
-      ck = mul_rn(mul_rn(dzi, dzi), rho0[k + gw]);
-      bk = sub_rn(mul_rn(rho0h[k + gw], kk), mul_rn(mul_rn(add_rn(rho0[k + gw], rho0[k + gw - 1]), dzi), dzi));
-    } else {
-      ck = 0.0;
-      bk = sub_rn(mul_rn(rho0h[k + gw], kk), mul_rn(mul_rn(rho0[k + gw - 1], dzi), dzi));
+  // The sweeps walk the levels in batches of kB; the loads of the next batch
+  // are issued before the current one is processed, so every thread keeps
+  // kB independent loads in flight behind its serial recurrence.
+  constexpr int kB = 8;
+  C cur[kB], nxt[kB];
+#pragma unroll
+  for (int m = 0; m < kB; ++m) cur[m] = (1 + m < nz) ? x[(long long)(1 + m) * ncol] : from_d<C>(0.0, 0.0);
+  for (int kb = 1; kb < nz; kb += kB) {
+#pragma unroll
+    for (int m = 0; m < kB; ++m) {
+      const int kn = kb + kB + m;
+      nxt[m] = (kn < nz) ? x[(long long)kn * ncol] : from_d<C>(0.0, 0.0);
     }
-    const double m = 1.0 / sub_rn(bk, mul_rn(ak, s_prev));
-    s_prev = mul_rn(ck, m);
-    scr[(long long)k * ncol] = s_prev;
-    double xkx, xky;
-    to_d(xin, xkx, xky);
-    xkx = mul_rn(sub_rn(xkx, mul_rn(ak, xpx)), m);
-    xky = mul_rn(sub_rn(xky, mul_rn(ak, xpy)), m);
-    // keep the FP64 forward-sweep values for the back substitution
-    x[(long long)k * ncol] = from_d<C>(xkx, xky);
-    xpx = xkx;
-    xpy = xky;
+#pragma unroll
+    for (int m = 0; m < kB; ++m) {
+      const int k = kb + m;
+      if (k < nz) {
+        const double ak = mul_rn(mul_rn(dzi, dzi), rho0[k + gw - 1]);
+        double ck, bk;
+        if (k < nz - 1) {
+          ck = mul_rn(mul_rn(dzi, dzi), rho0[k + gw]);
+          bk = sub_rn(mul_rn(rho0h[k + gw], kk), mul_rn(mul_rn(add_rn(rho0[k + gw], rho0[k + gw - 1]), dzi), dzi));
+        } else {
+          ck = 0.0;
+          bk = sub_rn(mul_rn(rho0h[k + gw], kk), mul_rn(mul_rn(rho0[k + gw - 1], dzi), dzi));
+        }
+        const double m_ = 1.0 / sub_rn(bk, mul_rn(ak, s_prev));
+        s_prev = mul_rn(ck, m_);
+        scr[(long long)k * ncol] = s_prev;
+        double xkx, xky;
+        to_d(cur[m], xkx, xky);
+        xkx = mul_rn(sub_rn(xkx, mul_rn(ak, xpx)), m_);
+        xky = mul_rn(sub_rn(xky, mul_rn(ak, xpy)), m_);
+        x[(long long)k * ncol] = from_d<C>(xkx, xky);
+        xpx = xkx;
+        xpy = xky;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < kB; ++m) cur[m] = nxt[m];
   }
-  // back substitution from the last value, reading the stored sweep values
-  // (two levels ahead, like the forward sweep)
-  double sa = nz > 1 ? scr[(long long)(nz - 2) * ncol] : 0.0;
-  double sb = nz > 2 ? scr[(long long)(nz - 3) * ncol] : 0.0;
-  xa = nz > 1 ? x[(long long)(nz - 2) * ncol] : from_d<C>(0.0, 0.0);
-  xb = nz > 2 ? x[(long long)(nz - 3) * ncol] : from_d<C>(0.0, 0.0);
-  for (int k = nz - 2; k >= 0; --k) {
-    const double sk = sa;
-    const C xin = xa;
-    sa = sb;
-    xa = xb;
-    if (k - 2 >= 0) {
-      sb = scr[(long long)(k - 2) * ncol];
-      xb = x[(long long)(k - 2) * ncol];
+  // back substitution from the last value, reading the stored sweep values,
+  // in batches of kB levels going down
+  double scur[kB], snxt[kB];
+#pragma unroll
+  for (int m = 0; m < kB; ++m) {
+    const int k = nz - 2 - m;
+    cur[m] = (k >= 0) ? x[(long long)k * ncol] : from_d<C>(0.0, 0.0);
+    scur[m] = (k >= 0) ? scr[(long long)k * ncol] : 0.0;
+  }
+  for (int kb = nz - 2; kb >= 0; kb -= kB) {
+#pragma unroll
+    for (int m = 0; m < kB; ++m) {
+      const int kn = kb - kB - m;
+      nxt[m] = (kn >= 0) ? x[(long long)kn * ncol] : from_d<C>(0.0, 0.0);
+      snxt[m] = (kn >= 0) ? scr[(long long)kn * ncol] : 0.0;
     }
-    double xkx, xky;
-    to_d(xin, xkx, xky);
-    xkx = sub_rn(xkx, mul_rn(sk, xpx));
-    xky = sub_rn(xky, mul_rn(sk, xpy));
-    x[(long long)k * ncol] = from_d<C>(xkx, xky);
-    xpx = xkx;
-    xpy = xky;
+#pragma unroll
+    for (int m = 0; m < kB; ++m) {
+      const int k = kb - m;
+      if (k >= 0) {
+        double xkx, xky;
+        to_d(cur[m], xkx, xky);
+        xkx = sub_rn(xkx, mul_rn(scur[m], xpx));
+        xky = sub_rn(xky, mul_rn(scur[m], xpy));
+        x[(long long)k * ncol] = from_d<C>(xkx, xky);
+        xpx = xkx;
+        xpy = xky;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < kB; ++m) {
+      cur[m] = nxt[m];
+      scur[m] = snxt[m];
+    }
   }
 }
 
@@ -653,12 +678,13 @@ size_t fft_smem(long long N, int lines, size_t elem) {
   return (size_t)(pow2(N) ? 1 : 2) * (size_t)line_ld((int)N) * lines * elem;
 }
 
-// Lines per FFT block: up to 16 (128-byte runs of FP64 levels / FP32
-// complex columns in the global accesses) within ~80 KiB of shared memory,
-// and nlines * N <= 16 * kFftThreads for the Stockham passes.
+// Lines per FFT block: a power of two, up to 16, with nlines * N <=
+// 16 * kFftThreads for the Stockham passes and the block's shared memory
+// within 48 KiB (FP32) / 80 KiB (FP64), so that several blocks share an SM
+// and one block's loads overlap another's passes.
 int lines_for(long long N, size_t elem) {
   const long long per = (pow2(N) ? 1 : 2) * (long long)line_ld((int)N) * (long long)elem;
-  long long L = 81920 / per;
+  long long L = (elem <= 8 ? 49152 : 81920) / per;
   if (L > 16) L = 16;
   if (pow2(N) && L * N > 16LL * kFftThreads) L = 16LL * kFftThreads / N;
   if (L < 1) L = 1;

@@ -86,15 +86,15 @@ using thermo_k::SaArgs;
 // ThermodynamicsSA.update (ThermodynamicsSA.pyx:176-213): clip_qt, eos_update,
 // buoyancy_update_sa, bvf_sa, thetali_update.
 //
-// Each warp owns one segment of kSeg levels of a column at a time: lane L
-// holds level k = kSeg*seg - 1 + L, lanes 1..kSeg are the segment's cells and
-// lanes 0 and kSeg+1 recompute the neighbouring levels (same code, same
-// inputs, same result as the warp that owns them), so the vertical
-// neighbours that buoyancy_update_sa / bvf_sa need come by shuffle and no
-// block barrier is needed: warps in the cloud layer, whose secant iterates,
-// do not hold up the others.  A warp keeps its segment and walks the
-// columns, so the per-level constants (p0, alpha0, the Exner function) are
-// evaluated once per lane.
+// Work is split into tasks of one segment of kSeg levels of one column:
+// lane L of the warp holds level k = kSeg*seg - 1 + L, lanes 1..kSeg are the
+// segment's cells and lanes 0 and kSeg+1 recompute the neighbouring levels
+// (same code, same inputs, same result as the warp that owns them), so the
+// vertical neighbours that buoyancy_update_sa / bvf_sa need come by shuffle
+// and no block barrier is needed.  Warps take the tasks in column-major
+// order, grid-stride, so every warp sees every segment and the cloud-layer
+// segments, whose secant iterates, are spread over all warps.  The Exner
+// function of every level is tabulated in shared memory once per block.
 //
 // SEED: after the first secant point, each warp compacts its saturated cells
 // into its slots, evaluates the network on them 16 at a time on the tensor
@@ -104,32 +104,34 @@ constexpr int kSeg = 30;
 constexpr int kSaThreads = 256;
 
 template <class M, bool SEED>
-__global__ void __launch_bounds__(kSaThreads) thermo_sa_kernel(Geo geo, SaArgs a, long long ncols, int nseg,
-                                                               long long nstreams) {
+__global__ void __launch_bounds__(kSaThreads) thermo_sa_kernel(Geo geo, SaArgs a, long long ncols, int nseg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x & 31;
+  const long long n2 = geo.n2;
+  double* exner_tab = reinterpret_cast<double*>(smraw);  // [n2]
+  for (int k = threadIdx.x; k < n2; k += blockDim.x) exner_tab[k] = pow(a.p0[k] / p_tilde, kappa);
   mlpk::Smem* net = nullptr;
   float* slots = nullptr;
   if constexpr (SEED) {
-    net = reinterpret_cast<mlpk::Smem*>(smraw);
+    net = reinterpret_cast<mlpk::Smem*>(smraw + (n2 * sizeof(double) + 15) / 16 * 16);
     slots = reinterpret_cast<float*>(net + 1) + (size_t)(threadIdx.x >> 5) * thermo_k::kSeedSlotFloats;
     mlpk::stage_weights(*net, a.net.w1, a.net.b1, a.net.w2, a.net.b2, a.net.w3, a.net.b3, threadIdx.x,
                         blockDim.x);
-    __syncthreads();
   }
-  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (gwarp >= nstreams * nseg) return;  // whole warps
-  const int seg = (int)(gwarp % nseg);
-  const long long n2 = geo.n2;
-  const long long k = (long long)seg * kSeg - 1 + lane;
-  const bool kin = k >= 0 && k < n2;
-  const bool own = kin && lane >= 1 && lane <= kSeg;
-  const double p0 = kin ? a.p0[k] : 1.0;
-  const double a0 = kin ? a.alpha0[k] : 1.0;
-  const double exner = pow(p0 / p_tilde, kappa);
+  __syncthreads();
+  const long long ntask = ncols * nseg;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   const double dzi = 1.0 / geo.dx2;
   unsigned long long my_it = 0, my_sat = 0;
-  for (long long col = gwarp / nseg; col < ncols; col += nstreams) {
+  for (long long task = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; task < ntask; task += nwarps) {
+    const long long col = task / nseg;
+    const int seg = (int)(task - col * nseg);
+    const long long k = (long long)seg * kSeg - 1 + lane;
+    const bool kin = k >= 0 && k < n2;
+    const bool own = kin && lane >= 1 && lane <= kSeg;
+    const double p0 = kin ? __ldg(a.p0 + k) : 1.0;
+    const double a0 = kin ? __ldg(a.alpha0 + k) : 1.0;
+    const double exner = kin ? exner_tab[k] : 1.0;
     const long long idx = col * n2 + k;  // columns are contiguous: (i*n1 + j)*n2
     double qt = 0.0, s = 0.0;
     EosStart st{};
@@ -301,7 +303,8 @@ __global__ void thermo_dry_kernel(Geo geo, DryArgs a, long long ncols) {
 
 template <class M, bool SEED>
 cudaError_t launch_sa(const Geo& geo, const SaArgs& a, cudaStream_t st) {
-  const size_t smem = SEED ? thermo_k::seed_smem_bytes(dim3(kSaThreads, 1)) : 0;
+  const size_t smem = (geo.n2 * sizeof(double) + 15) / 16 * 16 +
+                      (SEED ? thermo_k::seed_smem_bytes(dim3(kSaThreads, 1)) : 0);
   if (smem > 48 * 1024) {
     const cudaError_t e =
         cudaFuncSetAttribute(thermo_sa_kernel<M, SEED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -309,17 +312,15 @@ cudaError_t launch_sa(const Geo& geo, const SaArgs& a, cudaStream_t st) {
   }
   const long long ncols = geo.n0 * geo.n1;
   const int nseg = (int)((geo.n2 + kSeg - 1) / kSeg);
-  // resident blocks only; each warp walks its column stream
+  // resident blocks only; their warps stride over the tasks
   int dev = 0, sms = 148, per_sm = 1;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, thermo_sa_kernel<M, SEED>, kSaThreads, smem);
   if (per_sm < 1) per_sm = 1;
-  const long long warps = (long long)sms * per_sm * (kSaThreads / 32);
-  long long nstreams = warps / nseg;
-  if (nstreams < 1) nstreams = 1;
-  if (nstreams > ncols) nstreams = ncols;
-  const long long blocks = (nstreams * nseg + kSaThreads / 32 - 1) / (kSaThreads / 32);
-  thermo_sa_kernel<M, SEED><<<(unsigned)blocks, kSaThreads, smem, st>>>(geo, a, ncols, nseg, nstreams);
+  long long blocks = (long long)sms * per_sm;
+  const long long need = (ncols * nseg + kSaThreads / 32 - 1) / (kSaThreads / 32);
+  if (blocks > need) blocks = need;
+  thermo_sa_kernel<M, SEED><<<(unsigned)blocks, kSaThreads, smem, st>>>(geo, a, ncols, nseg);
   pb_note_launch();
   return cudaGetLastError();
 }
