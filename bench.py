@@ -455,6 +455,66 @@ def run_ours(args, rank, world, local_rank):
     return out, sim
 
 
+def run_accuracy(args, cfg):
+    """Error of the precision forms against the FP64 plain form: the three
+    forms start from the same seeded state and run N steps; per field the
+    relative L2 difference after 1 and N steps.  (The plain form equals the
+    reference's FP64 path to ~1e-13 after one step on the parity grids.)"""
+    import numpy as np
+    import torch
+
+    from pycles_b200.simulation import HotPathSimulation, namelist_for
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    log = lambda m: print(m, file=sys.stderr)
+    n = args.accuracy_steps
+    forms = [("fp64", "fp64", False), ("fp32", "fp32", False)]
+    if cfg["case"] != "dry_cbl" and not args.no_learned:
+        forms.append(("fp32+learned", "fp32", True))
+    fields, rs, trained = None, None, None
+    snaps = {}
+    for form, precision, learned in forms:
+        sim = HotPathSimulation(namelist_for(**cfg, precision=precision), device=dev)
+        if fields is None:
+            fields = sim.initialize(seed=0)
+            rs = sim.RS.profiles()
+        else:
+            sim.set_reference_state(rs)
+            sim.load_fields(fields)
+        if learned:
+            trained = trained or _train_seed(sim, fields, log)
+            if trained is not None:
+                sim.Th.mlp = trained[0]
+        sim.run(0)
+        sim.step()
+        snaps[form] = {1: sim.host_fields()}
+        t0 = time.time()
+        for _ in range(n - 1):
+            sim.step()
+        snaps[form][n] = sim.host_fields()
+        sim.check_device_errors()
+        log(f"{form}: {n} steps in {time.time() - t0:.1f} s")
+        del sim
+        torch.cuda.empty_cache()
+    err = {}
+    for form in snaps:
+        if form == "fp64":
+            continue
+        err[form] = {}
+        for step in (1, n):
+            a, b = snaps[form][step], snaps["fp64"][step]
+            e = {}
+            for name in b:
+                scale = np.linalg.norm(b[name])
+                if name in ("u", "v", "w"):  # components at rest: the velocity field's norm
+                    scale = np.sqrt(sum(np.linalg.norm(b[m]) ** 2 for m in ("u", "v", "w")))
+                e[name] = float(np.linalg.norm(a[name] - b[name]) / scale)
+            err[form][f"after_{step}_steps"] = e
+    return {"accuracy": err, "reference_form": "fp64 plain", "steps": n,
+            "config": {"workload": f"{args.config}: {cfg['nx']}x{cfg['ny']}x{cfg['nz']} cells", **cfg},
+            "norm": "relative L2 per field; u, v, w relative to the norm of the whole velocity field"}
+
+
 def _read_traffic(config, form, component):
     """DRAM bytes per RK stage of a component's kernels, from the committed
     ncu summaries (profiles/*.md lines
@@ -487,6 +547,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cores", type=int, default=None)
+    ap.add_argument("--accuracy-steps", type=int, default=0,
+                    help="instead of timing: run every form N steps from the same state and report each "
+                         "field's relative L2 error against the FP64 plain form after 1 and N steps")
     ap.add_argument("--grid", default=None, metavar="NXxNYxNZ",
                     help="override the configuration's cell counts (orders, gw, case and spacing kept), "
                          "e.g. a reduced case for profiler captures")
@@ -502,6 +565,10 @@ def main():
         nx, ny, nz = (int(t) for t in args.grid.lower().split("x"))
         CONFIGS[args.config] = dict(CONFIGS[args.config], nx=nx, ny=ny, nz=nz)
     cfg = dict(CONFIGS[args.config])
+
+    if args.accuracy_steps > 0:
+        print(json.dumps(run_accuracy(args, cfg)))
+        return 0
 
     if args.impl == "reference":
         if rank != 0:
