@@ -11,6 +11,7 @@
 
 namespace {
 struct ExactMath {
+  static constexpr bool exact = true;  // keep the reference's operations and order
   static __device__ __forceinline__ double exp(double x) { return crm::exp(x); }
   static __device__ __forceinline__ double log(double x) { return crm::log(x); }
 };

@@ -17,6 +17,7 @@ namespace thermo_f {
 using namespace pbc;
 
 struct FastMath {
+  static constexpr bool exact = false;  // free to reorder the reference's expressions
   static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
   static __device__ __forceinline__ double log(double x) { return ::log(x); }
 };
@@ -74,12 +75,39 @@ __device__ __forceinline__ double table_lookup(const pb_table& t, double x, unsi
   return y1 + (x - x1) * (y2 - y1) * t.dxi;
 }
 
-// temperature_no_ql (Csrc/thermodynamics_sa.h:10-15)
+// temperature_no_ql (Csrc/thermodynamics_sa.h:10-15).  The precision form
+// multiplies by 1/p_tilde instead of dividing (FP64 division is a
+// multi-instruction sequence).
 template <class M>
 __device__ __forceinline__ double temperature_no_ql(double pd, double pv, double s, double qt) {
-  return T_tilde * M::exp((s - (1.0 - qt) * (sd_tilde - Rd * M::log(pd / p_tilde)) -
-                           qt * (sv_tilde - Rv * M::log(pv / p_tilde))) /
-                          ((1.0 - qt) * cpd + qt * cpv));
+  if constexpr (M::exact) {
+    return T_tilde * M::exp((s - (1.0 - qt) * (sd_tilde - Rd * M::log(pd / p_tilde)) -
+                             qt * (sv_tilde - Rv * M::log(pv / p_tilde))) /
+                            ((1.0 - qt) * cpd + qt * cpv));
+  } else {
+    constexpr double ipt = 1.0 / p_tilde;
+    return T_tilde * M::exp((s - (1.0 - qt) * (sd_tilde - Rd * M::log(pd * ipt)) -
+                             qt * (sv_tilde - Rv * M::log(pv * ipt))) /
+                            ((1.0 - qt) * cpd + qt * cpv));
+  }
+}
+
+// Entropy of the saturated mixture at temperature T (the secant's s_1, s_2,
+// Csrc/thermodynamics_sa.h:37,54): the reference's operations in the plain
+// form; the precision form evaluates log(T/T_tilde) once for the dry and the
+// vapour parts and multiplies by the constant reciprocals (three logarithms
+// per secant iteration instead of four).
+template <class M>
+__device__ __forceinline__ double entropy_sat(double pd, double pv, double T, double qt, double L, double sigma) {
+  if constexpr (M::exact) {
+    return sd_c<M>(pd, T) * (1.0 - qt) + sv_c<M>(pv, T) * qt + sc_c(L, T) * sigma;
+  } else {
+    constexpr double ipt = 1.0 / p_tilde, iTt = 1.0 / T_tilde;
+    const double lT = M::log(T * iTt);
+    const double sd = sd_tilde + cpd * lT - Rd * M::log(pd * ipt);
+    const double sv = sv_tilde + cpv * lT - Rv * M::log(pv * ipt);
+    return sd * (1.0 - qt) + sv * qt + sc_c(L, T) * sigma;
+  }
 }
 
 // The secant's first point (Csrc/thermodynamics_sa.h:22-24): the temperature
@@ -139,8 +167,7 @@ __device__ __forceinline__ EosOut eos_finish(const pb_table& LT, const EosStart&
   o.sat = true;
   const double sigma_1 = qt - e.qv_star_1;
   const double L_1 = latent_heat(T_1);
-  const double s_1 =
-      sd_c<M>(e.pd_1, T_1) * (1.0 - qt) + sv_c<M>(e.pv_1, T_1) * qt + sc_c(L_1, T_1) * sigma_1;
+  const double s_1 = entropy_sat<M>(e.pd_1, e.pv_1, T_1, qt, L_1, sigma_1);
   double f_1 = s - s_1;
   double T_2 = T_1 + sigma_1 * L_1 / ((1.0 - qt) * cpd + e.qv_star_1 * cpv);
   if (use_seed) T_2 = seed;
@@ -154,7 +181,7 @@ __device__ __forceinline__ EosOut eos_finish(const pb_table& LT, const EosStart&
     const double pd_2 = p0 - pv_2;
     sigma_2 = qt - qv_star_2;
     const double L_2 = latent_heat(T_2);
-    const double s_2 = sd_c<M>(pd_2, T_2) * (1.0 - qt) + sv_c<M>(pv_2, T_2) * qt + sc_c(L_2, T_2) * sigma_2;
+    const double s_2 = entropy_sat<M>(pd_2, pv_2, T_2, qt, L_2, sigma_2);
     const double f_2 = s - s_2;
     const double T_n = T_2 - f_2 * (T_2 - T_1) / (f_2 - f_1);
     T_1 = T_2;
