@@ -1,16 +1,18 @@
 // Learned saturation-adjustment seed: a 3 -> 64 -> 64 -> 1 SiLU MLP.
 //
-// One warp evaluates a tile of 16 samples.  Layer 1 (K = 3) and layer 3
-// (N = 1) run on the FP32 pipes; the 64 x 64 layer runs on the tensor cores
-// with mma.sync m16n8k16 (BF16 operands, FP32 accumulation).  Each lane
-// computes exactly the layer-1 activations that its A fragments hold, so no
-// shuffles or shared memory are needed between layers:
+// One warp evaluates a tile of 16 samples.  Layers 1 and 2 run on the
+// tensor cores with mma.sync m16n8k16 (BF16 operands, FP32 accumulation;
+// layer 1's inputs split into BF16 high and low parts), layer 3 (N = 1) on
+// the FP32 pipes.  Layer 1's accumulator fragments are, after the
+// activation, exactly layer 2's A fragments, so no shuffles or shared memory
+// are needed between layers:
 //   A fragment (16x16, row-major), lane = 4*g + t (g = lane/4, t = lane%4):
 //     regs 0/1/2/3 = rows {g, g+8, g, g+8} x cols {2t, 2t, 2t+8, 2t+8} (+0,+1)
 //   B fragment (16x8, column-major): regs 0/1 = k {2t, 2t+8} (+0,+1), n = g
 //   C fragment (16x8): c0,c1 = row g, cols 2t,2t+1; c2,c3 = row g+8
 // so the C fragments of n-tiles 2kt and 2kt+1 are, reinterpreted, the A
-// fragment of k-tile kt (used by the backward pass).
+// fragment of k-tile kt (used between layers 1 and 2, and by the backward
+// pass).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -57,14 +59,17 @@ __device__ __forceinline__ void mma_bf16_16816(float c[4], const uint32_t a[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// Weights staged in shared memory by the block.  w1b packs layer 1's three
-// weights and bias per unit (one 16-byte load); w2f holds layer 2 in B
-// fragment order, [ntile][ktile][lane] -> {b0, b1}, so each lane's fragment
-// is one conflict-free 8-byte load.
+// Weights staged in shared memory by the block.  Layer 1 runs on the tensor
+// cores too: its A operand is the three inputs split into BF16 high and low
+// parts (columns 0-2 and 3-5, ~16 significant bits per input), so w1f holds
+// the B fragment [ntile][lane] of the 16x64 matrix whose rows 0-2 and 3-5
+// are both W1^T (rows 6-15 zero: only b0 is non-zero); the FP32 bias
+// initialises the accumulator.  w2f holds layer 2 in B fragment order,
+// [ntile][ktile][lane] -> {b0, b1}, so each lane's fragment is one
+// conflict-free 8-byte load.
 struct Smem {
-  float w1[H * 3];
   float b1[H];
-  float4 w1b[H];
+  uint32_t w1f[8 * 32];
   __nv_bfloat16 w2[H * H];  // [n][k]
   uint2 w2f[8 * 4 * 32];
   float b2[H];
@@ -78,13 +83,19 @@ __device__ __forceinline__ void stage_weights(Smem& sm, const __nv_bfloat16* w1,
                                               const __nv_bfloat16* w2, const float* b2, const __nv_bfloat16* w3,
                                               const float* b3, int tid, int nthreads) {
   for (int i = tid; i < H * H; i += nthreads) sm.w2[i] = w2[i];
-  for (int i = tid; i < H * 3; i += nthreads) sm.w1[i] = __bfloat162float(w1[i]);
   for (int i = tid; i < H; i += nthreads) {
     sm.b1[i] = b1[i];
     sm.b2[i] = b2[i];
     sm.w3[i] = __bfloat162float(w3[i]);
-    sm.w1b[i] = make_float4(__bfloat162float(w1[i * 3 + 0]), __bfloat162float(w1[i * 3 + 1]),
-                            __bfloat162float(w1[i * 3 + 2]), b1[i]);
+  }
+  for (int i = tid; i < 8 * 32; i += nthreads) {
+    const int lane = i & 31, nt = i >> 5;
+    const int n = nt * 8 + (lane >> 2), t = lane & 3;
+    // k rows 2t, 2t+1 of [W1^T; W1^T; 0]: row k holds W1[n][k mod 3] for k < 6
+    const int k0 = 2 * t, k1 = 2 * t + 1;
+    const uint16_t lo = k0 < 6 ? *reinterpret_cast<const uint16_t*>(w1 + n * 3 + k0 % 3) : 0;
+    const uint16_t hi = k1 < 6 ? *reinterpret_cast<const uint16_t*>(w1 + n * 3 + k1 % 3) : 0;
+    sm.w1f[i] = (uint32_t)lo | ((uint32_t)hi << 16);
   }
   for (int i = tid; i < 8 * 4 * 32; i += nthreads) {
     const int lane = i & 31, kt = (i >> 5) & 3, nt = i >> 7;
@@ -112,23 +123,39 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
                                              float& y1, Tile* keep) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
+  // layer 1: A = [x_hi, x_lo, 0...] (16 x 16), lane t holds columns 2t, 2t+1
+  uint32_t ax[4] = {0u, 0u, 0u, 0u};
+  {
+    float v0[6], v1[6];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      v0[i] = __bfloat162float(__float2bfloat16_rn(xr0[i]));
+      v0[3 + i] = xr0[i] - v0[i];
+      v1[i] = __bfloat162float(__float2bfloat16_rn(xr1[i]));
+      v1[3 + i] = xr1[i] - v1[i];
+    }
+    if (t < 3) {
+      ax[0] = pack_bf16(v0[2 * t], v0[2 * t + 1]);  // row g
+      ax[1] = pack_bf16(v1[2 * t], v1[2 * t + 1]);  // row g + 8
+    }
+  }
   uint32_t a1[4][4];
 #pragma unroll
-  for (int kt = 0; kt < 4; ++kt) {
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const float* x = (r & 1) ? xr1 : xr0;
-      const int col = kt * 16 + 2 * t + ((r & 2) ? 8 : 0);
-      float h[2];
-#pragma unroll
-      for (int p = 0; p < 2; ++p) {
-        const float4 wb = sm.w1b[col + p];
-        const float z = wb.w + wb.x * x[0] + wb.y * x[1] + wb.z * x[2];
-        if (keep) keep->z1[kt][r][p] = z;
-        h[p] = silu(z);
-      }
-      a1[kt][r] = pack_bf16(h[0], h[1]);
+  for (int nt = 0; nt < 8; ++nt) {
+    const int col = nt * 8 + 2 * t;
+    float c[4] = {sm.b1[col], sm.b1[col + 1], sm.b1[col], sm.b1[col + 1]};
+    const uint32_t b[2] = {sm.w1f[nt * 32 + lane], 0u};
+    mma_bf16_16816(c, ax, b);
+    // C fragments of n-tiles 2kt, 2kt+1 are the A fragment of layer 2's k-tile kt
+    const int kt = nt >> 1, half = nt & 1;
+    if (keep) {
+      keep->z1[kt][half * 2 + 0][0] = c[0];
+      keep->z1[kt][half * 2 + 0][1] = c[1];
+      keep->z1[kt][half * 2 + 1][0] = c[2];
+      keep->z1[kt][half * 2 + 1][1] = c[3];
     }
+    a1[kt][half * 2 + 0] = pack_bf16(silu(c[0]), silu(c[1]));
+    a1[kt][half * 2 + 1] = pack_bf16(silu(c[2]), silu(c[3]));
   }
   if (keep) {
 #pragma unroll
