@@ -477,12 +477,12 @@ template <int ORDER, bool F32>
 cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
   const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
   dim3 blk(32, 4);
-  if (F32) {  // precision form: one pass for the three advecting directions
+  if constexpr (F32) {  // precision form: one pass for the three advecting directions
     momentum_fused<ORDER, F32><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, 4), ceil_div(nl0, kChunk)), blk, 0, st>>>(
         g, a, kChunk);
     pb_note_launch();
     return cudaGetLastError();
-  }
+  } else {
   momentum_march<0, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, kChunk)), blk, 0,
                                   st>>>(g, a, kChunk);
   pb_note_launch();
@@ -494,6 +494,7 @@ cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
   momentum_z<ORDER, F32><<<ceil_div(nwarps, 4), 128, 0, st>>>(g, a, nwarps);
   pb_note_launch();
   return cudaGetLastError();
+  }
 }
 
 }  // namespace

@@ -111,6 +111,49 @@ __device__ __forceinline__ FastF operator-(FastF a, FastF b) { return FastF(a.v 
 __device__ __forceinline__ FastF operator*(FastF a, FastF b) { return FastF(a.v * b.v); }
 __device__ __forceinline__ FastF operator/(FastF a, FastF b) { return FastF(__fdividef(a.v, b.v)); }
 
+// The FP32 interpolants on a stencil shifted by its centre value, with the
+// zero centre folded out by hand: IEEE arithmetic does not let the compiler
+// drop x * 0, and the folded terms are a quarter of the WENO7 work.  Real-
+// arithmetic identical to weno5 / weno7 with phi = 0 (a* = phim*, b* = phip*).
+__device__ __forceinline__ float weno5_c0(float a2, float a1, float b1, float b2) {
+  const float p0 = (1.0f / 3.0f) * a2 - (7.0f / 6.0f) * a1;
+  const float p1 = (-1.0f / 6.0f) * a1 + (1.0f / 3.0f) * b1;
+  const float p2 = (5.0f / 6.0f) * b1 - (1.0f / 6.0f) * b2;
+  const float s2a = b2 - 2.0f * b1, s2b = b2 - 4.0f * b1;
+  const float s1a = a1 + b1, s1b = a1 - b1;
+  const float s0a = a2 - 2.0f * a1, s0b = a2 - 4.0f * a1;
+  const float e0 = (13.0f / 12.0f) * s0a * s0a + 0.25f * s0b * s0b + 1e-10f;
+  const float e1 = (13.0f / 12.0f) * s1a * s1a + 0.25f * s1b * s1b + 1e-10f;
+  const float e2 = (13.0f / 12.0f) * s2a * s2a + 0.25f * s2b * s2b + 1e-10f;
+  const float al0 = __fdividef(0.1f, e0 * e0);
+  const float al1 = __fdividef(0.6f, e1 * e1);
+  const float al2 = __fdividef(0.3f, e2 * e2);
+  const float inv = __fdividef(1.0f, al0 + al1 + al2);
+  return (al0 * inv) * p0 + (al1 * inv) * p1 + (al2 * inv) * p2;
+}
+
+__device__ __forceinline__ float weno7_c0(float a3, float a2, float a1, float b1, float b2, float b3) {
+  const float p0 = -0.25f * a3 + (13.0f / 12.0f) * a2 + (-23.0f / 12.0f) * a1;
+  const float p1 = (1.0f / 12.0f) * a2 + (-5.0f / 12.0f) * a1 + 0.25f * b1;
+  const float p2 = (-1.0f / 12.0f) * a1 + (7.0f / 12.0f) * b1 + (-1.0f / 12.0f) * b2;
+  const float p3 = (13.0f / 12.0f) * b1 + (-5.0f / 12.0f) * b2 + (1.0f / 12.0f) * b3;
+  const float be0 = a3 * (547.0f * a3 - 3882.0f * a2 + 4642.0f * a1) + a2 * (7043.0f * a2 - 17246.0f * a1) +
+                    11003.0f * a1 * a1;
+  const float be1 = a2 * (267.0f * a2 - 1642.0f * a1 - 494.0f * b1) + a1 * (2843.0f * a1 + 1922.0f * b1) +
+                    547.0f * b1 * b1;
+  const float be2 = a1 * (547.0f * a1 + 1922.0f * b1 - 494.0f * b2) + b1 * (2843.0f * b1 - 1642.0f * b2) +
+                    267.0f * b2 * b2;
+  const float be3 = b1 * (11003.0f * b1 - 17246.0f * b2 + 4642.0f * b3) + b2 * (7043.0f * b2 - 3882.0f * b3) +
+                    547.0f * b3 * b3;
+  const float e0 = be0 + 1e-10f, e1 = be1 + 1e-10f, e2 = be2 + 1e-10f, e3 = be3 + 1e-10f;
+  const float al0 = __fdividef(1.0f / 35.0f, e0 * e0);
+  const float al1 = __fdividef(12.0f / 35.0f, e1 * e1);
+  const float al2 = __fdividef(18.0f / 35.0f, e2 * e2);
+  const float al3 = __fdividef(4.0f / 35.0f, e3 * e3);
+  const float inv = __fdividef(1.0f, al0 + al1 + al2 + al3);
+  return (al0 * inv) * p0 + (al1 * inv) * p1 + (al2 * inv) * p2 + (al3 * inv) * p3;
+}
+
 // Face value from a stencil held in an array: ORDER 5 reads v[0..4]
 // (upwind-positive: centre v[2]), ORDER 7 reads v[0..6] (centre v[3]).
 // F32 selects the shifted mixed-precision evaluation described above.
@@ -121,17 +164,15 @@ __device__ __forceinline__ double weno_face(double a0, double a1, double a2, dou
     if constexpr (!F32) {
       return weno5<double>(a0, a1, a2, a3, a4);
     } else {
-      const float r = weno5<FastF>(FastF((float)(a0 - a2)), FastF((float)(a1 - a2)), FastF(0.0f),
-                                   FastF((float)(a3 - a2)), FastF((float)(a4 - a2))).v;
+      const float r = weno5_c0((float)(a0 - a2), (float)(a1 - a2), (float)(a3 - a2), (float)(a4 - a2));
       return a2 + (double)r;
     }
   } else {
     if constexpr (!F32) {
       return weno7<double>(a0, a1, a2, a3, a4, a5, a6);
     } else {
-      const float r = weno7<FastF>(FastF((float)(a0 - a3)), FastF((float)(a1 - a3)), FastF((float)(a2 - a3)),
-                                   FastF(0.0f), FastF((float)(a4 - a3)), FastF((float)(a5 - a3)),
-                                   FastF((float)(a6 - a3))).v;
+      const float r = weno7_c0((float)(a0 - a3), (float)(a1 - a3), (float)(a2 - a3), (float)(a4 - a3),
+                               (float)(a5 - a3), (float)(a6 - a3));
       return a3 + (double)r;
     }
   }
