@@ -40,6 +40,11 @@ class PressureSolver:
 
     def update(self, Gr, RS, DV, PV, PM=None, stream=None):
         """PressureSolver.update (PressureSolver.pyx:38-80)."""
+        self.solve(Gr, RS, DV, PV, stream=stream)
+        PV.update_all_bcs(Gr, PM, stream=stream)
+
+    def solve(self, Gr, RS, DV, PV, stream=None):
+        """PressureSolver.update up to its final ghost fill of PV."""
         nbytes = self._ensure_workspace(Gr, PV.values.device)
         u, v, w = (PV.field(n, Gr) for n in PV.velocity_names_directional)
         rc = _capi.load().pb_pressure_solve(
@@ -48,4 +53,3 @@ class PressureSolver:
             _capi.ptr(DV.field("divergence", Gr)), _capi.ptr(DV.field("dynamic_pressure", Gr)),
             _capi.ptr(self.workspace), nbytes, self.precision, self.refine_sweeps, _capi.stream_handle(stream))
         _capi.check(rc, "pb_pressure_solve")
-        PV.update_all_bcs(Gr, PM, stream=stream)

@@ -109,6 +109,73 @@ class HotPathSimulation:
         for rk in range(self.TS.n_rk_steps):
             self.stage(rk, stream=stream)
 
+    def step_host(self, host_values, stream=None, copy_stream=None):
+        """One time step whose prognostic state lives in pinned host memory,
+        as the reference keeps PV.values in host numpy arrays: the state is
+        copied to the device before the step and back after it.  The copies
+        run variable by variable on a copy stream so that the velocities'
+        upload overlaps the first thermodynamics update (which reads only the
+        scalars) and the scalars' download overlaps the last pressure solve
+        (which changes only the velocities; its ghost fill is restricted to
+        them, the scalars' ghosts being already filled).  Asynchronous:
+        host_values holds the new state once the copy stream has finished.
+        host_values: pinned CPU float64 tensor of nv * npg values."""
+        import torch
+        Gr, PV, DV, RS = self.Gr, self.PV, self.DV, self.RS
+        npg = Gr.dims.npg
+        st = stream if stream is not None else torch.cuda.current_stream(PV.values.device)
+        cs = copy_stream if copy_stream is not None else self._copy_stream()
+        vel = sorted(int(i) for i in PV.velocity_directions)
+        if vel != list(range(len(vel))):
+            raise ValueError("step_host expects the velocities to be the first prognostic variables")
+        nvel, nv = len(vel), PV.nv
+
+        def copy(dst, src, lo, hi):
+            dst[lo * npg:hi * npg].copy_(src[lo * npg:hi * npg], non_blocking=True)
+
+        e_prev = torch.cuda.Event()
+        e_prev.record(st)
+        cs.wait_event(e_prev)  # the previous step's work on PV.values is done
+        with torch.cuda.stream(cs):
+            copy(PV.values, host_values, nvel, nv)   # scalars first
+            e_sc = torch.cuda.Event()
+            e_sc.record(cs)
+            copy(PV.values, host_values, 0, nvel)    # then the velocities
+            e_all = torch.cuda.Event()
+            e_all.record(cs)
+        st.wait_event(e_sc)
+        last = self.TS.n_rk_steps - 1
+        for rk in range(self.TS.n_rk_steps):
+            self.Th.update(Gr, RS, PV, DV, stream=st)
+            if rk == 0:
+                st.wait_event(e_all)
+            self.SA.update(Gr, RS, PV, DV, stream=st)
+            self.MA.update(Gr, RS, PV, stream=st)
+            self.TS.rk_step = rk
+            self.TS.update(Gr, PV, stream=st)
+            PV.Update_all_bcs(Gr, stream=st)
+            if rk < last:
+                self.Pr.update(Gr, RS, DV, PV, stream=st)
+                continue
+            e_sc_done = torch.cuda.Event()
+            e_sc_done.record(st)
+            cs.wait_event(e_sc_done)
+            with torch.cuda.stream(cs):
+                copy(host_values, PV.values, nvel, nv)
+            self.Pr.solve(Gr, RS, DV, PV, stream=st)
+            PV.update_bcs_range(Gr, 0, nvel, stream=st)
+            e_vel_done = torch.cuda.Event()
+            e_vel_done.record(st)
+            cs.wait_event(e_vel_done)
+            with torch.cuda.stream(cs):
+                copy(host_values, PV.values, 0, nvel)
+
+    def _copy_stream(self):
+        import torch
+        if getattr(self, "_cs", None) is None:
+            self._cs = torch.cuda.Stream(device=self.PV.values.device)
+        return self._cs
+
     def run(self, nsteps: int, stream=None):
         """Simulation3d.run: ghost fill and a thermodynamics update before the
         loop (its first output), then nsteps time steps."""

@@ -226,3 +226,23 @@ def test_device_error_flags():
     assert _capi.get_error() & _capi.ERR_TABLE_RANGE
     _capi.clear_error()
     assert _capi.get_error() == 0
+
+
+def test_step_host_equals_device_step():
+    """HotPathSimulation.step_host (state in pinned host memory, copies
+    overlapped with the first thermodynamics update and the last pressure
+    solve) gives the device-resident step's state bit for bit."""
+    import torch
+    nl, rs, f = _setup(MOIST_SMALL, stir=False)
+    a, b = gpu_sim(nl, rs, f), gpu_sim(nl, rs, f)
+    for g in (a, b):
+        g.PV.Update_all_bcs(g.Gr)
+    host = torch.empty(b.PV.values.numel(), dtype=torch.float64, pin_memory=True)
+    host.copy_(b.PV.values)
+    for _ in range(2):
+        a.step()
+        b.step_host(host)
+    torch.cuda.synchronize()
+    ref = a.PV.values.cpu().numpy()
+    assert np.all(np.isfinite(ref))
+    assert np.array_equal(host.numpy(), ref)
