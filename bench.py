@@ -391,7 +391,8 @@ def run_ours(args, rank, world, local_rank):
         a.record(stream)
         for _ in range(args.steps):
             sim.step_host(host, stream=stream)
-        stream.wait_stream(sim._copy_stream())
+        for cs in sim.copy_streams():
+            stream.wait_stream(cs)
         b.record(stream)
         torch.cuda.synchronize()
         te_ms = max_over_ranks(a.elapsed_time(b), dev, world)

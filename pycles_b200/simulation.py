@@ -109,22 +109,26 @@ class HotPathSimulation:
         for rk in range(self.TS.n_rk_steps):
             self.stage(rk, stream=stream)
 
-    def step_host(self, host_values, stream=None, copy_stream=None):
+    def step_host(self, host_values, stream=None):
         """One time step whose prognostic state lives in pinned host memory,
         as the reference keeps PV.values in host numpy arrays: the state is
         copied to the device before the step and back after it.  The copies
-        run variable by variable on a copy stream so that the velocities'
-        upload overlaps the first thermodynamics update (which reads only the
-        scalars) and the scalars' download overlaps the last pressure solve
-        (which changes only the velocities; its ghost fill is restricted to
-        them, the scalars' ghosts being already filled).  Asynchronous:
-        host_values holds the new state once the copy stream has finished.
+        run variable group by variable group on two copy streams (one per
+        direction, so uploads and downloads can use both directions of the
+        link at once): the velocities' upload overlaps the first
+        thermodynamics update (which reads only the scalars), the scalars'
+        download overlaps the last pressure solve (which changes only the
+        velocities; its ghost fill is restricted to them, the scalars' ghosts
+        being already filled), and the next call's scalar upload overlaps
+        this call's velocity download.  Every host region is read only after
+        the download that wrote it.  Asynchronous: host_values holds the new
+        state once `copy_streams()[1]` has finished.
         host_values: pinned CPU float64 tensor of nv * npg values."""
         import torch
         Gr, PV, DV, RS = self.Gr, self.PV, self.DV, self.RS
         npg = Gr.dims.npg
         st = stream if stream is not None else torch.cuda.current_stream(PV.values.device)
-        cs = copy_stream if copy_stream is not None else self._copy_stream()
+        h2d, d2h = self.copy_streams()
         vel = sorted(int(i) for i in PV.velocity_directions)
         if vel != list(range(len(vel))):
             raise ValueError("step_host expects the velocities to be the first prognostic variables")
@@ -133,16 +137,22 @@ class HotPathSimulation:
         def copy(dst, src, lo, hi):
             dst[lo * npg:hi * npg].copy_(src[lo * npg:hi * npg], non_blocking=True)
 
-        e_prev = torch.cuda.Event()
-        e_prev.record(st)
-        cs.wait_event(e_prev)  # the previous step's work on PV.values is done
-        with torch.cuda.stream(cs):
-            copy(PV.values, host_values, nvel, nv)   # scalars first
-            e_sc = torch.cuda.Event()
-            e_sc.record(cs)
-            copy(PV.values, host_values, 0, nvel)    # then the velocities
-            e_all = torch.cuda.Event()
-            e_all.record(cs)
+        def event(stream_):
+            e = torch.cuda.Event()
+            e.record(stream_)
+            return e
+
+        h2d.wait_event(event(st))  # the previous step's work on PV.values is done
+        prev = getattr(self, "_host_events", None)
+        with torch.cuda.stream(h2d):
+            if prev is not None:
+                h2d.wait_event(prev[0])  # the previous scalar download has left PV.values / filled host
+            copy(PV.values, host_values, nvel, nv)
+            e_sc = event(h2d)
+            if prev is not None:
+                h2d.wait_event(prev[1])  # likewise the velocities
+            copy(PV.values, host_values, 0, nvel)
+            e_all = event(h2d)
         st.wait_event(e_sc)
         last = self.TS.n_rk_steps - 1
         for rk in range(self.TS.n_rk_steps):
@@ -157,24 +167,25 @@ class HotPathSimulation:
             if rk < last:
                 self.Pr.update(Gr, RS, DV, PV, stream=st)
                 continue
-            e_sc_done = torch.cuda.Event()
-            e_sc_done.record(st)
-            cs.wait_event(e_sc_done)
-            with torch.cuda.stream(cs):
+            d2h.wait_event(event(st))
+            with torch.cuda.stream(d2h):
                 copy(host_values, PV.values, nvel, nv)
+                e_sc_out = event(d2h)
             self.Pr.solve(Gr, RS, DV, PV, stream=st)
             PV.update_bcs_range(Gr, 0, nvel, stream=st)
-            e_vel_done = torch.cuda.Event()
-            e_vel_done.record(st)
-            cs.wait_event(e_vel_done)
-            with torch.cuda.stream(cs):
+            d2h.wait_event(event(st))
+            with torch.cuda.stream(d2h):
                 copy(host_values, PV.values, 0, nvel)
+                e_vel_out = event(d2h)
+        self._host_events = (e_sc_out, e_vel_out)
 
-    def _copy_stream(self):
+    def copy_streams(self):
+        """The (host->device, device->host) streams of step_host."""
         import torch
-        if getattr(self, "_cs", None) is None:
-            self._cs = torch.cuda.Stream(device=self.PV.values.device)
-        return self._cs
+        if getattr(self, "_copy_streams", None) is None:
+            dev = self.PV.values.device
+            self._copy_streams = (torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev))
+        return self._copy_streams
 
     def run(self, nsteps: int, stream=None):
         """Simulation3d.run: ghost fill and a thermodynamics update before the
