@@ -465,11 +465,32 @@ cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* fl
 template <int ORDER, bool F32>
 cudaError_t launch_scalar_ns(int ns, const Geo& g, ScalarArgs base, double* const* flux_dir[3],
                              const double* const vel[3], cudaStream_t st) {
-  switch (ns) {
-    case 1: return launch_scalar_group<ORDER, F32, 1>(g, base, flux_dir, vel, st);
-    case 2: return launch_scalar_group<ORDER, F32, 2>(g, base, flux_dir, vel, st);
-    case 3: return launch_scalar_group<ORDER, F32, 3>(g, base, flux_dir, vel, st);
-    default: return launch_scalar_group<ORDER, F32, 4>(g, base, flux_dir, vel, st);
+  if constexpr (F32) {
+    // precision form: one scalar per launch keeps the FP32 kernels at ~56
+    // registers (twice the resident warps of the two-scalar windows); the
+    // velocity is read once more per scalar
+    for (int q = 0; q < ns; ++q) {
+      ScalarArgs a = base;
+      a.s[0] = base.s[q];
+      a.t[0] = base.t[q];
+      a.ns = 1;
+      double* fq[3][1];
+      double* const* fd[3];
+      for (int d = 0; d < 3; ++d) {
+        fq[d][0] = flux_dir[d] ? flux_dir[d][q] : nullptr;
+        fd[d] = flux_dir[d] ? fq[d] : nullptr;
+      }
+      const cudaError_t e = launch_scalar_group<ORDER, F32, 1>(g, a, fd, vel, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  } else {
+    switch (ns) {
+      case 1: return launch_scalar_group<ORDER, F32, 1>(g, base, flux_dir, vel, st);
+      case 2: return launch_scalar_group<ORDER, F32, 2>(g, base, flux_dir, vel, st);
+      case 3: return launch_scalar_group<ORDER, F32, 3>(g, base, flux_dir, vel, st);
+      default: return launch_scalar_group<ORDER, F32, 4>(g, base, flux_dir, vel, st);
+    }
   }
 }
 
