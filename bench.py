@@ -72,8 +72,10 @@ COMPONENT_BYTES_PER_CELL = {
 }
 COMPONENT_KERNELS = {
     "thermo": "thermo_sa_kernel (saturation adjustment, buoyancy, bvf, thetali; one launch per stage)",
-    "scalar_adv": "scalar_march x, y + scalar_z (WENO fluxes + divergence, 3 launches per stage)",
-    "momentum_adv": "momentum_march x, y + momentum_z (3 launches per stage)",
+    "scalar_adv": "scalar_march x, y + scalar_z (WENO fluxes + divergence; 3 launches per stage and scalar "
+                  "in the precision form, 3 per stage in the plain form)",
+    "momentum_adv": "momentum_fused in the precision form (1 launch per stage); momentum_march x, y + "
+                    "momentum_z in the plain form (3 launches)",
     "rk3+bcs": "rk3_kernel + ghost_fill_kernel",
     "pressure": "hmean, fft_x_fwd, fft_y, tdma, fft_x_inv (+ refinement), ghost_sym, correction",
 }
@@ -422,11 +424,19 @@ def run_ours(args, rank, world, local_rank):
     comps["scalar_adv+momentum_adv"] = {
         "flops_per_cell_stage": ADV_FLOPS_PER_CELL[flops_key],
         "achieved_tflops": round(ADV_FLOPS_PER_CELL[flops_key] * npl / (adv_ms / 1e3) / 1e12, 2)}
-    top = max(r["component_ms_per_step"], key=lambda c: r["component_ms_per_step"][c])
+    # the headline is the dominant kernel: the single-launch component (one
+    # kernel per RK stage, so its CUDA-event time is that kernel's launch
+    # duration) with the largest time; every component is in "components"
+    single = [c for c in r["component_ms_per_step"] if c == "thermo" or (c == "momentum_adv" and "fp32" in head)]
+    top = max(single, key=lambda c: r["component_ms_per_step"][c])
     roofline = {"bound": "hbm", "achieved": comps[top]["achieved_gbs"], "peak": peak, "unit": "GB/s",
                 "frac": comps[top]["frac"], "traffic": comps[top]["traffic_bytes_per_stage"],
                 "peak_source": peak_kind, "kernel": COMPONENT_KERNELS[top],
                 "algorithmic_bytes_per_cell_stage": comps[top]["algorithmic_bytes_per_cell_stage"],
+                "launch_ms": comps[top]["ms_per_stage"],
+                "note": ("bytes are compulsory bytes per launch over the CUDA-event launch time; "
+                         + ("the thermodynamics is bound by its FP64 transcendentals, not by HBM"
+                            if top == "thermo" else "the fused advection is bound by instruction issue")),
                 "components": comps}
 
     out = None
