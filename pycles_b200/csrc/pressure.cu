@@ -396,14 +396,20 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
     const long long ijk = (g.gw + il) * g.is + j * g.js + k;
     double d;
     if (!RESID) {
-      const double ah = a.alpha0_half[k];
-      d = 0.0;
-      d = add_rn(d, mul_rn(sub_rn(a.u[ijk] / ah, a.u[ijk - g.is] / ah), dxi0));
-      d = add_rn(d, mul_rn(sub_rn(a.v[ijk] / ah, a.v[ijk - g.js] / ah), dxi1));
       // w after remove_mean_u3 (PressureSolver.pyx:113-136), w - mean[k]
       const double wc = sub_rn(a.w[ijk], a.mean[k]);
       const double wm = sub_rn(a.w[ijk - 1], a.mean[k - 1]);
-      d = add_rn(d, mul_rn(sub_rn(wc / a.alpha0[k], wm / a.alpha0[k - 1]), dxi2));
+      if constexpr (sizeof(C) == sizeof(double2)) {  // plain form: the reference's divisions and order
+        const double ah = a.alpha0_half[k];
+        d = 0.0;
+        d = add_rn(d, mul_rn(sub_rn(a.u[ijk] / ah, a.u[ijk - g.is] / ah), dxi0));
+        d = add_rn(d, mul_rn(sub_rn(a.v[ijk] / ah, a.v[ijk - g.js] / ah), dxi1));
+        d = add_rn(d, mul_rn(sub_rn(wc / a.alpha0[k], wm / a.alpha0[k - 1]), dxi2));
+      } else {  // precision form: times rho0 = 1/alpha0 instead of six FP64 divisions
+        const double rh = a.rho0_half[k];
+        d = (a.u[ijk] - a.u[ijk - g.is]) * rh * dxi0 + (a.v[ijk] - a.v[ijk - g.js]) * rh * dxi1 +
+            (wc * a.rho0[k] - wm * a.rho0[k - 1]) * dxi2;
+      }
       a.div[ijk] = d;
     } else {
       const double* p = a.p;
