@@ -108,12 +108,23 @@ __global__ void __launch_bounds__(kSaThreads) thermo_sa_kernel(Geo geo, SaArgs a
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x & 31;
   const long long n2 = geo.n2;
-  double* exner_tab = reinterpret_cast<double*>(smraw);  // [n2]
-  for (int k = threadIdx.x; k < n2; k += blockDim.x) exner_tab[k] = pow(a.p0[k] / p_tilde, kappa);
+  // per level: the Exner function, and for the precision form the
+  // reciprocals of p0, alpha0 and the Exner function (FP64 divisions by
+  // them become multiplications)
+  double* exner_tab = reinterpret_cast<double*>(smraw);  // [n2] (x4 in the precision form)
+  for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+    const double ex = pow(a.p0[k] / p_tilde, kappa);
+    exner_tab[k] = ex;
+    if constexpr (!M::exact) {
+      exner_tab[n2 + k] = 1.0 / ex;
+      exner_tab[2 * n2 + k] = 1.0 / a.p0[k];
+      exner_tab[3 * n2 + k] = 1.0 / a.alpha0[k];
+    }
+  }
   mlpk::Smem* net = nullptr;
   float* slots = nullptr;
   if constexpr (SEED) {
-    net = reinterpret_cast<mlpk::Smem*>(smraw + (n2 * sizeof(double) + 15) / 16 * 16);
+    net = reinterpret_cast<mlpk::Smem*>(smraw + ((M::exact ? 1 : 4) * n2 * sizeof(double) + 15) / 16 * 16);
     slots = reinterpret_cast<float*>(net + 1) + (size_t)(threadIdx.x >> 5) * thermo_k::kSeedSlotFloats;
     mlpk::stage_weights(*net, a.net.w1, a.net.b1, a.net.w2, a.net.b2, a.net.w3, a.net.b3, threadIdx.x,
                         blockDim.x);
@@ -182,11 +193,18 @@ __global__ void __launch_bounds__(kSaThreads) thermo_sa_kernel(Geo geo, SaArgs a
       const EosOut e = eos_finish<M>(a.LT, st, p0, s, qt, a.max_iter, SEED && st.sat, seed, a.err);
       T = e.T;
       qv = e.qv;
-      const double al = alpha_c(p0, T, qt, qv);
-      // bvf_sa first loop (:147-157): theta_rho on k in [1, n2-1)
-      if (k >= 1 && k < n2 - 1) thr = T * (1.0 - qt + eps_vi * qv) / exner;
-      // buoyancy_update_sa first loop (:110-119): k in [0, n2-1)
-      if (k < n2 - 1) b = buoyancy_c(a0, al);
+      double al;
+      if constexpr (M::exact) {
+        al = alpha_c(p0, T, qt, qv);
+        // bvf_sa first loop (:147-157): theta_rho on k in [1, n2-1)
+        if (k >= 1 && k < n2 - 1) thr = T * (1.0 - qt + eps_vi * qv) / exner;
+        // buoyancy_update_sa first loop (:110-119): k in [0, n2-1)
+        if (k < n2 - 1) b = buoyancy_c(a0, al);
+      } else {
+        al = (Rd * T) * exner_tab[2 * n2 + k] * (1.0 - qt + eps_vi * qv);
+        if (k >= 1 && k < n2 - 1) thr = T * (1.0 - qt + eps_vi * qv) * exner_tab[n2 + k];
+        if (k < n2 - 1) b = g * (al - a0) * exner_tab[3 * n2 + k];
+      }
       if (own) {
         if (!isfinite(T)) pb_flag_at(a.err, PB_ERR_NONFINITE);
         my_it += (unsigned long long)e.iters;
@@ -198,7 +216,7 @@ __global__ void __launch_bounds__(kSaThreads) thermo_sa_kernel(Geo geo, SaArgs a
         a.alpha[idx] = al;
         // thetali_update (:185-211) with thetali_c (thermodynamic_functions.h:15-18);
         // without condensate the exponential is exp(-0) = 1 exactly
-        const double theta = T / exner;
+        const double theta = M::exact ? T / exner : T * exner_tab[n2 + k];
         if (e.ql == 0.0 && e.qi == 0.0) {
           a.thetali[idx] = theta * 1.0;
         } else {
@@ -303,7 +321,7 @@ __global__ void thermo_dry_kernel(Geo geo, DryArgs a, long long ncols) {
 
 template <class M, bool SEED>
 cudaError_t launch_sa(const Geo& geo, const SaArgs& a, cudaStream_t st) {
-  const size_t smem = (geo.n2 * sizeof(double) + 15) / 16 * 16 +
+  const size_t smem = ((M::exact ? 1 : 4) * geo.n2 * sizeof(double) + 15) / 16 * 16 +
                       (SEED ? thermo_k::seed_smem_bytes(dim3(kSaThreads, 1)) : 0);
   if (smem > 48 * 1024) {
     const cudaError_t e =
