@@ -40,7 +40,10 @@ __device__ __forceinline__ float tanh_approx(float x) {
   return y;
 }
 __device__ __forceinline__ float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
-__device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
+__device__ __forceinline__ float silu(float z) {  // z/2 + (z/2) tanh(z/2)
+  const float hz = 0.5f * z;
+  return fmaf(hz, tanh_approx(hz), hz);
+}
 __device__ __forceinline__ float silu_grad(float z) {
   const float s = sigmoid(z);
   return s * (1.0f + z * (1.0f - s));
@@ -49,6 +52,17 @@ __device__ __forceinline__ float silu_grad(float z) {
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// Two SiLU activations computed and returned as a BF16 pair (layer 1's
+// activations are BF16 operands of layer 2 anyway): z/2 rounded to BF16,
+// then z/2 + (z/2) tanh(z/2) with the packed BF16 tanh and FMA.
+__device__ __forceinline__ uint32_t silu_bf16x2(float z0, float z1) {
+  const uint32_t hz = pack_bf16(0.5f * z0, 0.5f * z1);
+  uint32_t t, h;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(hz));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(hz), "r"(t));
+  return h;
 }
 
 __device__ __forceinline__ void mma_bf16_16816(float c[4], const uint32_t a[4], const uint32_t b[2]) {
@@ -154,8 +168,8 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
       keep->z1[kt][half * 2 + 1][0] = c[2];
       keep->z1[kt][half * 2 + 1][1] = c[3];
     }
-    a1[kt][half * 2 + 0] = pack_bf16(silu(c[0]), silu(c[1]));
-    a1[kt][half * 2 + 1] = pack_bf16(silu(c[2]), silu(c[3]));
+    a1[kt][half * 2 + 0] = silu_bf16x2(c[0], c[1]);
+    a1[kt][half * 2 + 1] = silu_bf16x2(c[2], c[3]);
   }
   if (keep) {
 #pragma unroll
@@ -166,7 +180,8 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
   float p0 = 0.0f, p1 = 0.0f;
 #pragma unroll
   for (int nt = 0; nt < 8; ++nt) {
-    float c[4] = {0.f, 0.f, 0.f, 0.f};
+    const int c0 = nt * 8 + 2 * t;
+    float c[4] = {sm.b2[c0], sm.b2[c0 + 1], sm.b2[c0], sm.b2[c0 + 1]};  // bias in the accumulator
 #pragma unroll
     for (int kt = 0; kt < 4; ++kt) {
       const uint2 bf = sm.w2f[(nt * 4 + kt) * 32 + lane];
@@ -176,7 +191,7 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int col = nt * 8 + 2 * t + (q & 1);
-      const float z = c[q] + sm.b2[col];
+      const float z = c[q];
       const float h = silu(z);
       if (keep) {
         keep->z2[nt][q] = z;
