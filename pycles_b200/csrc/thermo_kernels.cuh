@@ -104,7 +104,7 @@ constexpr int kSeg = 30;
 constexpr int kSaThreads = 256;
 
 template <class M, bool SEED>
-__global__ void __launch_bounds__(kSaThreads, 3) thermo_sa_kernel(Geo geo, SaArgs a, long long ncols, int nseg) {
+__global__ void __launch_bounds__(kSaThreads, 4) thermo_sa_kernel(Geo geo, SaArgs a, long long ncols, int nseg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x & 31;
   const long long n2 = geo.n2;
