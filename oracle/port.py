@@ -304,7 +304,8 @@ def eos_c(LT: Table, p0, s, qt, max_iter=10_000, T2_seed=None):
     """Vectorised eos_c (Csrc/thermodynamics_sa.h:17-66).
 
     Returns T, qv, ql, qi, iterations.  ``T2_seed`` (optional) replaces the
-    first secant point T_2 of :39 -- the learned-guess variant; the loop
+    first secant point T_2 of :39 -- the learned-guess variant -- clamped to
+    [T_1 + (T_2 - T_1)/16, T_2], the interval that holds the root; the loop
     itself is unchanged.
     """
     p0 = np.asarray(p0, dtype=np.float64)
@@ -339,7 +340,8 @@ def eos_c(LT: Table, p0, s, qt, max_iter=10_000, T2_seed=None):
         f_1 = S - s_1
         t2 = t1 + sigma_1 * L_1 / ((1.0 - Q) * cpd + qvs1 * cpv)
         if T2_seed is not None:
-            t2 = np.asarray(T2_seed, dtype=np.float64).reshape(-1)[sat].copy()
+            guess = np.asarray(T2_seed, dtype=np.float64).reshape(-1)[sat]
+            t2 = np.fmin(np.fmax(guess, t1 + 0.0625 * (t2 - t1)), t2)
         out_T = np.empty_like(t1)
         out_qv = np.empty_like(t1)
         out_sig = np.empty_like(t1)

@@ -1,10 +1,23 @@
 // Anelastic pressure solve on one GPU.
 //
 // The reference's pencil transposes (ParallelMPI.Pencil) become a choice of
-// layout: the spectral work array is W[k][j][i] (complex, i fastest), so
-// the x-FFT reads physical rows and writes contiguous i, the y-FFT works on
-// j-lines batched over contiguous i, and the Thomas solver gives one thread
-// to each (kx,ky) column with consecutive threads on consecutive i.
+// layout: the spectral work array is W[k][j][m] (complex, m fastest), so
+// the x-FFT reads physical rows and writes contiguous m, the y-FFT works on
+// j-lines batched over contiguous m, and the Thomas solver gives one thread
+// to each (kx,ky) column with consecutive threads on consecutive m.
+//
+// The reference transforms the real right-hand side with a complex FFT and
+// solves every (kx,ky) column.  The field is real, so the x-spectrum of each
+// row is Hermitian, X[n0 - m] = conj(X[m]); the tridiagonal matrix is real
+// and depends on kx only through kx^2, which is even in m; so the columns
+// m > n0/2 hold the conjugates of the columns n0 - m (with ky reflected) and
+// carry no information.  W keeps the n0/2 + 1 columns m = 0..n0/2.  Two real
+// rows (levels 2p, 2p+1) share one complex FFT, z = a + i b, and are
+// separated by A[m] = (Z[m] + conj Z[n0-m]) / 2, B[m] = (Z[m] - conj Z[n0-m]) / 2i;
+// the inverse rebuilds Z = A + i B over all m from the stored half and
+// returns a = Re z, b = Im z.  This halves the x-FFT work, and the y-FFT,
+// Thomas and spectral-array traffic, with the same mathematics as the
+// reference's full-spectrum solve.
 //
 //   hmean_partial/hmean_final  HorizontalMean(w), deterministic two-pass sum
 //   (remove_mean_u3)           w -= mean[k] on every cell, applied where w is
@@ -50,8 +63,9 @@ PLayout playout(const pb_dims* d) {
   L.twyf = off;    off += align256(n1 * 8);
   L.kx2 = off;     off += align256(n0 * 8);
   L.ky2 = off;     off += align256(n1 * 8);
-  L.spec = off;    off += align256(n0 * n1 * n2 * 16);
-  L.scr = off;     off += align256(n0 * n1 * n2 * 8);
+  // spectral array W[k][j][m], m < n0/2 + 1 (Hermitian half in x)
+  L.spec = off;    off += align256((n0 / 2 + 1) * n1 * n2 * 16);
+  L.scr = off;     off += align256((n0 / 2 + 1) * n1 * n2 * 8);
   L.total = off;
   return L;
 }
@@ -368,7 +382,8 @@ __global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
 }
 
 // ---- divergence (or refinement residual) + forward x-FFT --------------------
-// block = (interior j, chunk of KC interior levels); smem KC lines of n0.
+// block = (interior j, chunk of KC = 2 LC interior levels); smem LC complex
+// lines of n0, line p holding levels 2p (real part) and 2p + 1 (imaginary).
 // RESID = false: the right-hand side is second_order_divergence
 //   (PressureSolver.pyx:138-175, d = 0, 1, 2 in order), written to `div`.
 // RESID = true: the right-hand side is the residual div - A p of the current
@@ -378,20 +393,29 @@ __global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
 //   precision form.
 template <class C, bool RESID>
 __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC) {
+  using R = decltype(C().x);
   extern __shared__ __align__(16) unsigned char smraw[];
   C* in = reinterpret_cast<C*>(smraw);
+  R* inr = reinterpret_cast<R*>(smraw);
   const int N = (int)(g.n0 - 2 * g.gw);
+  const int Nh = N / 2 + 1;
   const int nz = (int)(g.n2 - 2 * g.gw);
   const int jl = blockIdx.x;
   const int k0 = blockIdx.y * KC;
   const int kc = min(KC, nz - k0);
+  const int lc = (kc + 1) >> 1;
   const long long j = g.gw + jl;
   const int ld = line_ld(N);
   const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
+#pragma unroll 4
   for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
     int kl, il;
     split_idx(e, KC, il, kl);
-    if (kl >= kc) continue;
+    const int slot = 2 * ((kl >> 1) * ld + swz(il)) + (kl & 1);
+    if (kl >= kc) {  // the imaginary half of an odd chunk's last line
+      inr[slot] = (R)0;
+      continue;
+    }
     const long long k = g.gw + k0 + kl;
     const long long ijk = (g.gw + il) * g.is + j * g.js + k;
     double d;
@@ -422,31 +446,45 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
       if (kk > 0) vert -= a.rho0[k - 1] * (pc - p[ijk - 1]);
       d = a.div[ijk] - (lap_h + vert * (dxi2 * dxi2));
     }
-    in[kl * ld + swz(il)] = creal<C>(d);
+    inr[slot] = (R)d;
   }
   __syncthreads();
-  const C* res = fft_lines<C>(in, kc, KC, N, twx_of<C>(a), false);
+  const C* res = fft_lines<C>(in, lc, KC >> 1, N, twx_of<C>(a), false);
+  // separate the two rows of each line; write the columns m = 0..N/2
   C* spec = reinterpret_cast<C*>(a.spec);
-  const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
-  for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
-    int kl, il;
-    split_idx(e, N, kl, il);
-    spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il] = res[kl * ld + swz(il)];
+  const long long nxy = (long long)Nh * (g.n1 - 2 * g.gw);
+  const R half = (R)0.5;
+  for (int e = threadIdx.x; e < Nh * kc; e += blockDim.x) {
+    const int kl = e / Nh;
+    const int m = e - kl * Nh;
+    const C* line = res + (kl >> 1) * ld;
+    const C z = line[swz(m)];
+    const C zr = line[swz(m == 0 ? 0 : N - m)];  // Z[N - m]
+    C o;
+    if ((kl & 1) == 0) {  // A = (Z[m] + conj Z[N-m]) / 2
+      o.x = (z.x + zr.x) * half;
+      o.y = (z.y - zr.y) * half;
+    } else {              // B = (Z[m] - conj Z[N-m]) / 2i
+      o.x = (z.y + zr.y) * half;
+      o.y = (zr.x - z.x) * half;
+    }
+    spec[(long long)(k0 + kl) * nxy + (long long)jl * Nh + m] = o;
   }
 }
 
-// ---- y-FFT over W[k][j][i] lines along j, IC columns i per block ----------
+// ---- y-FFT over W[k][j][m] lines along j, IC columns m per block ----------
 template <class C>
 __global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, bool inverse) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* in = reinterpret_cast<C*>(smraw);
-  const int Nx = (int)(g.n0 - 2 * g.gw);
+  const int Nx = (int)(g.n0 - 2 * g.gw) / 2 + 1;  // stored x-modes
   const int N = (int)(g.n1 - 2 * g.gw);
   const int kk = blockIdx.y;
   const int i0 = blockIdx.x * IC;
   const int ic = min(IC, Nx - i0);
   const int ld = line_ld(N);
   C* plane = reinterpret_cast<C*>(a.spec) + (long long)kk * N * Nx;
+#pragma unroll 4
   for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
     int il, jl;
     split_idx(e, IC, jl, il);
@@ -483,7 +521,7 @@ template <> __device__ __forceinline__ float2 from_d<float2>(double x, double y)
 // real and imaginary parts (the matrix is real, so both share m and scratch).
 template <class C>
 __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
-  const int Nx = (int)(g.n0 - 2 * g.gw);
+  const int Nx = (int)(g.n0 - 2 * g.gw) / 2 + 1;  // stored x-modes
   const int Ny = (int)(g.n1 - 2 * g.gw);
   const int nz = (int)(g.n2 - 2 * g.gw);
   const long long ncol = (long long)Nx * Ny;
@@ -597,25 +635,45 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
 }
 
 // ---- inverse x-FFT -> pressure (ACC: add to the current pressure) ----------
+// block = (interior j, chunk of KC = 2 LC levels).  Line p gets
+// Z = A + i B over all m, A and B the stored half-spectra of levels 2p and
+// 2p + 1 extended by A[N-m] = conj A[m]; the inverse transform returns the
+// two real rows as Re z and Im z.
 template <class C, bool ACC>
 __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* in = reinterpret_cast<C*>(smraw);
   const int N = (int)(g.n0 - 2 * g.gw);
+  const int Nh = N / 2 + 1;
   const int nz = (int)(g.n2 - 2 * g.gw);
   const int jl = blockIdx.x;
   const int k0 = blockIdx.y * KC;
   const int kc = min(KC, nz - k0);
+  const int lc = (kc + 1) >> 1;
   const int ld = line_ld(N);
   const C* spec = reinterpret_cast<const C*>(a.spec);
-  const long long nxy = (long long)N * (g.n1 - 2 * g.gw);
-  for (int e = threadIdx.x; e < N * kc; e += blockDim.x) {
-    int kl, il;
-    split_idx(e, N, kl, il);
-    in[kl * ld + swz(il)] = spec[(long long)(k0 + kl) * nxy + (long long)jl * N + il];
+  const long long nxy = (long long)Nh * (g.n1 - 2 * g.gw);
+#pragma unroll 4
+  for (int e = threadIdx.x; e < Nh * lc; e += blockDim.x) {
+    const int p = e / Nh;
+    const int m = e - p * Nh;
+    const long long src = (long long)(k0 + 2 * p) * nxy + (long long)jl * Nh + m;
+    const C A = spec[src];
+    const C B = (2 * p + 1 < kc) ? spec[src + nxy] : czero<C>();
+    C* line = in + p * ld;
+    C z;
+    z.x = A.x - B.y;
+    z.y = A.y + B.x;
+    line[swz(m)] = z;
+    if (m >= 1 && m <= N - Nh) {  // Z[N-m] = conj A[m] + i conj B[m]
+      C zr;
+      zr.x = A.x + B.y;
+      zr.y = B.x - A.y;
+      line[swz(N - m)] = zr;
+    }
   }
   __syncthreads();
-  const C* res = fft_lines<C>(in, kc, KC, N, twx_of<C>(a), true);
+  const C* res = fft_lines<C>(in, lc, KC >> 1, N, twx_of<C>(a), true);
   const double sc = 1.0 / (double)N;
   const long long j = g.gw + jl;
   for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
@@ -623,7 +681,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
     split_idx(e, KC, il, kl);
     if (kl >= kc) continue;
     const long long ijk = (g.gw + il) * g.is + j * g.js + g.gw + k0 + kl;
-    const double val = (double)res[kl * ld + swz(il)].x * sc;
+    const C z = res[(kl >> 1) * ld + swz(il)];
+    const double val = (double)((kl & 1) ? z.y : z.x) * sc;
     if (ACC) a.p[ijk] += val;
     else a.p[ijk] = val;
   }
@@ -746,8 +805,10 @@ extern "C" int pb_pressure_init(const pb_dims* dims, void* workspace, long long 
 template <class C>
 static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t st) {
   const long long Nx = g.n0 - 2 * g.gw, Ny = g.n1 - 2 * g.gw, nz = g.n2 - 2 * g.gw;
-  const int KC = lines_for(Nx, sizeof(C));
-  const size_t smx = fft_smem(Nx, KC, sizeof(C));
+  const long long Nh = Nx / 2 + 1;  // stored x-modes
+  const int LC = lines_for(Nx, sizeof(C));  // complex lines per x-FFT block
+  const int KC = 2 * LC;                    // levels per x-FFT block (two per line)
+  const size_t smx = fft_smem(Nx, LC, sizeof(C));
   const int IC = lines_for(Ny, sizeof(C));
   const size_t smy = fft_smem(Ny, IC, sizeof(C));
   if (smx > 48 * 1024) {
@@ -759,7 +820,7 @@ static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t 
   if (smy > 48 * 1024)
     PB_CUDA_TRY(cudaFuncSetAttribute(fft_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
   const dim3 gx((unsigned)Ny, ceil_div(nz, KC));
-  const dim3 gy(ceil_div(Nx, IC), (unsigned)nz);
+  const dim3 gy(ceil_div(Nh, IC), (unsigned)nz);
   if (resid)
     fft_x_fwd<C, true><<<gx, kFftThreads, smx, st>>>(g, a, KC);
   else
@@ -769,7 +830,7 @@ static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t 
   fft_y<C><<<gy, kFftThreads, smy, st>>>(g, a, IC, false);
   pb_note_launch();
   PB_LAUNCH_CHECK();
-  tdma_kernel<C><<<ceil_div(Nx * Ny, 256), 256, 0, st>>>(g, a);
+  tdma_kernel<C><<<ceil_div(Nh * Ny, 256), 256, 0, st>>>(g, a);
   pb_note_launch();
   PB_LAUNCH_CHECK();
   fft_y<C><<<gy, kFftThreads, smy, st>>>(g, a, IC, true);

@@ -149,7 +149,12 @@ __device__ __forceinline__ EosStart eos_start(const pb_table& LT, double p0, dou
 // capped at max_iter (the reference loops without a cap), reaching the cap
 // sets PB_ERR_SECANT_CAP.  use_seed replaces the second secant point T_2
 // (:39) by a learned guess; the loop and its stopping test stay the
-// reference's.
+// reference's.  The root lies between T_1 (no condensate) and the
+// reference's T_2 (all of sigma_1 condensed at T_1's latent heat) -- over
+// saturated states at 700-1020 hPa it sits at 0.20-0.87 of that interval --
+// so the guess is clamped to [T_1 + (T_2 - T_1)/16, T_2]: a good guess is
+// untouched, a wild one (or NaN) cannot take the secant off the saturation
+// table, and T_2 != T_1 keeps the first secant step defined.
 template <class M>
 __device__ __forceinline__ EosOut eos_finish(const pb_table& LT, const EosStart& e, double p0, double s, double qt,
                                              int max_iter, bool use_seed, double seed, unsigned int* err) {
@@ -170,7 +175,7 @@ __device__ __forceinline__ EosOut eos_finish(const pb_table& LT, const EosStart&
   const double s_1 = entropy_sat<M>(e.pd_1, e.pv_1, T_1, qt, L_1, sigma_1);
   double f_1 = s - s_1;
   double T_2 = T_1 + sigma_1 * L_1 / ((1.0 - qt) * cpd + e.qv_star_1 * cpv);
-  if (use_seed) T_2 = seed;
+  if (use_seed) T_2 = fmin(fmax(seed, T_1 + 0.0625 * (T_2 - T_1)), T_2);
   double delta_T;
   double qv_star_2, sigma_2;
   int it = 0;

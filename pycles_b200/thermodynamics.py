@@ -162,8 +162,9 @@ def eos_sa_host(CC, p0, s, qt, T2_seed=None, max_iter=100):
         s1 = _sd(pd_1[sat], t1) * (1.0 - Q) + _sv(pv_1[sat], t1) * Q + (-L1 / t1) * sig1
         f1 = S - s1
         t2 = t1 + sig1 * L1 / ((1.0 - Q) * cpd + q1 * cpv)
-        if T2_seed is not None:
-            t2 = np.asarray(T2_seed, dtype=np.float64).ravel()[sat].copy()
+        if T2_seed is not None:  # clamped to the bracket of the root, as on the device
+            guess = np.asarray(T2_seed, dtype=np.float64).ravel()[sat]
+            t2 = np.fmin(np.fmax(guess, t1 + 0.0625 * (t2 - t1)), t2)
         outT = t2.copy()
         outs = np.zeros_like(t2)
         outit = np.zeros(t2.shape, dtype=np.int64)

@@ -24,6 +24,9 @@ MOIST_W7 = dict(case="bomex", nx=12, ny=16, nz=18, dx=100.0, dy=100.0, dz=40.0, 
                 scalar_order=7, momentum_order=7)
 DRY_SMALL = dict(case="dry_cbl", nx=16, ny=16, nz=16, dx=50.0, dy=50.0, dz=50.0, gw=3, dt=0.5)
 ODD = dict(case="bomex", nx=12, ny=10, nz=14, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
+# odd nx (no Nyquist column in the half spectrum) and odd nz (the last
+# packed pair of levels of the x-FFT has one row)
+ODD_XZ = dict(case="bomex", nx=9, ny=10, nz=13, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
 
 
 def _stir(fields, seed=1, amp=0.5):
@@ -162,7 +165,7 @@ def test_rk3_stages():
         assert float(g.PV.tendencies.abs().max()) == 0.0
 
 
-@pytest.mark.parametrize("cfg", [MOIST_SMALL, ODD, DRY_SMALL], ids=["pow2ish", "odd", "dry"])
+@pytest.mark.parametrize("cfg", [MOIST_SMALL, ODD, ODD_XZ, DRY_SMALL], ids=["pow2ish", "odd", "odd_xz", "dry"])
 def test_pressure(cfg):
     nl, rs, f = _setup(cfg)
     o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)
