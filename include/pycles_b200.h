@@ -267,8 +267,8 @@ int pb_pressure_init(const pb_dims* dims, void* workspace, long long workspace_b
  * second_order_pressure_correction (:83-110).
  *   workspace : >= pb_pressure_workspace_bytes(dims) bytes, 256-byte aligned,
  *               initialised by pb_pressure_init.
- *   n[0], n[1] : powers of two up to 8192 (Stockham radix-8 FFTs), other
- *                sizes up to 1024 (direct DFT).
+ *   n[0], n[1] : powers of two up to 4096 (Stockham radix-8 FFTs), other
+ *                sizes up to 1024 (direct DFT); PB_ERR_UNSUPPORTED otherwise.
  *   precision  : PB_FP64 -- the reference method in FP64 (refine_sweeps
  *                ignored).  PB_FP32 -- the precision form: FFTs in FP32,
  *                tridiagonal solves in FP64, then refine_sweeps (0..8)

@@ -72,6 +72,11 @@ PLayout playout(const pb_dims* d) {
 
 __device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 
+// Lines per FFT block for a power-of-two length 2^lg (16 lines, or fewer so
+// that a block's passes hold nlines * N <= 16 * kFftThreads elements); the
+// host's lines_for gives the same count for every power of two.
+__host__ __device__ constexpr int ct_lines(int lg) { return (16 * 256 >> lg) < 16 ? (16 * 256 >> lg) : 16; }
+
 // Complex arithmetic on double2 (plain form) or float2 (precision form).
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -150,7 +155,9 @@ __device__ __forceinline__ void dft8(C* v, bool inverse) {
 // every thread reads its items (R values each, stride N/R), twiddles them by
 // exp(-+2 pi i (j mod Ns) r / (Ns R)), transforms, and after a barrier
 // writes them to (j div Ns) Ns R + (j mod Ns) + r Ns.  Input and output are
-// in natural order.  Needs nlines * N <= 16 * blockDim.x.
+// in natural order.  Needs nlines * N <= 16 * kFftThreads (the FFT kernels'
+// block size).  When lgN, lgNs and nlines are compile-time constants (the
+// kernels instantiated for one length) all index arithmetic folds away.
 template <class C, int R>
 __device__ __forceinline__ void stockham_pass(C* buf, int nlines, int lgN, int lgNs, const C* __restrict__ tw,
                                               bool inverse) {
@@ -166,7 +173,7 @@ __device__ __forceinline__ void stockham_pass(C* buf, int nlines, int lgN, int l
   C v[MAXI][R];
 #pragma unroll
   for (int it = 0; it < MAXI; ++it) {
-    const int b = threadIdx.x + it * blockDim.x;
+    const int b = threadIdx.x + it * kFftThreads;
     if (b < total) {
       const int l = b >> lg_per;
       const int j = b & (per_line - 1);
@@ -190,7 +197,7 @@ __device__ __forceinline__ void stockham_pass(C* buf, int nlines, int lgN, int l
   __syncthreads();
 #pragma unroll
   for (int it = 0; it < MAXI; ++it) {
-    const int b = threadIdx.x + it * blockDim.x;
+    const int b = threadIdx.x + it * kFftThreads;
     if (b < total) {
       const int l = b >> lg_per;
       const int j = b & (per_line - 1);
@@ -206,13 +213,11 @@ __device__ __forceinline__ void stockham_pass(C* buf, int nlines, int lgN, int l
 
 // Power-of-two N: radix-8 passes, then one radix-4 or radix-2 pass.
 template <class C>
-__device__ void fft_lines_pow2(C* buf, int nlines, int N, const C* __restrict__ tw, bool inverse) {
+__device__ __forceinline__ void fft_lines_pow2(C* buf, int nlines, int N, const C* __restrict__ tw, bool inverse) {
   const int lgN = __ffs(N) - 1;
   int lgNs = 0;
-  while (lgNs + 3 <= lgN) {
-    stockham_pass<C, 8>(buf, nlines, lgN, lgNs, tw, inverse);
-    lgNs += 3;
-  }
+#pragma unroll
+  for (; lgNs + 3 <= lgN; lgNs += 3) stockham_pass<C, 8>(buf, nlines, lgN, lgNs, tw, inverse);
   if (lgNs + 2 == lgN) stockham_pass<C, 4>(buf, nlines, lgN, lgNs, tw, inverse);
   else if (lgNs + 1 == lgN) stockham_pass<C, 2>(buf, nlines, lgN, lgNs, tw, inverse);
 }
@@ -235,7 +240,7 @@ __device__ __forceinline__ void split_idx(int e, int d, int& q, int& r) {
 template <class C>
 __device__ void dft_lines(const C* in, C* out, int nlines, int N, const C* __restrict__ tw, bool inverse) {
   const int ld = line_ld(N);
-  for (int e = threadIdx.x; e < nlines * N; e += blockDim.x) {
+  for (int e = threadIdx.x; e < nlines * N; e += kFftThreads) {
     const int line = e / N;
     const int m = e - line * N;
     C acc = czero<C>();
@@ -391,13 +396,19 @@ __global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
 //   differences in x and y, the rows of compute_off_diagonals /
 //   compute_diagonal in z); used by the iterative refinement of the
 //   precision form.
-template <class C, bool RESID>
-__global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC) {
+//
+// LGN > 0 instantiates the kernel for N = 2^LGN (KC = 2 ct_lines(LGN)), so
+// that the index arithmetic and the FFT passes are compile-time; LGN = 0
+// takes N and KC at run time.
+template <class C, bool RESID, int LGN>
+__global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KCrt) {
   using R = decltype(C().x);
+  constexpr bool CT = LGN > 0;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* in = reinterpret_cast<C*>(smraw);
   R* inr = reinterpret_cast<R*>(smraw);
-  const int N = (int)(g.n0 - 2 * g.gw);
+  const int N = CT ? (1 << LGN) : (int)(g.n0 - 2 * g.gw);
+  const int KC = CT ? 2 * ct_lines(LGN) : KCrt;
   const int Nh = N / 2 + 1;
   const int nz = (int)(g.n2 - 2 * g.gw);
   const int jl = blockIdx.x;
@@ -408,7 +419,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
   const int ld = line_ld(N);
   const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
 #pragma unroll 4
-  for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
+  for (int e = threadIdx.x; e < N * KC; e += kFftThreads) {
     int kl, il;
     split_idx(e, KC, il, kl);
     const int slot = 2 * ((kl >> 1) * ld + swz(il)) + (kl & 1);
@@ -449,12 +460,13 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
     inr[slot] = (R)d;
   }
   __syncthreads();
-  const C* res = fft_lines<C>(in, lc, KC >> 1, N, twx_of<C>(a), false);
+  const C* res = fft_lines<C>(in, CT ? (KC >> 1) : lc, KC >> 1, N, twx_of<C>(a), false);
   // separate the two rows of each line; write the columns m = 0..N/2
   C* spec = reinterpret_cast<C*>(a.spec);
   const long long nxy = (long long)Nh * (g.n1 - 2 * g.gw);
   const R half = (R)0.5;
-  for (int e = threadIdx.x; e < Nh * kc; e += blockDim.x) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < Nh * kc; e += kFftThreads) {
     const int kl = e / Nh;
     const int m = e - kl * Nh;
     const C* line = res + (kl >> 1) * ld;
@@ -473,33 +485,37 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KC)
 }
 
 // ---- y-FFT over W[k][j][m] lines along j, IC columns m per block ----------
-template <class C>
-__global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int IC, bool inverse) {
+// (LGN as for fft_x_fwd: N = 2^LGN and IC = ct_lines(LGN) at compile time.)
+template <class C, bool INV, int LGN>
+__global__ void __launch_bounds__(kFftThreads) fft_y(Geo g, PArgs a, int ICrt) {
+  constexpr bool CT = LGN > 0;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* in = reinterpret_cast<C*>(smraw);
   const int Nx = (int)(g.n0 - 2 * g.gw) / 2 + 1;  // stored x-modes
-  const int N = (int)(g.n1 - 2 * g.gw);
+  const int N = CT ? (1 << LGN) : (int)(g.n1 - 2 * g.gw);
+  const int IC = CT ? ct_lines(LGN) : ICrt;
   const int kk = blockIdx.y;
   const int i0 = blockIdx.x * IC;
   const int ic = min(IC, Nx - i0);
   const int ld = line_ld(N);
   C* plane = reinterpret_cast<C*>(a.spec) + (long long)kk * N * Nx;
 #pragma unroll 4
-  for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
+  for (int e = threadIdx.x; e < N * IC; e += kFftThreads) {
     int il, jl;
     split_idx(e, IC, jl, il);
     if (il >= ic) continue;
     in[il * ld + swz(jl)] = plane[(long long)jl * Nx + i0 + il];
   }
   __syncthreads();
-  const C* res = fft_lines<C>(in, ic, IC, N, twy_of<C>(a), inverse);
-  const double sc = inverse ? 1.0 / (double)N : 1.0;
-  for (int e = threadIdx.x; e < N * IC; e += blockDim.x) {
+  const C* res = fft_lines<C>(in, CT ? IC : ic, IC, N, twy_of<C>(a), INV);
+  const double sc = INV ? 1.0 / (double)N : 1.0;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * IC; e += kFftThreads) {
     int il, jl;
     split_idx(e, IC, jl, il);
     if (il >= ic) continue;
     C r = res[il * ld + swz(jl)];
-    if (inverse) {
+    if (INV) {
       r.x *= sc;
       r.y *= sc;
     }
@@ -639,11 +655,14 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
 // Z = A + i B over all m, A and B the stored half-spectra of levels 2p and
 // 2p + 1 extended by A[N-m] = conj A[m]; the inverse transform returns the
 // two real rows as Re z and Im z.
-template <class C, bool ACC>
-__global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC) {
+// (LGN as for fft_x_fwd.)
+template <class C, bool ACC, int LGN>
+__global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KCrt) {
+  constexpr bool CT = LGN > 0;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* in = reinterpret_cast<C*>(smraw);
-  const int N = (int)(g.n0 - 2 * g.gw);
+  const int N = CT ? (1 << LGN) : (int)(g.n0 - 2 * g.gw);
+  const int KC = CT ? 2 * ct_lines(LGN) : KCrt;
   const int Nh = N / 2 + 1;
   const int nz = (int)(g.n2 - 2 * g.gw);
   const int jl = blockIdx.x;
@@ -654,7 +673,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
   const C* spec = reinterpret_cast<const C*>(a.spec);
   const long long nxy = (long long)Nh * (g.n1 - 2 * g.gw);
 #pragma unroll 4
-  for (int e = threadIdx.x; e < Nh * lc; e += blockDim.x) {
+  for (int e = threadIdx.x; e < Nh * lc; e += kFftThreads) {
     const int p = e / Nh;
     const int m = e - p * Nh;
     const long long src = (long long)(k0 + 2 * p) * nxy + (long long)jl * Nh + m;
@@ -673,10 +692,11 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KC)
     }
   }
   __syncthreads();
-  const C* res = fft_lines<C>(in, lc, KC >> 1, N, twx_of<C>(a), true);
+  const C* res = fft_lines<C>(in, CT ? (KC >> 1) : lc, KC >> 1, N, twx_of<C>(a), true);
   const double sc = 1.0 / (double)N;
   const long long j = g.gw + jl;
-  for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * KC; e += kFftThreads) {
     int kl, il;
     split_idx(e, KC, il, kl);
     if (kl >= kc) continue;
@@ -738,6 +758,17 @@ int stream_blocks(long long work) {
 }
 
 bool pow2(long long n) { return (n & (n - 1)) == 0; }
+
+// Horizontal sizes the line FFTs support: powers of two up to 4096 (a
+// block's Stockham passes hold at most 16 * kFftThreads elements, one line of
+// 4096) and other lengths up to 1024 (direct DFT).
+bool fft_sizes_ok(const pb_dims* d) {
+  for (int dim = 0; dim < 2; ++dim) {
+    const long long n = d->n[dim];
+    if (pow2(n) ? n > 4096 : n > 1024) return false;
+  }
+  return true;
+}
 
 size_t fft_smem(long long N, int lines, size_t elem) {
   return (size_t)(pow2(N) ? 1 : 2) * (size_t)line_ld((int)N) * lines * elem;
@@ -802,6 +833,71 @@ extern "C" int pb_pressure_init(const pb_dims* dims, void* workspace, long long 
   return PB_OK;
 }
 
+// log2 of a length that has compile-time FFT kernels (128 ... 1024), else 0
+int ct_lg(long long n) {
+  if (!pow2(n) || n < 128 || n > 1024) return 0;
+  int lg = 0;
+  while ((1LL << lg) < n) ++lg;
+  return lg;
+}
+
+template <class C, int LG>
+static int launch_x_fwd(const Geo& g, PArgs& a, bool resid, dim3 grid, size_t sm, int KC, cudaStream_t st) {
+  if (sm > 48 * 1024) {
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, false, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if constexpr (sizeof(C) == 8)
+      PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, true, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  }
+  if constexpr (sizeof(C) == 8) {  // the refinement residual exists in the precision form only
+    if (resid) {
+      fft_x_fwd<C, true, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
+      return PB_OK;
+    }
+  }
+  fft_x_fwd<C, false, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
+  return PB_OK;
+}
+
+template <class C, int LG>
+static int launch_x_inv(const Geo& g, PArgs& a, bool acc, dim3 grid, size_t sm, int KC, cudaStream_t st) {
+  if (sm > 48 * 1024) {
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, false, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if constexpr (sizeof(C) == 8)
+      PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, true, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  }
+  if constexpr (sizeof(C) == 8) {
+    if (acc) {
+      fft_x_inv<C, true, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
+      return PB_OK;
+    }
+  }
+  fft_x_inv<C, false, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
+  return PB_OK;
+}
+
+template <class C, int LG>
+static int launch_y(const Geo& g, PArgs& a, bool inverse, dim3 grid, size_t sm, int IC, cudaStream_t st) {
+  if (sm > 48 * 1024) {
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_y<C, false, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_y<C, true, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  }
+  if (inverse)
+    fft_y<C, true, LG><<<grid, kFftThreads, sm, st>>>(g, a, IC);
+  else
+    fft_y<C, false, LG><<<grid, kFftThreads, sm, st>>>(g, a, IC);
+  return PB_OK;
+}
+
+// Dispatch on a length's compile-time instantiation (LG = 0: run-time length).
+#define PB_FFT_DISPATCH(lg, call)         \
+  switch (lg) {                           \
+    case 7: { constexpr int L_ = 7; call; } break;   \
+    case 8: { constexpr int L_ = 8; call; } break;   \
+    case 9: { constexpr int L_ = 9; call; } break;   \
+    case 10: { constexpr int L_ = 10; call; } break; \
+    default: { constexpr int L_ = 0; call; } break;  \
+  }
+
 template <class C>
 static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t st) {
   const long long Nx = g.n0 - 2 * g.gw, Ny = g.n1 - 2 * g.gw, nz = g.n2 - 2 * g.gw;
@@ -811,39 +907,33 @@ static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t 
   const size_t smx = fft_smem(Nx, LC, sizeof(C));
   const int IC = lines_for(Ny, sizeof(C));
   const size_t smy = fft_smem(Ny, IC, sizeof(C));
-  if (smx > 48 * 1024) {
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-  }
-  if (smy > 48 * 1024)
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+  const int lgx = ct_lg(Nx), lgy = ct_lg(Ny);
+  if ((lgx && LC != ct_lines(lgx)) || (lgy && IC != ct_lines(lgy))) return PB_ERR_UNSUPPORTED;
   const dim3 gx((unsigned)Ny, ceil_div(nz, KC));
   const dim3 gy(ceil_div(Nh, IC), (unsigned)nz);
-  if (resid)
-    fft_x_fwd<C, true><<<gx, kFftThreads, smx, st>>>(g, a, KC);
-  else
-    fft_x_fwd<C, false><<<gx, kFftThreads, smx, st>>>(g, a, KC);
+  int rc = PB_OK;
+  PB_FFT_DISPATCH(lgx, rc = (launch_x_fwd<C, L_>(g, a, resid, gx, smx, KC, st)));
+  if (rc) return rc;
   pb_note_launch();
   PB_LAUNCH_CHECK();
-  fft_y<C><<<gy, kFftThreads, smy, st>>>(g, a, IC, false);
+  PB_FFT_DISPATCH(lgy, rc = (launch_y<C, L_>(g, a, false, gy, smy, IC, st)));
+  if (rc) return rc;
   pb_note_launch();
   PB_LAUNCH_CHECK();
   tdma_kernel<C><<<ceil_div(Nh * Ny, 256), 256, 0, st>>>(g, a);
   pb_note_launch();
   PB_LAUNCH_CHECK();
-  fft_y<C><<<gy, kFftThreads, smy, st>>>(g, a, IC, true);
+  PB_FFT_DISPATCH(lgy, rc = (launch_y<C, L_>(g, a, true, gy, smy, IC, st)));
+  if (rc) return rc;
   pb_note_launch();
   PB_LAUNCH_CHECK();
-  if (acc)
-    fft_x_inv<C, true><<<gx, kFftThreads, smx, st>>>(g, a, KC);
-  else
-    fft_x_inv<C, false><<<gx, kFftThreads, smx, st>>>(g, a, KC);
+  PB_FFT_DISPATCH(lgx, rc = (launch_x_inv<C, L_>(g, a, acc, gx, smx, KC, st)));
+  if (rc) return rc;
   pb_note_launch();
   PB_LAUNCH_CHECK();
   return PB_OK;
 }
+#undef PB_FFT_DISPATCH
 
 static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const double* rho0_half,
                                const double* alpha0, const double* alpha0_half, double* u, double* v, double* w,
@@ -923,8 +1013,7 @@ extern "C" int pb_pressure_solve(const pb_dims* dims, const double* rho0, const 
   const PLayout L = playout(dims);
   if (!workspace || workspace_bytes < L.total) return PB_ERR_WORKSPACE;
   if (reinterpret_cast<uintptr_t>(workspace) & 255) return PB_ERR_WORKSPACE;
-  if ((!pow2(dims->n[0]) && dims->n[0] > 1024) || (!pow2(dims->n[1]) && dims->n[1] > 1024)) return PB_ERR_UNSUPPORTED;
-  if (dims->n[0] > 8192 || dims->n[1] > 8192) return PB_ERR_UNSUPPORTED;
+  if (!fft_sizes_ok(dims)) return PB_ERR_UNSUPPORTED;
   return pressure_solve_impl(dims, rho0, rho0_half, alpha0, alpha0_half, u, v, w, divergence, dynamic_pressure,
                              static_cast<char*>(workspace), precision, refine_sweeps, as_stream(stream));
 }

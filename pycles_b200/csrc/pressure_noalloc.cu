@@ -58,7 +58,7 @@ extern "C" int pb_pressure_solve_noalloc(const pb_dims* dims, const double* rho0
     return PB_ERR_ARG;
   const long long need = pb_pressure_workspace_bytes(dims);
   if (need < 0 || need > PB_PRESSURE_NOALLOC_MAX_BYTES) return PB_ERR_WORKSPACE;
-  if ((!pow2(dims->n[0]) && dims->n[0] > 1024) || (!pow2(dims->n[1]) && dims->n[1] > 1024)) return PB_ERR_UNSUPPORTED;
+  if (!fft_sizes_ok(dims)) return PB_ERR_UNSUPPORTED;
   int dev = 0;
   PB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return PB_ERR_UNSUPPORTED;

@@ -27,6 +27,9 @@ ODD = dict(case="bomex", nx=12, ny=10, nz=14, dx=100.0, dy=100.0, dz=40.0, gw=3,
 # odd nx (no Nyquist column in the half spectrum) and odd nz (the last
 # packed pair of levels of the x-FFT has one row)
 ODD_XZ = dict(case="bomex", nx=9, ny=10, nz=13, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
+# lengths with compile-time FFT kernels (128 ... 1024), odd nz
+FFT_CT = dict(case="bomex", nx=256, ny=128, nz=7, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
+FFT_CT_WIDE = dict(case="bomex", nx=512, ny=1024, nz=3, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0)
 
 
 def _stir(fields, seed=1, amp=0.5):
@@ -165,7 +168,8 @@ def test_rk3_stages():
         assert float(g.PV.tendencies.abs().max()) == 0.0
 
 
-@pytest.mark.parametrize("cfg", [MOIST_SMALL, ODD, ODD_XZ, DRY_SMALL], ids=["pow2ish", "odd", "odd_xz", "dry"])
+@pytest.mark.parametrize("cfg", [MOIST_SMALL, ODD, ODD_XZ, DRY_SMALL, FFT_CT, FFT_CT_WIDE],
+                         ids=["pow2ish", "odd", "odd_xz", "dry", "fft_ct", "fft_ct_wide"])
 def test_pressure(cfg):
     nl, rs, f = _setup(cfg)
     o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f)

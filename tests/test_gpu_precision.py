@@ -50,7 +50,11 @@ def _levels_demeaned(p, d):
     return P - P.mean(axis=(0, 1), keepdims=True)
 
 
-def test_fp32_pressure_refinement_converges():
+MOIST_FFT_CT = dict(MOIST, nx=256, ny=128, nz=12)  # compile-time FFT kernels
+
+
+@pytest.mark.parametrize("cfg", [MOIST, MOIST_FFT_CT], ids=["runtime_fft", "ct_fft"])
+def test_fp32_pressure_refinement_converges(cfg):
     """Refinement computes the residual div - A p in FP64 and solves for the
     correction with the FP32 transforms.  The solver projects out the (0,0)
     horizontal mode (the reference zeroes it), so refinement cannot correct
@@ -60,7 +64,7 @@ def test_fp32_pressure_refinement_converges():
     solve's remove_mean_u3 removes.  Everything else must converge to the FP64
     solution."""
     from helpers import oracle_dims
-    nl, rs, f = host_case(**MOIST)
+    nl, rs, f = host_case(**cfg)
     f = _stir(f)
     o = oracle_sim(nl, rs, f)
     o.update_all_bcs()
@@ -80,7 +84,7 @@ def test_fp32_pressure_refinement_converges():
     print("pressure vs FP64 by refinement sweeps: raw", raw, "level means removed", demeaned)
     assert demeaned[0] < 1e-5
     assert demeaned[1] < demeaned[0] * 1e-4
-    assert demeaned[2] < 1e-12
+    assert demeaned[2] < 1e-11  # FP64 level: the plain form's own pressure tolerance
     assert max(raw) < 1e-5 and raw[2] < 1e-7
 
 
