@@ -12,7 +12,7 @@
 // k on the lanes; lane L computes the flux of face f = k0-1+L and takes the
 // flux of face f-1 from lane L-1 by shuffle (31 cells per warp).  The
 // precision form's momentum advection runs all three directions in one pass
-// instead (momentum_fused).
+// instead (momentum_tile).
 //
 // Order of the tendency updates per variable is the reference's: d = 0, 1, 2
 // (ScalarAdvection.pyx:81, MomentumAdvection.pyx:56-60), each
@@ -111,18 +111,14 @@ __global__ void __launch_bounds__(128) scalar_march(Geo g, ScalarArgs a, int chu
 // scalars, z direction
 // ---------------------------------------------------------------------------
 template <int ORDER, bool F32, int NS>
-__global__ void __launch_bounds__(128) scalar_z(Geo g, ScalarArgs a, long long nwarps) {
+__global__ void __launch_bounds__(128) scalar_z(Geo g, ScalarArgs a) {
   constexpr int R = St<ORDER>::R;
   const int lane = threadIdx.x & 31;
-  const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (wid >= nwarps) return;
-  const long long nl1 = g.n1 - 2 * g.gw;
-  const long long nl2 = g.n2 - 2 * g.gw;
-  const long long nseg = (nl2 + 30) / 31;
-  const long long seg = wid % nseg;
-  const long long rest = wid / nseg;
-  const long long j = g.gw + rest % nl1;
-  const long long i = g.gw + rest / nl1;
+  // grid (segment, group of 4 rows, x): warp w of the block takes row 4*blockIdx.y + w
+  const long long seg = blockIdx.x;
+  const long long j = g.gw + (long long)blockIdx.y * 4 + (threadIdx.x >> 5);
+  const long long i = g.gw + (long long)blockIdx.z;
+  if (j >= g.n1 - g.gw) return;  // whole warps
   const long long f = g.gw + seg * 31 - 1 + lane;   // face of this lane = cell of this lane
   const bool valid = f <= g.n2 - g.gw - 1;
   const long long col = i * g.is + j * g.js;
@@ -142,6 +138,111 @@ __global__ void __launch_bounds__(128) scalar_z(Geo g, ScalarArgs a, long long n
     const double Fm = __shfl_up_sync(0xffffffffu, F, 1);
     if (valid && lane > 0) a.t[q][col + f] -= a.alpha0_half[f] * (F - Fm) * dzi;
   }
+}
+
+// ---------------------------------------------------------------------------
+// scalars, precision form: first-difference windows
+// ---------------------------------------------------------------------------
+// x / y: the marching thread keeps the FP32 first differences of the face's
+// stencil (2R-1 of them) and the FP64 values phi[f .. f+R] (the possible
+// centres, now and for the next R faces); each new cell costs one FP64
+// subtraction and one rounding to FP32.  Face flux vel * phi_face * rho, the
+// tendency update t -= (alpha dxi) (F - F_prev).
+template <int D, int ORDER>
+__global__ void __launch_bounds__(128) scalar_march_f32(Geo g, ScalarArgs a, int chunk) {
+  constexpr int R = St<ORDER>::R;
+  constexpr int ND = 2 * R - 1;
+  const long long k = g.gw + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long o = g.gw + (long long)blockIdx.y * blockDim.y + threadIdx.y;
+  const long long nD = (D == 0) ? g.n0 : g.n1;
+  const long long nO = (D == 0) ? g.n1 : g.n0;
+  if (k >= g.n2 - g.gw || o >= nO - g.gw) return;
+  const long long sD = (D == 0) ? g.is : g.js;
+  const long long sO = (D == 0) ? g.js : g.is;
+  const long long c0 = g.gw + (long long)blockIdx.z * chunk;
+  if (c0 >= nD - g.gw) return;
+  const long long c1 = min(c0 + (long long)chunk, nD - g.gw);
+  const double* __restrict__ phi = a.s[0] + o * sO + k;
+  const double* __restrict__ vel = a.vel + o * sO + k;
+  double* __restrict__ tend = a.t[0] + o * sO + k;
+  double* __restrict__ flux = a.flux[0] ? a.flux[0] + o * sO + k : nullptr;
+  const double rho = a.rho0_half[k];
+  const double ad = a.alpha0_half[k] * ((D == 0) ? g.dxi0 : g.dxi1);
+
+  // first face f = c0 - 1 reads phi[f-R+1 .. f+R]
+  float d[ND];
+  double ph[R + 1];  // phi[f .. f+R]
+  {
+    double w[2 * R];
+#pragma unroll
+    for (int m = 0; m < 2 * R; ++m) w[m] = phi[(c0 - R + m) * sD];
+#pragma unroll
+    for (int m = 0; m < ND; ++m) d[m] = (float)(w[m + 1] - w[m]);
+#pragma unroll
+    for (int m = 0; m <= R; ++m) ph[m] = w[R - 1 + m];
+  }
+  double nxt = phi[(c0 + R) * sD];
+  double vnxt = vel[(c0 - 1) * sD];
+  double tnxt = tend[c0 * sD];
+  double fprev = 0.0;
+  for (long long f = c0 - 1; f < c1; ++f) {
+    const double u = vnxt;
+    const double lead = nxt;
+    const double t = tnxt;
+    // prefetch: the next face's velocity and tendency, and the cell the
+    // window takes on after the next face (none after the last face: phi
+    // stays in bounds)
+    if (f + 1 < c1) {
+      vnxt = vel[(f + 1) * sD];
+      tnxt = tend[(f + 1) * sD];
+    }
+    if (f + 2 < c1) nxt = phi[(f + 2 + R) * sD];
+    const bool pos = u >= 0.0;
+    const float r = weno_delta<ORDER>(pos, d);
+    const double F = u * ((pos ? ph[0] : ph[1]) + (double)r) * rho;
+    if (f >= c0) tend[f * sD] = fma(-ad, F - fprev, t);
+    if (flux != nullptr) flux[f * sD] = F;
+    fprev = F;
+#pragma unroll
+    for (int m = 0; m < ND - 1; ++m) d[m] = d[m + 1];
+    d[ND - 1] = (float)(lead - ph[R]);
+#pragma unroll
+    for (int m = 0; m < R; ++m) ph[m] = ph[m + 1];
+    ph[R] = lead;
+  }
+}
+
+// z: lane L takes face f = k0 - 1 + L from the 2R values around it (L1
+// hits: the warp's lanes overlap) and the lower face's flux from lane L-1.
+template <int ORDER>
+__global__ void __launch_bounds__(128) scalar_z_f32(Geo g, ScalarArgs a) {
+  constexpr int R = St<ORDER>::R;
+  constexpr int ND = 2 * R - 1;
+  const int lane = threadIdx.x & 31;
+  // grid (segment, group of 4 rows, x): warp w of the block takes row 4*blockIdx.y + w
+  const long long seg = blockIdx.x;
+  const long long j = g.gw + (long long)blockIdx.y * 4 + (threadIdx.x >> 5);
+  const long long i = g.gw + (long long)blockIdx.z;
+  if (j >= g.n1 - g.gw) return;  // whole warps
+  const long long f = g.gw + seg * 31 - 1 + lane;
+  const bool valid = f <= g.n2 - g.gw - 1;
+  const long long col = i * g.is + j * g.js;
+  double F = 0.0;
+  if (valid) {
+    const double* s = a.s[0] + col + f - (R - 1);
+    double w[2 * R];
+#pragma unroll
+    for (int m = 0; m < 2 * R; ++m) w[m] = s[m];
+    float d[ND];
+#pragma unroll
+    for (int m = 0; m < ND; ++m) d[m] = (float)(w[m + 1] - w[m]);
+    const double u = a.vel[col + f];
+    const bool pos = u >= 0.0;
+    F = u * ((pos ? w[R - 1] : w[R]) + (double)weno_delta<ORDER>(pos, d)) * a.rho0[f];
+    if (a.flux[0] != nullptr) a.flux[0][col + f] = F;
+  }
+  const double Fm = __shfl_up_sync(0xffffffffu, F, 1);
+  if (valid && lane > 0) a.t[0][col + f] = fma(-a.alpha0_half[f] * g.dxi2, F - Fm, a.t[0][col + f]);
 }
 
 // ---------------------------------------------------------------------------
@@ -226,17 +327,13 @@ __global__ void __launch_bounds__(128) momentum_march(Geo g, MomArgs a, int chun
 // momentum, z direction (advecting velocity = w)
 // ---------------------------------------------------------------------------
 template <int ORDER, bool F32>
-__global__ void __launch_bounds__(128) momentum_z(Geo g, MomArgs a, long long nwarps) {
+__global__ void __launch_bounds__(128) momentum_z(Geo g, MomArgs a) {
   const int lane = threadIdx.x & 31;
-  const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (wid >= nwarps) return;
-  const long long nl1 = g.n1 - 2 * g.gw;
-  const long long nl2 = g.n2 - 2 * g.gw;
-  const long long nseg = (nl2 + 30) / 31;
-  const long long seg = wid % nseg;
-  const long long rest = wid / nseg;
-  const long long j = g.gw + rest % nl1;
-  const long long i = g.gw + rest / nl1;
+  // grid (segment, group of 4 rows, x): warp w of the block takes row 4*blockIdx.y + w
+  const long long seg = blockIdx.x;
+  const long long j = g.gw + (long long)blockIdx.y * 4 + (threadIdx.x >> 5);
+  const long long i = g.gw + (long long)blockIdx.z;
+  if (j >= g.n1 - g.gw) return;  // whole warps
   const long long f = g.gw + seg * 31 - 1 + lane;
   const bool valid = f <= g.n2 - g.gw - 1;
   const long long idx = i * g.is + j * g.js + f;
@@ -270,159 +367,239 @@ __global__ void __launch_bounds__(128) momentum_z(Geo g, MomArgs a, long long nw
 }
 
 // ---------------------------------------------------------------------------
-// momentum, all three advecting directions in one pass (precision form)
+// momentum, precision form: the three advecting directions in one pass
 // ---------------------------------------------------------------------------
-// Block (32, 4): lane L holds level k = k0 - 1 + L (lanes 1..31 are cells,
-// lane 0 the level below), threadIdx.y the row j; every thread marches along
-// x over a chunk of cells.  Per cell and advected component: the x face flux
-// from the register window (the previous face kept in a register), the two
-// y face fluxes from the row's neighbours (L1-cached loads), the z face flux
-// of the lane's upper face with the lower one from lane L-1 by shuffle.  The
-// x windows also give the x neighbours that the y and z faces'
-// advecting-velocity interpolations need (v and w along x); the rest comes
-// from L1-cached loads.  Each tendency gets its x, y and z terms in the
-// reference's order and is read and written once, so u, v, w and the three
-// tendencies cross DRAM about once per stage instead of three times; the
-// y faces are evaluated twice (once by each neighbouring cell), which costs
-// less than a shared-memory exchange with its barriers (measured: 4.9 ms
-// per stage for the three split launches, 4.6-4.9 fused, 512x512x256).
-template <int ORDER, bool F32>
-__device__ __forceinline__ double interp_c(const double* p) {  // p[0 .. ORDER-2]: the interpolant's points
+// A block of TJ + 1 warps marches along x over a chunk of cells.  Warp w
+// holds row j = j0 - 1 + w (w = 0 is the row below the block's cells and
+// only supplies the y face j0 - 1/2), lane L level k = k0 - 1 + L (lane 0
+// only supplies the z face k0 - 1/2): TJ x 31 cells per x step.  Per x
+// position f and advected component c:
+//   x face  from the thread's register window along x (FP32 first
+//           differences + the FP64 values phi[f-HI .. f+R]), the face
+//           below kept from the previous step;
+//   y face  j+1/2 from the y-z plane of u, v, w at x = f in shared memory
+//           (the block's rows and levels with a halo of R); the face j-1/2
+//           is the upper face of the warp below, through shared memory;
+//   z face  k+1/2 from the plane; the face k-1/2 from lane L-1 by shuffle.
+// Every face is evaluated once, every global load is issued one step ahead
+// of its use, and each tendency is read and written once per stage with the
+// x, y and z terms subtracted in the reference's order.  The advecting
+// velocity of each face is the reference's interpolant
+// (momentum_advection_weno.h:145-236), in FP64; the WENO runs on FP32 first
+// differences (weno_delta) and the flux vel * phi * rho in FP64.
+template <int ORDER>
+struct MomTile {
+  static constexpr int R = St<ORDER>::R;
+  static constexpr int NI = ORDER - 1;         // points of the advecting-velocity interpolant
+  static constexpr int HI = NI / 2 - 1;        // it reads offsets -HI .. NI-1-HI from the face's lower cell
+  static constexpr int TJ = 15;                // cell rows per block (16 warps)
+  static constexpr int NW = TJ + 1;            // warps
+  static constexpr int NT = NW * 32;           // threads
+  static constexpr int NR = TJ + 2 * R;        // plane rows j0-R .. j0+TJ+R-1
+  static constexpr int NK = 31 + 2 * R;        // plane levels k0-R .. k0+30+R
+  static constexpr int NKP = NK + 1;           // plane row length
+  static constexpr int PLANE = NR * NKP;
+  static constexpr int NHALO = NR * NK - NT;   // plane entries no thread owns
+  static constexpr int HPT = (NHALO + NT - 1) / NT;
+  static constexpr int NX = HI + 1 + R;        // FP64 window values phi[f-HI .. f+R]
+};
+
+template <int ORDER>
+__device__ __forceinline__ double interp_n(const double* p) {  // p[0 .. NI-1]
   if constexpr (ORDER == 5)
     return interp_4<double>(p[0], p[1], p[2], p[3]);
   else
     return interp_6<double>(p[0], p[1], p[2], p[3], p[4], p[5]);
 }
 
-template <int ORDER, bool F32>
-__global__ void __launch_bounds__(128) momentum_fused(Geo g, MomArgs a, int chunk) {
-  constexpr int R = St<ORDER>::R;
-  constexpr int W = St<ORDER>::W;
-  constexpr int NI = ORDER - 1;  // points of the advecting-velocity interpolant (4 or 6)
-  constexpr int HI = NI / 2 - 1; // it reads offsets -HI .. NI-1-HI around the face's lower cell
-  const int lane = threadIdx.x;
-  const long long k = g.gw - 1 + (long long)blockIdx.x * 31 + lane;
-  const long long j = g.gw + (long long)blockIdx.y * blockDim.y + threadIdx.y;
-  if (j >= g.n1 - g.gw) return;  // whole warps
+template <int ORDER>
+__global__ void __launch_bounds__(MomTile<ORDER>::NT, 1) momentum_tile(Geo g, MomArgs a, int chunk) {
+  using T = MomTile<ORDER>;
+  constexpr int R = T::R, NI = T::NI, HI = T::HI, NX = T::NX, NKP = T::NKP;
+  constexpr int ND = 2 * R - 1;
+  __shared__ double plane[3][T::PLANE];
+  __shared__ double fy[3][T::NW][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long k0 = g.gw + (long long)blockIdx.x * 31;
+  const long long j0 = g.gw + (long long)blockIdx.y * T::TJ;
+  const long long k = k0 - 1 + lane, j = j0 - 1 + w;
   const long long c0 = g.gw + (long long)blockIdx.z * chunk;
   const long long c1 = min(c0 + (long long)chunk, g.n0 - g.gw);
-  const bool face_ok = k <= g.n2 - g.gw - 1;
-  const bool cell = face_ok && lane >= 1;
-  const long long base = j * g.js + k;
-  const double rho_h = face_ok ? a.rho0_half[k] : 0.0;
-  const double rho_f = face_ok ? a.rho0[k] : 0.0;
-  const double rho_h1 = face_ok ? a.rho0_half[k + 1] : 0.0;
-  const double al_h = face_ok ? a.alpha0_half[k] : 0.0;
-  const double al_f = face_ok ? a.alpha0[k] : 0.0;
-  const double dxi = g.dxi0, dyi = g.dxi1, dzi = g.dxi2;
-  const double* __restrict__ U = a.vel[0];
-  const double* __restrict__ V = a.vel[1];
-  const double* __restrict__ Wv = a.vel[2];
+  const bool own_ok = j < g.n1 && k < g.n2;  // j, k >= gw - 1 >= 0
+  const bool cell = w >= 1 && lane >= 1 && j <= g.n1 - g.gw - 1 && k <= g.n2 - g.gw - 1;
+  const int rs = w - 1 + R, ls = lane - 1 + R;  // this thread's plane row and level
+  const int me = rs * NKP + ls;
+  const int jk = (int)(j * g.js + k);  // offset within an x plane (n1 * n2 < 2^31)
 
-  double win[3][W];
-  double fprev[3];
-  double nxt[3];
+  // halo entries of this thread: plane index and offset within an x plane
+  // (-1: none, or outside the arrays; such entries are zero and are read by
+  // no cell of the domain)
+  int hs[T::HPT], hg[T::HPT];
+#pragma unroll
+  for (int q = 0; q < T::HPT; ++q) {
+    const int h = threadIdx.x + q * T::NT;
+    hs[q] = -1;
+    hg[q] = -1;
+    if (h < T::NHALO) {
+      constexpr int A = (R - 1) * T::NK, BW = T::NK - 32, B = T::NW * BW;
+      int r, l;
+      if (h < A) {
+        r = h / T::NK;
+        l = h - r * T::NK;
+      } else if (h < A + B) {
+        const int t = h - A;
+        r = R - 1 + t / BW;
+        const int m = t - (t / BW) * BW;
+        l = (m < R - 1) ? m : m + 32;
+      } else {
+        const int t = h - A - B;
+        r = R - 1 + T::NW + t / T::NK;
+        l = t - (t / T::NK) * T::NK;
+      }
+      hs[q] = r * NKP + l;
+      const long long jj = j0 - R + r, kk = k0 - R + l;
+      if (jj < g.n1 && kk < g.n2) hg[q] = (int)(jj * g.js + kk);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < T::HPT; ++q)
+    if (hs[q] >= 0 && hg[q] < 0)
+      for (int c = 0; c < 3; ++c) plane[c][hs[q]] = 0.0;
+
+  const double rho_h = own_ok ? a.rho0_half[k] : 0.0;  // the halo row and level supply faces too
+  const double rho_f = own_ok ? a.rho0[k] : 0.0;
+  const double rho_h1 = (own_ok && k + 1 < g.n2) ? a.rho0_half[k + 1] : 0.0;
+  const double al_h = cell ? a.alpha0_half[k] : 0.0, al_f = cell ? a.alpha0[k] : 0.0;
+
+  // x windows: face f = c0 - 1 reads phi[f-R+1 .. f+R]
+  float dl[3][ND];
+  double ph[3][NX];  // phi[f-HI .. f+R]
+  double nxt[3], hv[3][T::HPT], tcur[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
+    double wv[2 * R];
 #pragma unroll
-    for (int m = 0; m < W - 1; ++m) win[c][m] = face_ok ? a.vel[c][(c0 - R + m) * g.is + base] : 0.0;
-    nxt[c] = face_ok ? a.vel[c][(c0 - 1 + R) * g.is + base] : 0.0;
-    fprev[c] = 0.0;
+    for (int m = 0; m < 2 * R; ++m) wv[m] = own_ok ? a.vel[c][(c0 - R + m) * g.is + jk] : 0.0;
+#pragma unroll
+    for (int m = 0; m < ND; ++m) dl[c][m] = (float)(wv[m + 1] - wv[m]);
+#pragma unroll
+    for (int n = 0; n < NX; ++n) ph[c][n] = wv[R - 1 - HI + n];
+    nxt[c] = own_ok ? a.vel[c][(c0 + R) * g.is + jk] : 0.0;
+#pragma unroll
+    for (int q = 0; q < T::HPT; ++q) hv[c][q] = hg[q] >= 0 ? a.vel[c][(c0 - 1) * g.is + hg[q]] : 0.0;
+    tcur[c] = cell ? a.tend[c][c0 * g.is + jk] : 0.0;
   }
+  double fxp[3] = {0.0, 0.0, 0.0};
+
   for (long long f = c0 - 1; f < c1; ++f) {
-    const long long idx = f * g.is + base;
-    const bool more = f + 1 < c1;
-    const bool upd = f >= c0;
+    // (a) the plane at x = f
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      win[c][W - 1] = nxt[c];
-      if (more && face_ok) nxt[c] = a.vel[c][(f + 1 + R) * g.is + base];
+      plane[c][me] = ph[c][HI];
+#pragma unroll
+      for (int q = 0; q < T::HPT; ++q)
+        if (hg[q] >= 0) plane[c][hs[q]] = hv[c][q];
     }
-    // window entry m holds x index f - R + 1 + m: the interpolant points
-    // f - HI .. f - HI + NI - 1 start at m = R - 1 - HI
-    constexpr int MI = R - 1 - HI;
+    // (b) loads for the next steps
+    double lead[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      lead[c] = nxt[c];
+      if (f + 1 < c1) {
+#pragma unroll
+        for (int q = 0; q < T::HPT; ++q)
+          if (hg[q] >= 0) hv[c][q] = a.vel[c][(f + 1) * g.is + hg[q]];
+      }
+      if (f + 2 < c1 && own_ok) nxt[c] = a.vel[c][(f + 2 + R) * g.is + jk];
+    }
+    __syncthreads();
+    const double* PU = plane[0];
+    const double* PV = plane[1];
+    const double* PW = plane[2];
+    // (c) x faces f+1/2
     double Fx[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      double vel_adv = 0.0;
-      if (c == 0) {
-        vel_adv = interp_c<ORDER, F32>(&win[0][MI]);
-      } else if (face_ok) {
-        const long long st = (c == 1) ? g.js : 1;
-        double p[NI];
+      double p[NI];
 #pragma unroll
-        for (int m = 0; m < NI; ++m) p[m] = U[idx + (m - HI) * st];
-        vel_adv = interp_c<ORDER, F32>(p);
-      }
-      Fx[c] = upwind_flux1(vel_adv, weno_upwind<ORDER, F32>(vel_adv >= 0.0, win[c]), (c == 2) ? rho_f : rho_h);
+      for (int m = 0; m < NI; ++m)
+        p[m] = (c == 0) ? ph[0][m] : ((c == 1) ? PU[me + (m - HI) * NKP] : PU[me + (m - HI)]);
+      const double va = interp_n<ORDER>(p);
+      const bool pos = va >= 0.0;
+      const float r = weno_delta<ORDER>(pos, dl[c]);
+      Fx[c] = va * ((pos ? ph[c][HI] : ph[c][HI + 1]) + (double)r) * ((c == 2) ? rho_f : rho_h);
+      asm volatile("" ::: "memory");  // one component's shared-memory reads at a time: fewer live registers
     }
-    if (upd) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const double al = (c == 2) ? al_f : al_h;
-        double ty = 0.0, Fz = 0.0;
-        if (face_ok) {
-          const double* pc = a.vel[c] + idx;
-          double ys[2 * R + 1];  // component c along y, rows j-R .. j+R
-#pragma unroll
-          for (int m = 0; m <= 2 * R; ++m) ys[m] = pc[(m - R) * g.js];
-          // advecting v interpolated along c, at the faces j+1/2 (row j) and j-1/2 (row j-1)
-          double vap, vam;
-          if (c == 0) {
-            vap = interp_c<ORDER, F32>(&win[1][MI]);
-            double p[NI];
-#pragma unroll
-            for (int m = 0; m < NI; ++m) p[m] = V[idx - g.js + (m - HI) * g.is];
-            vam = interp_c<ORDER, F32>(p);
-          } else if (c == 1) {
-            vap = interp_c<ORDER, F32>(&ys[R - HI]);
-            vam = interp_c<ORDER, F32>(&ys[R - 1 - HI]);
-          } else {
-            double p[NI], q[NI];
-#pragma unroll
-            for (int m = 0; m < NI; ++m) {
-              p[m] = V[idx + (m - HI)];
-              q[m] = V[idx - g.js + (m - HI)];
-            }
-            vap = interp_c<ORDER, F32>(p);
-            vam = interp_c<ORDER, F32>(q);
-          }
-          const double rho = (c == 2) ? rho_f : rho_h;
-          const double Fyp = upwind_flux1(vap, weno_upwind<ORDER, F32>(vap >= 0.0, ys + 1), rho);
-          const double Fym = upwind_flux1(vam, weno_upwind<ORDER, F32>(vam >= 0.0, ys), rho);
-          ty = al * (Fyp - Fym) * dyi;
-          // z face k+1/2: component c along z, advecting w interpolated along c
-          double zs[2 * R];
-#pragma unroll
-          for (int m = 0; m < 2 * R; ++m) zs[m] = pc[m - R + 1];
-          double waz;
-          if (c == 0) {
-            waz = interp_c<ORDER, F32>(&win[2][MI]);
-          } else if (c == 1) {
-            double p[NI];
-#pragma unroll
-            for (int m = 0; m < NI; ++m) p[m] = Wv[idx + (m - HI) * g.js];
-            waz = interp_c<ORDER, F32>(p);
-          } else {
-            waz = interp_c<ORDER, F32>(&zs[R - 1 - HI]);
-          }
-          Fz = upwind_flux1(waz, weno_upwind<ORDER, F32>(waz >= 0.0, zs), (c == 2) ? rho_h1 : rho_f);
-        }
-        const double Fzm = __shfl_up_sync(0xffffffffu, Fz, 1);
-        if (cell) {
-          double t = a.tend[c][idx];
-          t -= al * (Fx[c] - fprev[c]) * dxi;
-          t -= ty;
-          t -= al * (Fz - Fzm) * dzi;
-          a.tend[c][idx] = t;
-        }
-      }
-    }
+    // x terms of the tendencies now, so that fewer values live across the barrier
+    double tx[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      fprev[c] = Fx[c];
+      tx[c] = fma(-((c == 2) ? al_f : al_h) * g.dxi0, Fx[c] - fxp[c], tcur[c]);
+      fxp[c] = Fx[c];
+    }
+    // (d) y faces j+1/2 (to shared memory) and z faces k+1/2
+    double dFz[3];
 #pragma unroll
-      for (int m = 0; m < W - 1; ++m) win[c][m] = win[c][m + 1];
+    for (int c = 0; c < 3; ++c) {
+      const double* P = plane[c];
+      {
+        double v[2 * R];
+#pragma unroll
+        for (int m = 0; m < 2 * R; ++m) v[m] = P[me + (m - R + 1) * NKP];
+        float d[ND];
+#pragma unroll
+        for (int m = 0; m < ND; ++m) d[m] = (float)(v[m + 1] - v[m]);
+        double p[NI];
+#pragma unroll
+        for (int m = 0; m < NI; ++m)
+          p[m] = (c == 0) ? ph[1][m] : ((c == 1) ? PV[me + (m - HI) * NKP] : PV[me + (m - HI)]);
+        const double va = interp_n<ORDER>(p);
+        const bool pos = va >= 0.0;
+        const float r = weno_delta<ORDER>(pos, d);
+        fy[c][w][lane] = va * ((pos ? v[R - 1] : v[R]) + (double)r) * ((c == 2) ? rho_f : rho_h);
+      }
+      asm volatile("" ::: "memory");
+      {
+        double v[2 * R];
+#pragma unroll
+        for (int m = 0; m < 2 * R; ++m) v[m] = P[me + (m - R + 1)];
+        float d[ND];
+#pragma unroll
+        for (int m = 0; m < ND; ++m) d[m] = (float)(v[m + 1] - v[m]);
+        double p[NI];
+#pragma unroll
+        for (int m = 0; m < NI; ++m)
+          p[m] = (c == 0) ? ph[2][m] : ((c == 1) ? PW[me + (m - HI) * NKP] : PW[me + (m - HI)]);
+        const double va = interp_n<ORDER>(p);
+        const bool pos = va >= 0.0;
+        const float r = weno_delta<ORDER>(pos, d);
+        const double Fz = va * ((pos ? v[R - 1] : v[R]) + (double)r) * ((c == 2) ? rho_h1 : rho_f);
+        dFz[c] = Fz - __shfl_up_sync(0xffffffffu, Fz, 1);
+      }
+      asm volatile("" ::: "memory");
+    }
+    __syncthreads();
+    // (e) tendencies of the cells at x = f
+    const bool upd = cell && f >= c0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (upd) {
+        const double al = (c == 2) ? al_f : al_h;
+        double t = fma(-al * g.dxi1, fy[c][w][lane] - fy[c][w - 1][lane], tx[c]);
+        t = fma(-al * g.dxi2, dFz[c], t);
+        a.tend[c][f * g.is + jk] = t;
+      }
+      if (cell && f + 1 < c1) tcur[c] = a.tend[c][(f + 1) * g.is + jk];
+    }
+    // (f) advance the x windows by one cell
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int m = 0; m < ND - 1; ++m) dl[c][m] = dl[c][m + 1];
+      dl[c][ND - 1] = (float)(lead[c] - ph[c][NX - 1]);
+#pragma unroll
+      for (int n = 0; n < NX - 1; ++n) ph[c][n] = ph[c][n + 1];
+      ph[c][NX - 1] = lead[c];
     }
   }
 }
@@ -439,7 +616,10 @@ cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* fl
     a.vel = vel[0];
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[0] ? flux_dir[0][q] : nullptr;
     dim3 grd(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, kChunk));
-    scalar_march<0, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
+    if constexpr (F32 && NS == 1)
+      scalar_march_f32<0, ORDER><<<grd, blk, 0, st>>>(g, a, kChunk);
+    else
+      scalar_march<0, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
     pb_note_launch();
   }
   {
@@ -447,16 +627,21 @@ cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* fl
     a.vel = vel[1];
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[1] ? flux_dir[1][q] : nullptr;
     dim3 grd(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, kChunk));
-    scalar_march<1, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
+    if constexpr (F32 && NS == 1)
+      scalar_march_f32<1, ORDER><<<grd, blk, 0, st>>>(g, a, kChunk);
+    else
+      scalar_march<1, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
     pb_note_launch();
   }
   {
     ScalarArgs a = base;
     a.vel = vel[2];
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[2] ? flux_dir[2][q] : nullptr;
-    const long long nseg = (nl2 + 30) / 31;
-    const long long nwarps = nl0 * nl1 * nseg;
-    scalar_z<ORDER, F32, NS><<<ceil_div(nwarps, 4), 128, 0, st>>>(g, a, nwarps);
+    const dim3 grd(ceil_div(nl2, 31), ceil_div(nl1, 4), (unsigned)nl0);
+    if constexpr (F32 && NS == 1)
+      scalar_z_f32<ORDER><<<grd, 128, 0, st>>>(g, a);
+    else
+      scalar_z<ORDER, F32, NS><<<grd, 128, 0, st>>>(g, a);
     pb_note_launch();
   }
   return cudaGetLastError();
@@ -499,7 +684,8 @@ cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
   const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
   dim3 blk(32, 4);
   if constexpr (F32) {  // precision form: one pass for the three advecting directions
-    momentum_fused<ORDER, F32><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, 4), ceil_div(nl0, kChunk)), blk, 0, st>>>(
+    using T = MomTile<ORDER>;
+    momentum_tile<ORDER><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, kChunk)), T::NT, 0, st>>>(
         g, a, kChunk);
     pb_note_launch();
     return cudaGetLastError();
@@ -510,9 +696,7 @@ cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
   momentum_march<1, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, kChunk)), blk, 0,
                                   st>>>(g, a, kChunk);
   pb_note_launch();
-  const long long nseg = (nl2 + 30) / 31;
-  const long long nwarps = nl0 * nl1 * nseg;
-  momentum_z<ORDER, F32><<<ceil_div(nwarps, 4), 128, 0, st>>>(g, a, nwarps);
+  momentum_z<ORDER, F32><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, 4), (unsigned)nl0), 128, 0, st>>>(g, a);
   pb_note_launch();
   return cudaGetLastError();
   }

@@ -115,43 +115,66 @@ __device__ __forceinline__ FastF operator/(FastF a, FastF b) { return FastF(__fd
 // zero centre folded out by hand: IEEE arithmetic does not let the compiler
 // drop x * 0, and the folded terms are a quarter of the WENO7 work.  Real-
 // arithmetic identical to weno5 / weno7 with phi = 0 (a* = phim*, b* = phip*).
+//
+// The arithmetic runs on packed FP32 pairs (FFMA2: two lanes per
+// instruction).  The smoothness indicators pair up exactly: WENO7's beta0
+// and beta3 are the same quadratic form of (a3, a2, a1) and (b3, b2, b1),
+// beta1 and beta2 the same form of (a2, a1, b1) and (b2, b1, a1), WENO5's
+// beta0 and beta2 the same form of (a2, a1) and (b2, b1); the candidate
+// polynomials pair with per-lane coefficients.
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
 __device__ __forceinline__ float weno5_c0(float a2, float a1, float b1, float b2) {
-  const float p0 = (1.0f / 3.0f) * a2 - (7.0f / 6.0f) * a1;
+  const float2 X2 = f2(a2, b2), X1 = f2(a1, b1);
+  // (p0, p2) = (1/3 a2 - 7/6 a1, -1/6 b2 + 5/6 b1); p1 = -1/6 a1 + 1/3 b1
+  const float2 P02 = fma2(X2, f2(1.0f / 3.0f, -1.0f / 6.0f), mul2(X1, f2(-7.0f / 6.0f, 5.0f / 6.0f)));
   const float p1 = (-1.0f / 6.0f) * a1 + (1.0f / 3.0f) * b1;
-  const float p2 = (5.0f / 6.0f) * b1 - (1.0f / 6.0f) * b2;
-  const float s2a = b2 - 2.0f * b1, s2b = b2 - 4.0f * b1;
+  // (beta0, beta2) = 13/12 (X2 - 2 X1)^2 + 1/4 (X2 - 4 X1)^2
+  const float2 Sa = fma2(X1, f2(-2.0f, -2.0f), X2);
+  const float2 Sb = fma2(X1, f2(-4.0f, -4.0f), X2);
+  const float2 E02 = fma2(mul2(Sa, f2(13.0f / 12.0f, 13.0f / 12.0f)), Sa,
+                          fma2(mul2(Sb, f2(0.25f, 0.25f)), Sb, f2(1e-10f, 1e-10f)));
   const float s1a = a1 + b1, s1b = a1 - b1;
-  const float s0a = a2 - 2.0f * a1, s0b = a2 - 4.0f * a1;
-  const float e0 = (13.0f / 12.0f) * s0a * s0a + 0.25f * s0b * s0b + 1e-10f;
   const float e1 = (13.0f / 12.0f) * s1a * s1a + 0.25f * s1b * s1b + 1e-10f;
-  const float e2 = (13.0f / 12.0f) * s2a * s2a + 0.25f * s2b * s2b + 1e-10f;
-  const float al0 = __fdividef(0.1f, e0 * e0);
+  const float2 Q02 = mul2(E02, E02);
+  const float al0 = __fdividef(0.1f, Q02.x);
+  const float al2 = __fdividef(0.3f, Q02.y);
   const float al1 = __fdividef(0.6f, e1 * e1);
-  const float al2 = __fdividef(0.3f, e2 * e2);
   const float inv = __fdividef(1.0f, al0 + al1 + al2);
-  return (al0 * inv) * p0 + (al1 * inv) * p1 + (al2 * inv) * p2;
+  const float2 acc = mul2(f2(al0, al2), P02);
+  return (acc.x + acc.y + al1 * p1) * inv;
 }
 
 __device__ __forceinline__ float weno7_c0(float a3, float a2, float a1, float b1, float b2, float b3) {
-  const float p0 = -0.25f * a3 + (13.0f / 12.0f) * a2 + (-23.0f / 12.0f) * a1;
-  const float p1 = (1.0f / 12.0f) * a2 + (-5.0f / 12.0f) * a1 + 0.25f * b1;
-  const float p2 = (-1.0f / 12.0f) * a1 + (7.0f / 12.0f) * b1 + (-1.0f / 12.0f) * b2;
-  const float p3 = (13.0f / 12.0f) * b1 + (-5.0f / 12.0f) * b2 + (1.0f / 12.0f) * b3;
-  const float be0 = a3 * (547.0f * a3 - 3882.0f * a2 + 4642.0f * a1) + a2 * (7043.0f * a2 - 17246.0f * a1) +
-                    11003.0f * a1 * a1;
-  const float be1 = a2 * (267.0f * a2 - 1642.0f * a1 - 494.0f * b1) + a1 * (2843.0f * a1 + 1922.0f * b1) +
-                    547.0f * b1 * b1;
-  const float be2 = a1 * (547.0f * a1 + 1922.0f * b1 - 494.0f * b2) + b1 * (2843.0f * b1 - 1642.0f * b2) +
-                    267.0f * b2 * b2;
-  const float be3 = b1 * (11003.0f * b1 - 17246.0f * b2 + 4642.0f * b3) + b2 * (7043.0f * b2 - 3882.0f * b3) +
-                    547.0f * b3 * b3;
-  const float e0 = be0 + 1e-10f, e1 = be1 + 1e-10f, e2 = be2 + 1e-10f, e3 = be3 + 1e-10f;
-  const float al0 = __fdividef(1.0f / 35.0f, e0 * e0);
-  const float al1 = __fdividef(12.0f / 35.0f, e1 * e1);
-  const float al2 = __fdividef(18.0f / 35.0f, e2 * e2);
-  const float al3 = __fdividef(4.0f / 35.0f, e3 * e3);
-  const float inv = __fdividef(1.0f, al0 + al1 + al2 + al3);
-  return (al0 * inv) * p0 + (al1 * inv) * p1 + (al2 * inv) * p2 + (al3 * inv) * p3;
+  const float2 X3 = f2(a3, b3), X2 = f2(a2, b2), X1 = f2(a1, b1), X0 = f2(b1, a1);
+  // (p0, p3) and (p1, p2)
+  const float2 P03 = fma2(X3, f2(-0.25f, 1.0f / 12.0f),
+                          fma2(X2, f2(13.0f / 12.0f, -5.0f / 12.0f), mul2(X1, f2(-23.0f / 12.0f, 13.0f / 12.0f))));
+  const float2 P12 = fma2(X2, f2(1.0f / 12.0f, -1.0f / 12.0f),
+                          fma2(X1, f2(-5.0f / 12.0f, 7.0f / 12.0f), mul2(X0, f2(0.25f, -1.0f / 12.0f))));
+  // (beta0, beta3) = Q(X3, X2, X1), Q(x3, x2, x1) = x3 (547 x3 - 3882 x2 + 4642 x1)
+  //                  + x2 (7043 x2 - 17246 x1) + 11003 x1^2
+  const float2 t3 = fma2(X1, f2(4642.0f, 4642.0f), fma2(X2, f2(-3882.0f, -3882.0f), mul2(X3, f2(547.0f, 547.0f))));
+  const float2 t2 = fma2(X1, f2(-17246.0f, -17246.0f), mul2(X2, f2(7043.0f, 7043.0f)));
+  const float2 E03 = fma2(mul2(X1, f2(11003.0f, 11003.0f)), X1, fma2(X2, t2, fma2(X3, t3, f2(1e-10f, 1e-10f))));
+  // (beta1, beta2) = Q'(X2, X1, X0), Q'(y2, y1, y0) = y2 (267 y2 - 1642 y1 - 494 y0)
+  //                  + y1 (2843 y1 + 1922 y0) + 547 y0^2
+  const float2 u2 = fma2(X0, f2(-494.0f, -494.0f), fma2(X1, f2(-1642.0f, -1642.0f), mul2(X2, f2(267.0f, 267.0f))));
+  const float2 u1 = fma2(X0, f2(1922.0f, 1922.0f), mul2(X1, f2(2843.0f, 2843.0f)));
+  const float2 E12 = fma2(mul2(X0, f2(547.0f, 547.0f)), X0, fma2(X1, u1, fma2(X2, u2, f2(1e-10f, 1e-10f))));
+  const float2 Q03 = mul2(E03, E03), Q12 = mul2(E12, E12);
+  const float al0 = __fdividef(1.0f / 35.0f, Q03.x);
+  const float al3 = __fdividef(4.0f / 35.0f, Q03.y);
+  const float al1 = __fdividef(12.0f / 35.0f, Q12.x);
+  const float al2 = __fdividef(18.0f / 35.0f, Q12.y);
+  const float2 A03 = f2(al0, al3), A12 = f2(al1, al2);
+  const float2 S = add2(A03, A12);
+  const float inv = __fdividef(1.0f, S.x + S.y);
+  const float2 acc = fma2(A12, P12, mul2(A03, P03));
+  return (acc.x + acc.y) * inv;
 }
 
 // Face value from a stencil held in an array: ORDER 5 reads v[0..4]
@@ -204,6 +227,33 @@ __device__ __forceinline__ double weno_upwind(bool pos, const double* v) {
     return weno_face<5, F32>(st[0], st[1], st[2], st[3], st[4]);
   else
     return weno_face<7, F32>(st[0], st[1], st[2], st[3], st[4], st[5], st[6]);
+}
+
+// The precision form's upwind face value from first differences: d[m] =
+// (float)(phi[f-R+2+m] - phi[f-R+1+m]), m = 0 .. 2R-2 (R = (ORDER+1)/2, so
+// d[R-1] = phi[f+1] - phi[f]), each formed once per cell in FP64 and
+// rounded once.  The stencil's differences from its centre are partial sums
+// of d: for u >= 0 (centre phi[f]) phi[f-o] - phi[f] = -(d_{f-1} + ... +
+// d_{f-o}) and phi[f+o] - phi[f] = d_f + ... + d_{f+o-1}; for u < 0 (centre
+// phi[f+1], stencil mirrored) the same with the roles of the sides swapped.
+// Returns r with face value = centre + r.
+template <int ORDER>
+__device__ __forceinline__ float weno_delta(bool pos, const float* d) {
+  if constexpr (ORDER == 5) {  // d_{f+o} = d[2 + o]
+    const float a1 = pos ? -d[1] : d[3];
+    const float a2 = a1 + (pos ? -d[0] : d[4]);
+    const float b1 = pos ? d[2] : -d[2];
+    const float b2 = b1 + (pos ? d[3] : -d[1]);
+    return weno5_c0(a2, a1, b1, b2);
+  } else {                     // d_{f+o} = d[3 + o]
+    const float a1 = pos ? -d[2] : d[4];
+    const float a2 = a1 + (pos ? -d[1] : d[5]);
+    const float a3 = a2 + (pos ? -d[0] : d[6]);
+    const float b1 = pos ? d[3] : -d[3];
+    const float b2 = b1 + (pos ? d[4] : -d[2]);
+    const float b3 = b2 + (pos ? d[5] : -d[1]);
+    return weno7_c0(a3, a2, a1, b1, b2, b3);
+  }
 }
 
 __device__ __forceinline__ double upwind_flux1(double vel, double phi, double rho) {
