@@ -29,8 +29,14 @@ def _stir(f, seed=1, amp=0.3):
     return f
 
 
-def test_fp32_advection_tendencies():
-    nl, rs, f = host_case(**MOIST)
+# tiles of the one-pass kernels cut mid-domain: 33 rows (15 + 15 + 3), 40
+# levels (31 + 9), an odd x extent
+MOIST_TILES = dict(MOIST, nx=19, ny=33, nz=40)
+
+
+@pytest.mark.parametrize("cfg", [MOIST, MOIST_TILES], ids=["small", "tiles"])
+def test_fp32_advection_tendencies(cfg):
+    nl, rs, f = host_case(**cfg)
     f = _stir(f)
     o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f, precision="fp32")
     o.update_all_bcs()
@@ -42,6 +48,30 @@ def test_fp32_advection_tendencies():
     gt = gpu_tends(g)
     for n in o.names:
         assert rel_l2(gt[n], o.tend(n)) < 1e-5, n
+
+
+def test_fp32_scalar_fluxes():
+    """Face fluxes of the precision form on the faces the divergence reads."""
+    import torch
+    nl, rs, f = host_case(**MOIST_TILES)
+    f = _stir(f)
+    nl["gpu"] = {"keep_scalar_fluxes": True}
+    o, g = oracle_sim(nl, rs, f), gpu_sim(nl, rs, f, precision="fp32")
+    g.SA.keep_fluxes = True
+    g.SA.initialize(g.Gr, g.PV)
+    o.update_all_bcs()
+    g.PV.Update_all_bcs(g.Gr)
+    o.sa_update()
+    g.SA.update(g.Gr, g.RS, g.PV, g.DV)
+    torch.cuda.synchronize()
+    gf = g.SA.flux.cpu().numpy().reshape(2, 3, *g.Gr.shape)
+    of = o.flux.reshape(2, 3, *g.Gr.shape)
+    gw = nl["grid"]["gw"]
+    sh = g.Gr.shape
+    for d in range(3):
+        sl = [slice(gw, sh[a] - gw) for a in range(3)]
+        sl[d] = slice(gw - 1, sh[d] - gw)
+        assert rel_l2(gf[(slice(None), d) + tuple(sl)], of[(slice(None), d) + tuple(sl)]) < 1e-7, d
 
 
 def _levels_demeaned(p, d):
