@@ -150,6 +150,11 @@ struct Tile {
   float h2[8][4];
 };
 
+// COMPACT keeps the layer-2/3 loop over k-tiles rolled (a quarter of the
+// code), for callers that share the instruction cache with much other code
+// (the fused thermodynamics kernel); the training and stand-alone forward
+// kernels unroll it.  keep must be nullptr when COMPACT.
+template <bool COMPACT = false>
 __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3], const float xr1[3], float& y0,
                                              float& y1, Tile* keep) {
   const int lane = threadIdx.x & 31;
@@ -199,7 +204,7 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
   // is a complete A fragment of layer 3 and goes straight into it (fewer
   // live registers than holding all of h2)
   float c3[4] = {sm.b3, 0.0f, sm.b3, 0.0f};
-#pragma unroll
+#pragma unroll(COMPACT ? 1 : 4)
   for (int kt = 0; kt < 4; ++kt) {
     uint32_t a2[4];
 #pragma unroll
@@ -215,7 +220,7 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
       }
       a2[half * 2 + 0] = silu_bf16x2(c[0], c[1]);
       a2[half * 2 + 1] = silu_bf16x2(c[2], c[3]);
-      if (keep) {
+      if (!COMPACT && keep) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) keep->z2[nt][q] = c[q];
         const __nv_bfloat162 h01 = *reinterpret_cast<const __nv_bfloat162*>(&a2[half * 2 + 0]);

@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kSaThreads, 4) thermo_sa_kernel(Geo geo, SaArg
           if (r1 < count)
             for (int i = 0; i < 3; ++i) x1[i] = slots[r1 * 4 + i];
           float y0, y1;
-          mlpk::forward_tile(*net, x0, x1, y0, y1, nullptr);
+          mlpk::forward_tile<true>(*net, x0, x1, y0, y1, nullptr);
           if (t == 0) {
             if (r0 < count) slots[r0 * 4 + 3] = y0;
             if (r1 < count) slots[r1 * 4 + 3] = y1;
