@@ -60,6 +60,55 @@ struct Geo {
   double dx2;
 };
 
+// Ghost cell number t -> (i, j, k).  The ghost set is ordered as: the x
+// slabs (i < gw or i >= n0-gw, all j, k), then the y slabs of the interior
+// x range, then the z slabs of the interior columns.  Unsigned 32-bit
+// division when the field has fewer than 2^31 cells (a few instructions
+// instead of a 64-bit division sequence), 64-bit otherwise.
+template <class I>
+__device__ __forceinline__ void ghost_decode_t(I t, I gw, I n0, I n1, I n2, I& i, I& j, I& k) {
+  const I nl0 = n0 - 2 * gw, nl1 = n1 - 2 * gw;
+  const I A = 2 * gw * n1 * n2;
+  const I B = nl0 * 2 * gw * n2;
+  if (t < A) {
+    const I gi = t / (n1 * n2);
+    const I r = t - gi * (n1 * n2);
+    i = gi < gw ? gi : n0 - 2 * gw + gi;
+    j = r / n2;
+    k = r - j * n2;
+  } else if (t < A + B) {
+    const I u = t - A;
+    const I q = u / (2 * gw * n2);
+    const I r = u - q * (2 * gw * n2);
+    i = gw + q;
+    const I gj = r / n2;
+    j = gj < gw ? gj : n1 - 2 * gw + gj;
+    k = r - gj * n2;
+  } else {
+    const I u = t - A - B;
+    const I q = u / (nl1 * 2 * gw);
+    const I r = u - q * (nl1 * 2 * gw);
+    i = gw + q;
+    const I rj = r / (2 * gw);
+    j = gw + rj;
+    const I gk = r - rj * (2 * gw);
+    k = gk < gw ? gk : n2 - 2 * gw + gk;
+  }
+}
+
+__device__ __forceinline__ void ghost_decode(const Geo& g, long long t, long long& i, long long& j, long long& k) {
+  if (g.npg < (1LL << 31)) {
+    unsigned int i32, j32, k32;
+    ghost_decode_t<unsigned int>((unsigned int)t, (unsigned int)g.gw, (unsigned int)g.n0, (unsigned int)g.n1,
+                                 (unsigned int)g.n2, i32, j32, k32);
+    i = i32;
+    j = j32;
+    k = k32;
+  } else {
+    ghost_decode_t<long long>(t, g.gw, g.n0, g.n1, g.n2, i, j, k);
+  }
+}
+
 static inline Geo make_geo(const pb_dims* d) {
   Geo g;
   g.n0 = d->nlg[0];

@@ -347,36 +347,6 @@ __global__ void hmean_final(Geo g, const double* __restrict__ partial, double* _
   if (threadIdx.x == 0) mean[k] = red[0] * n_horizontal_i;
 }
 
-__device__ __forceinline__ void ghost_decode(const Geo& g, long long t, long long& i, long long& j, long long& k) {
-  const long long gw = g.gw, n0 = g.n0, n1 = g.n1, n2 = g.n2;
-  const long long nl0 = n0 - 2 * gw, nl1 = n1 - 2 * gw;
-  const long long A = 2 * gw * n1 * n2;
-  const long long B = nl0 * 2 * gw * n2;
-  if (t < A) {
-    const long long gi = t / (n1 * n2);
-    const long long r = t - gi * (n1 * n2);
-    i = gi < gw ? gi : n0 - 2 * gw + gi;
-    j = r / n2;
-    k = r - j * n2;
-  } else if (t < A + B) {
-    const long long u = t - A;
-    const long long q = u / (2 * gw * n2);
-    const long long r = u - q * (2 * gw * n2);
-    i = gw + q;
-    const long long gj = r / n2;
-    j = gj < gw ? gj : n1 - 2 * gw + gj;
-    k = r - gj * n2;
-  } else {
-    const long long u = t - A - B;
-    const long long q = u / (nl1 * 2 * gw);
-    const long long r = u - q * (nl1 * 2 * gw);
-    i = gw + q;
-    j = gw + r / (2 * gw);
-    const long long gk = r % (2 * gw);
-    k = gk < gw ? gk : n2 - 2 * gw + gk;
-  }
-}
-
 __global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nghost; t += stride) {
@@ -536,7 +506,7 @@ template <> __device__ __forceinline__ float2 from_d<float2>(double x, double y)
 // compute_diagonal (:129-148); Thomas algorithm of TDMA.solve applied to the
 // real and imaginary parts (the matrix is real, so both share m and scratch).
 template <class C>
-__global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 4 : 2) tdma_kernel(Geo g, PArgs a) {
   const int Nx = (int)(g.n0 - 2 * g.gw) / 2 + 1;  // stored x-modes
   const int Ny = (int)(g.n1 - 2 * g.gw);
   const int nz = (int)(g.n2 - 2 * g.gw);
@@ -575,7 +545,7 @@ __global__ void __launch_bounds__(256) tdma_kernel(Geo g, PArgs a) {
   // The sweeps walk the levels in batches of kB; the loads of the next batch
   // are issued before the current one is processed, so every thread keeps
   // kB independent loads in flight behind its serial recurrence.
-  constexpr int kB = 8;
+  constexpr int kB = sizeof(C) == 8 ? 4 : 8;  // FP32 spectra: 4 blocks per SM at 64 registers
   C cur[kB], nxt[kB];
 #pragma unroll
   for (int m = 0; m < kB; ++m) cur[m] = (1 + m < nz) ? x[(long long)(1 + m) * ncol] : from_d<C>(0.0, 0.0);

@@ -84,34 +84,10 @@ __global__ void __launch_bounds__(256) ghost_fill_kernel(Geo g, double* __restri
   const long long gw = g.gw;
   const long long n0 = g.n0, n1 = g.n1, n2 = g.n2;
   const long long nl0 = n0 - 2 * gw, nl1 = n1 - 2 * gw, nl2 = n2 - 2 * gw;
-  const long long A = 2 * gw * n1 * n2;
-  const long long B = nl0 * 2 * gw * n2;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nghost; t += stride) {
     long long i, j, k;
-    if (t < A) {
-      const long long gi = t / (n1 * n2);
-      const long long r = t - gi * (n1 * n2);
-      i = gi < gw ? gi : n0 - 2 * gw + gi;
-      j = r / n2;
-      k = r - j * n2;
-    } else if (t < A + B) {
-      const long long u = t - A;
-      const long long q = u / (2 * gw * n2);
-      const long long r = u - q * (2 * gw * n2);
-      i = gw + q;
-      const long long gj = r / n2;
-      j = gj < gw ? gj : n1 - 2 * gw + gj;
-      k = r - gj * n2;
-    } else {
-      const long long u = t - A - B;
-      const long long q = u / (nl1 * 2 * gw);
-      const long long r = u - q * (nl1 * 2 * gw);
-      i = gw + q;
-      j = gw + r / (2 * gw);
-      const long long gk = r % (2 * gw);
-      k = gk < gw ? gk : n2 - 2 * gw + gk;
-    }
+    ghost_decode(g, t, i, j, k);
     const long long is_ = (i < gw) ? i + nl0 : ((i >= n0 - gw) ? i - nl0 : i);
     const long long js_ = (j < gw) ? j + nl1 : ((j >= n1 - gw) ? j - nl1 : j);
     const long long dst = i * g.is + j * g.js + k;
