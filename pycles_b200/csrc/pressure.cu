@@ -388,6 +388,14 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KCr
   const long long j = g.gw + jl;
   const int ld = line_ld(N);
   const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
+  // distinct arrays: lets the unrolled loop issue its loads ahead of the
+  // divergence stores of earlier iterations
+  const double* __restrict__ U = a.u;
+  const double* __restrict__ V = a.v;
+  const double* __restrict__ Wv = a.w;
+  const double* __restrict__ P = a.p;
+  const double* __restrict__ mean = a.mean;
+  double* __restrict__ div = a.div;
 #pragma unroll 4
   for (int e = threadIdx.x; e < N * KC; e += kFftThreads) {
     int kl, il;
@@ -402,22 +410,22 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KCr
     double d;
     if (!RESID) {
       // w after remove_mean_u3 (PressureSolver.pyx:113-136), w - mean[k]
-      const double wc = sub_rn(a.w[ijk], a.mean[k]);
-      const double wm = sub_rn(a.w[ijk - 1], a.mean[k - 1]);
+      const double wc = sub_rn(Wv[ijk], mean[k]);
+      const double wm = sub_rn(Wv[ijk - 1], mean[k - 1]);
       if constexpr (sizeof(C) == sizeof(double2)) {  // plain form: the reference's divisions and order
         const double ah = a.alpha0_half[k];
         d = 0.0;
-        d = add_rn(d, mul_rn(sub_rn(a.u[ijk] / ah, a.u[ijk - g.is] / ah), dxi0));
-        d = add_rn(d, mul_rn(sub_rn(a.v[ijk] / ah, a.v[ijk - g.js] / ah), dxi1));
+        d = add_rn(d, mul_rn(sub_rn(U[ijk] / ah, U[ijk - g.is] / ah), dxi0));
+        d = add_rn(d, mul_rn(sub_rn(V[ijk] / ah, V[ijk - g.js] / ah), dxi1));
         d = add_rn(d, mul_rn(sub_rn(wc / a.alpha0[k], wm / a.alpha0[k - 1]), dxi2));
       } else {  // precision form: times rho0 = 1/alpha0 instead of six FP64 divisions
         const double rh = a.rho0_half[k];
-        d = (a.u[ijk] - a.u[ijk - g.is]) * rh * dxi0 + (a.v[ijk] - a.v[ijk - g.js]) * rh * dxi1 +
+        d = (U[ijk] - U[ijk - g.is]) * rh * dxi0 + (V[ijk] - V[ijk - g.js]) * rh * dxi1 +
             (wc * a.rho0[k] - wm * a.rho0[k - 1]) * dxi2;
       }
-      a.div[ijk] = d;
+      div[ijk] = d;
     } else {
-      const double* p = a.p;
+      const double* __restrict__ p = P;
       const double pc = p[ijk];
       const double lap_h = a.rho0_half[k] * ((p[ijk + g.is] - 2.0 * pc + p[ijk - g.is]) * (dxi0 * dxi0) +
                                              (p[ijk + g.js] - 2.0 * pc + p[ijk - g.js]) * (dxi1 * dxi1));
@@ -425,7 +433,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KCr
       double vert = 0.0;
       if (kk < nz - 1) vert += a.rho0[k] * (p[ijk + 1] - pc);
       if (kk > 0) vert -= a.rho0[k - 1] * (pc - p[ijk - 1]);
-      d = a.div[ijk] - (lap_h + vert * (dxi2 * dxi2));
+      d = div[ijk] - (lap_h + vert * (dxi2 * dxi2));
     }
     inr[slot] = (R)d;
   }
@@ -665,16 +673,29 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KCr
   const C* res = fft_lines<C>(in, CT ? (KC >> 1) : lc, KC >> 1, N, twx_of<C>(a), true);
   const double sc = 1.0 / (double)N;
   const long long j = g.gw + jl;
-#pragma unroll 4
-  for (int e = threadIdx.x; e < N * KC; e += kFftThreads) {
-    int kl, il;
-    split_idx(e, KC, il, kl);
-    if (kl >= kc) continue;
-    const long long ijk = (g.gw + il) * g.is + j * g.js + g.gw + k0 + kl;
-    const C z = res[(kl >> 1) * ld + swz(il)];
-    const double val = (double)((kl & 1) ? z.y : z.x) * sc;
-    if (ACC) a.p[ijk] += val;
-    else a.p[ijk] = val;
+  double* __restrict__ p = a.p;
+  // batches of kBatch elements: the pressure loads of a batch (ACC) are all
+  // issued before its stores
+  constexpr int kBatch = 8;
+  for (int e0 = threadIdx.x; e0 < N * KC; e0 += kBatch * kFftThreads) {
+    long long ijk[kBatch];
+    double val[kBatch], old[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int e = e0 + b * kFftThreads;
+      int kl = 0, il = 0;
+      split_idx(e, KC, il, kl);
+      const bool ok = e < N * KC && kl < kc;
+      ijk[b] = ok ? (g.gw + il) * g.is + j * g.js + g.gw + k0 + kl : -1;
+      if (ok) {
+        const C z = res[(kl >> 1) * ld + swz(il)];
+        val[b] = (double)((kl & 1) ? z.y : z.x) * sc;
+      }
+      old[b] = (ACC && ok) ? p[ijk[b]] : 0.0;
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (ijk[b] >= 0) p[ijk[b]] = ACC ? old[b] + val[b] : val[b];
   }
 }
 
