@@ -311,22 +311,37 @@ __global__ void hmean_partial(Geo g, const double* __restrict__ w, double* __res
   const long long per = (ncol + gridDim.x - 1) / gridDim.x;
   const long long c0 = (long long)blockIdx.x * per;
   const long long c1 = min(ncol, c0 + per);
+  // the chunk's first column, then a walk along j wrapping to the next i
+  // (no index division per element)
+  const long long i0 = g.gw + c0 / nl1, j0 = g.gw + c0 % nl1;
   for (long long k = threadIdx.x; k < g.n2; k += blockDim.x) {
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    long long off = i0 * g.is + j0 * g.js + k;
+    long long j = j0;
     long long c = c0;
-    auto at = [&](long long cc) {
-      const long long i = g.gw + cc / nl1;
-      const long long j = g.gw + cc % nl1;
-      return w[i * g.is + j * g.js + k];
-    };
     for (; c + 3 < c1; c += 4) {
-      s0 += at(c);
-      s1 += at(c + 1);
-      s2 += at(c + 2);
-      s3 += at(c + 3);
+      double v[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        v[m] = w[off];
+        off += g.js;
+        if (++j == g.gw + nl1) {
+          j = g.gw;
+          off += g.is - nl1 * g.js;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 4; ++m) s[m] += v[m];
     }
-    for (; c < c1; ++c) s0 += at(c);
-    partial[(long long)blockIdx.x * g.n2 + k] = (s0 + s1) + (s2 + s3);
+    for (; c < c1; ++c) {
+      s[0] += w[off];
+      off += g.js;
+      if (++j == g.gw + nl1) {
+        j = g.gw;
+        off += g.is - nl1 * g.js;
+      }
+    }
+    partial[(long long)blockIdx.x * g.n2 + k] = (s[0] + s[1]) + (s[2] + s[3]);
   }
 }
 

@@ -103,7 +103,21 @@ class HotPathSimulation:
         self.TS.rk_step = rk_step
         self.TS.update(Gr, PV, stream=stream)
         PV.Update_all_bcs(Gr, stream=stream)
-        self.Pr.update(Gr, RS, DV, PV, stream=stream)
+        # PressureSolver.update: the solve, then its ghost fill -- of the
+        # velocities only, the one thing the correction changed (the
+        # scalars' ghosts are the ones filled just above)
+        self.Pr.solve(Gr, RS, DV, PV, stream=stream)
+        self._fill_velocity_ghosts(stream)
+
+    def _fill_velocity_ghosts(self, stream=None):
+        """Ghost fill of the velocities alone when they are the first
+        prognostic variables (the usual order), else of all variables."""
+        PV = self.PV
+        vel = sorted(int(i) for i in PV.velocity_directions)
+        if vel == list(range(len(vel))):
+            PV.update_bcs_range(self.Gr, 0, len(vel), stream=stream)
+        else:
+            PV.Update_all_bcs(self.Gr, stream=stream)
 
     def step(self, stream=None):
         for rk in range(self.TS.n_rk_steps):
@@ -165,7 +179,8 @@ class HotPathSimulation:
             self.TS.update(Gr, PV, stream=st)
             PV.Update_all_bcs(Gr, stream=st)
             if rk < last:
-                self.Pr.update(Gr, RS, DV, PV, stream=st)
+                self.Pr.solve(Gr, RS, DV, PV, stream=st)
+                PV.update_bcs_range(Gr, 0, nvel, stream=st)
                 continue
             d2h.wait_event(event(st))
             with torch.cuda.stream(d2h):
