@@ -241,8 +241,11 @@ __device__ __forceinline__ void forward_tile(const Smem& sm, const float xr0[3],
   y1 = __shfl_sync(0xffffffffu, c3[2], lane & ~3);  // row g + 8
 }
 
+// 2 (v - lo) / (hi - lo) - 1: the offset in FP64, the scaling in FP32 with
+// a fast reciprocal (no FP64 division, whose slow path adds code to every
+// kernel that inlines this)
 __device__ __forceinline__ float norm_in(double v, float lo, float hi) {
-  return (float)(2.0 * (v - (double)lo) / ((double)hi - (double)lo) - 1.0);
+  return fmaf((float)(v - (double)lo), __fdividef(2.0f, hi - lo), -1.0f);
 }
 
 }  // namespace mlpk

@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(kSaThreads, 4) thermo_sa_kernel(Geo geo, SaArg
         }
         __syncwarp();
         const int g = lane >> 2, t = lane & 3;
+#pragma unroll 1
         for (int t0 = 0; t0 < count; t0 += 16) {
           const int r0 = t0 + g, r1 = t0 + g + 8;
           float x0[3] = {0.f, 0.f, 0.f}, x1[3] = {0.f, 0.f, 0.f};
