@@ -78,7 +78,13 @@ typedef struct pb_table {
  * by in_lo/in_hi; the seed is T = T_1 + out_mean + out_scale * y with T_1
  * the secant's first point (the network learns the correction to it).
  * Weight layouts: w1 [64][3], w2 [64][64], w3 [64] (row = output unit),
- * biases FP32.
+ * biases FP32.  seed_y: the seed's state between pb_thermo_sa calls, a
+ * device float[npg] owned by the caller and zeroed before the first call
+ * (the network's output y per cell); seed_refresh: whether pb_thermo_sa
+ * re-evaluates the network into seed_y before its kernel (a caller may
+ * refresh once per time step rather than once per RK stage: y moves ~1e-4 K
+ * within a step, the network's own error is ~1e-2 K).  Both are unused by
+ * pb_mlp_forward / pb_mlp_grad.
  */
 typedef struct pb_mlp {
   const void* w1;   /* bf16 [64*3]  */
@@ -91,6 +97,8 @@ typedef struct pb_mlp {
   float in_hi[3];
   float out_mean;
   float out_scale;
+  float* seed_y;    /* [npg], see above */
+  int seed_refresh; /* pb_thermo_sa: nonzero = refresh seed_y first */
 } pb_mlp;
 
 /* ------------------------------------------------------------------------
@@ -142,10 +150,19 @@ int pb_momentum_advection(const pb_dims* dims, const double* rho0, const double*
  * Latent heat: latent_heat_variable, lambda = 1 (Microphysics.pxd:65-75).
  *   mlp (nullable)        : learned seed for the secant's second point
  *                           (no counterpart in the reference; precision
- *                           PB_FP32 only): evaluated inside the kernel for
- *                           the saturated cells, T_2 = T_1 + out_mean +
- *                           out_scale * MLP(p0, s, qt), T_1 the secant's
- *                           first point (:22-24).
+ *                           PB_FP32 only; mlp->seed_y required).  First,
+ *                           if mlp->seed_refresh, the network refreshes
+ *                           seed_y = MLP(p0, s, qt) for every cell with
+ *                           ql > 0 on entry (saturated at the previous
+ *                           call); then each saturated cell
+ *                           starts its secant from T_2 = T_1 + out_mean +
+ *                           out_scale * seed_y, clamped to the bracket
+ *                           [T_1 + (T_2r - T_1)/16, T_2r] of the root (T_1
+ *                           the first point :22-24, T_2r the reference's
+ *                           second point :39).  Cells newly saturated
+ *                           start from an older or zero y: the clamp keeps
+ *                           any start safe and the secant's stopping test
+ *                           decides the result.
  *   secant_iters (nullable): device long long[2]; receives
  *                           {sum of secant iterations, saturated cells}.
  *   max_iter              : secant iteration cap (the reference has none);

@@ -36,7 +36,8 @@ class PbTable(ctypes.Structure):
 class PbMlp(ctypes.Structure):
     _fields_ = [("w1", _vp), ("b1", _vp), ("w2", _vp), ("b2", _vp), ("w3", _vp), ("b3", _vp),
                 ("in_lo", ctypes.c_float * 3), ("in_hi", ctypes.c_float * 3),
-                ("out_mean", ctypes.c_float), ("out_scale", ctypes.c_float)]
+                ("out_mean", ctypes.c_float), ("out_scale", ctypes.c_float), ("seed_y", _vp),
+                ("seed_refresh", ctypes.c_int)]
 
 
 PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_UNSUPPORTED, PB_ERR_WORKSPACE = 0, 1, 2, 3, 4

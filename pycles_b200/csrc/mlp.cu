@@ -61,6 +61,78 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(FwdArgs a) {
   }
 }
 
+// Refresh of the learned seed's per-cell network output y for the cells
+// that were saturated at the previous thermodynamics update (ql > 0 there):
+// a warp takes 32 consecutive cells (consecutive levels of a column),
+// compacts the flagged ones into per-warp shared slots and evaluates the
+// network on them 16 at a time.  Runs as its own kernel ahead of the
+// thermodynamics kernel, which then reads y: the network's code and shared
+// memory stay out of the FP64 secant kernel (whose instruction cache it
+// overflowed), and the tiles are as full as the flagged runs allow.
+struct RefreshArgs {
+  const __nv_bfloat16* w1;
+  const float* b1;
+  const __nv_bfloat16* w2;
+  const float* b2;
+  const __nv_bfloat16* w3;
+  const float* b3;
+  float lo[3], hi[3];
+  const double* p0;  // per level (n2)
+  const double* s;
+  const double* qt;
+  const double* ql;  // the previous update's condensate: the flag
+  float* y;
+  long long npg;
+  int n2;
+};
+
+constexpr int kRefreshWarps = 4;
+
+__global__ void __launch_bounds__(32 * kRefreshWarps) mlp_seed_refresh_kernel(RefreshArgs a) {
+  __shared__ Smem sm;
+  __shared__ float slots[kRefreshWarps][32 * 4];
+  stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int g = lane >> 2;
+  float* sl = slots[wid];
+  const long long nchunk = (a.npg + 31) / 32;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunk; c += nwarps) {
+    const long long idx = c * 32 + lane;
+    const bool sat = idx < a.npg && a.ql[idx] > 0.0;
+    const unsigned mask = __ballot_sync(0xffffffffu, sat);
+    if (!mask) continue;  // warp-uniform
+    const int pos = __popc(mask & ((1u << lane) - 1u));
+    const int count = __popc(mask);
+    if (sat) {
+      const int k = (int)(idx % a.n2);
+      sl[pos * 4 + 0] = norm_in(a.p0[k], a.lo[0], a.hi[0]);
+      sl[pos * 4 + 1] = norm_in(a.s[idx], a.lo[1], a.hi[1]);
+      sl[pos * 4 + 2] = norm_in(a.qt[idx], a.lo[2], a.hi[2]);
+    }
+    __syncwarp();
+    for (int t0 = 0; t0 < count; t0 += 16) {
+      const int r0 = t0 + g, r1 = t0 + g + 8;
+      float x0[3] = {0.f, 0.f, 0.f}, x1[3] = {0.f, 0.f, 0.f};
+      if (r0 < count)
+        for (int i = 0; i < 3; ++i) x0[i] = sl[r0 * 4 + i];
+      if (r1 < count)
+        for (int i = 0; i < 3; ++i) x1[i] = sl[r1 * 4 + i];
+      float y0, y1;
+      forward_tile(sm, x0, x1, y0, y1, nullptr);
+      __syncwarp();
+      if ((lane & 3) == 0) {
+        if (r0 < count) sl[r0 * 4 + 3] = y0;
+        if (r1 < count) sl[r1 * 4 + 3] = y1;
+      }
+      __syncwarp();
+    }
+    if (sat) a.y[idx] = sl[pos * 4 + 3];
+    __syncwarp();  // the slots are reused by the next chunk
+  }
+}
+
 // Gradient of sum_r 0.5 (y_r - target_r)^2 over n normalised samples,
 // accumulated into grad[NPARAM] (packed, FP32), loss sum into *loss.
 struct GradArgs {
@@ -263,6 +335,36 @@ __global__ void mlp_adam_kernel(AdamArgs a) {
 }
 
 }  // namespace mlpk
+
+static int mlp_blocks(long long work_tiles, int warps_per_block);
+
+// y[cell] = MLP(p0, s, qt) for every cell with ql > 0 (called by
+// pb_thermo_sa before its kernel; mlp validated there).
+cudaError_t pb_mlp_seed_refresh(const pb_mlp* mlp, const Geo& g, const double* p0, const double* s,
+                                const double* qt, const double* ql, cudaStream_t st) {
+  mlpk::RefreshArgs a;
+  a.w1 = static_cast<const __nv_bfloat16*>(mlp->w1);
+  a.b1 = mlp->b1;
+  a.w2 = static_cast<const __nv_bfloat16*>(mlp->w2);
+  a.b2 = mlp->b2;
+  a.w3 = static_cast<const __nv_bfloat16*>(mlp->w3);
+  a.b3 = mlp->b3;
+  for (int i = 0; i < 3; ++i) {
+    a.lo[i] = mlp->in_lo[i];
+    a.hi[i] = mlp->in_hi[i];
+  }
+  a.p0 = p0;
+  a.s = s;
+  a.qt = qt;
+  a.ql = ql;
+  a.y = mlp->seed_y;
+  a.npg = g.npg;
+  a.n2 = (int)g.n2;
+  mlpk::mlp_seed_refresh_kernel<<<mlp_blocks((g.npg + 31) / 32, mlpk::kRefreshWarps), 32 * mlpk::kRefreshWarps, 0,
+                                  st>>>(a);
+  pb_note_launch();
+  return cudaGetLastError();
+}
 
 static int mlp_blocks(long long work_tiles, int warps_per_block) {
   int dev = 0, sms = 148;

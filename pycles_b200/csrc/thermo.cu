@@ -27,11 +27,6 @@ void column_launch_shape(long long n2, int per_col_arrays, dim3* blk, size_t* sm
   *smem = (size_t)per_col_arrays * kpad * cols * sizeof(double);
 }
 
-size_t seed_smem_bytes(dim3 blk) {
-  const size_t nwarps = (size_t)blk.x * blk.y / 32;
-  return (sizeof(mlpk::Smem) + 15) / 16 * 16 + nwarps * kSeedSlotFloats * sizeof(float);
-}
-
 cudaError_t launch_sa_exact(const Geo& geo, const SaArgs& a, cudaStream_t st) {
   return thermo_kk::launch_sa<ExactMath, false>(geo, a, st);
 }
@@ -43,6 +38,10 @@ cudaError_t launch_dry_exact(const Geo& geo, const DryArgs& a, cudaStream_t st) 
 }  // namespace thermo_k
 
 using namespace thermo_k;
+
+// mlp.cu: refresh of the seed's per-cell network output (cells with ql > 0)
+cudaError_t pb_mlp_seed_refresh(const pb_mlp* mlp, const Geo& g, const double* p0, const double* s,
+                                const double* qt, const double* ql, cudaStream_t st);
 
 extern "C" int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const double* alpha0_half,
                             const pb_table* table, const double* s, double* qt, double* T, double* qv,
@@ -56,7 +55,8 @@ extern "C" int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const do
     return PB_ERR_ARG;
   if (max_iter < 1) return PB_ERR_ARG;
   if (precision != PB_FP64 && precision != PB_FP32) return PB_ERR_ARG;
-  if (mlp && (precision != PB_FP32 || !mlp->w1 || !mlp->b1 || !mlp->w2 || !mlp->b2 || !mlp->w3 || !mlp->b3))
+  if (mlp && (precision != PB_FP32 || !mlp->w1 || !mlp->b1 || !mlp->w2 || !mlp->b2 || !mlp->w3 || !mlp->b3 ||
+              !mlp->seed_y))
     return PB_ERR_ARG;
   if (dims->nlg[2] > 1024) return PB_ERR_UNSUPPORTED;
   const Geo geo = make_geo(dims);
@@ -81,21 +81,16 @@ extern "C" int pb_thermo_sa(const pb_dims* dims, const double* p0_half, const do
   if (!a.err) return PB_ERR_CUDA;
   a.clip = clip_qt;
   a.max_iter = max_iter;
+  const cudaStream_t st = as_stream(stream);
   if (mlp) {
-    a.net.w1 = static_cast<const __nv_bfloat16*>(mlp->w1);
-    a.net.b1 = mlp->b1;
-    a.net.w2 = static_cast<const __nv_bfloat16*>(mlp->w2);
-    a.net.b2 = mlp->b2;
-    a.net.w3 = static_cast<const __nv_bfloat16*>(mlp->w3);
-    a.net.b3 = mlp->b3;
-    for (int i = 0; i < 3; ++i) {
-      a.net.lo[i] = mlp->in_lo[i];
-      a.net.hi[i] = mlp->in_hi[i];
-    }
+    // the network's output for the cells saturated at the previous call,
+    // at the current (p0, s, qt); the kernel below starts their secant there
+    a.net.y = mlp->seed_y;
     a.net.out_mean = mlp->out_mean;
     a.net.out_scale = mlp->out_scale;
+    if (mlp->seed_refresh && pb_mlp_seed_refresh(mlp, geo, p0_half, s, qt, ql, st) != cudaSuccess)
+      return PB_ERR_CUDA;
   }
-  const cudaStream_t st = as_stream(stream);
   const cudaError_t e = precision == PB_FP64 ? launch_sa_exact(geo, a, st) : launch_sa_fast(geo, a, mlp != nullptr, st);
   return e == cudaSuccess ? PB_OK : PB_ERR_CUDA;
 }

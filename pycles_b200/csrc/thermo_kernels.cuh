@@ -10,18 +10,11 @@
 
 #include "pb_common.cuh"
 #include "thermo_funcs.cuh"
-#include "mlp.cuh"
 
 namespace thermo_k {
 
 struct SeedNet {             // learned seed (precision form), see pb_mlp
-  const __nv_bfloat16* w1;
-  const float* b1;
-  const __nv_bfloat16* w2;
-  const float* b2;
-  const __nv_bfloat16* w3;
-  const float* b3;
-  float lo[3], hi[3];
+  const float* y;            // network output per cell, refreshed before the kernel
   float out_mean, out_scale;
 };
 
@@ -62,10 +55,8 @@ struct DryArgs {
 
 // Launch shape of the dry kernel: blocks of (kpad, cols) threads, kpad = n2
 // rounded up to a warp, cols columns per block; dynamic shared memory for the
-// per-column arrays.  seed_smem_bytes: the network and its per-warp slots.
+// per-column arrays.
 void column_launch_shape(long long n2, int per_col_arrays, dim3* blk, size_t* smem);
-constexpr size_t kSeedSlotFloats = 32 * 4;  // per warp: 3 inputs + 1 output per lane
-size_t seed_smem_bytes(dim3 blk);
 
 // Per-translation-unit launchers.
 cudaError_t launch_sa_exact(const Geo& geo, const SaArgs& a, cudaStream_t st);
@@ -96,10 +87,9 @@ using thermo_k::SaArgs;
 // segments, whose secant iterates, are spread over all warps.  The Exner
 // function of every level is tabulated in shared memory once per block.
 //
-// SEED: after the first secant point, each warp compacts its saturated cells
-// into its slots, evaluates the network on them 16 at a time on the tensor
-// cores, and each saturated cell starts the secant from
-//   T_2 = T_1 + out_mean + out_scale * y.
+// SEED: each saturated cell starts the secant from
+//   T_2 = T_1 + out_mean + out_scale * y[cell]
+// (clamped in eos_finish), y refreshed by the network kernel beforehand.
 constexpr int kSeg = 30;
 constexpr int kSaThreads = 256;
 
@@ -120,14 +110,6 @@ __global__ void __launch_bounds__(kSaThreads, 4) thermo_sa_kernel(Geo geo, SaArg
       exner_tab[2 * n2 + k] = 1.0 / a.p0[k];
       exner_tab[3 * n2 + k] = 1.0 / a.alpha0[k];
     }
-  }
-  mlpk::Smem* net = nullptr;
-  float* slots = nullptr;
-  if constexpr (SEED) {
-    net = reinterpret_cast<mlpk::Smem*>(smraw + ((M::exact ? 1 : 4) * n2 * sizeof(double) + 15) / 16 * 16);
-    slots = reinterpret_cast<float*>(net + 1) + (size_t)(threadIdx.x >> 5) * thermo_k::kSeedSlotFloats;
-    mlpk::stage_weights(*net, a.net.w1, a.net.b1, a.net.w2, a.net.b2, a.net.w3, a.net.b3, threadIdx.x,
-                        blockDim.x);
   }
   __syncthreads();
   const long long ntask = ncols * nseg;
@@ -157,37 +139,7 @@ __global__ void __launch_bounds__(kSaThreads, 4) thermo_sa_kernel(Geo geo, SaArg
     }
     double seed = 0.0;
     if constexpr (SEED) {
-      const bool sat = kin && st.sat;
-      const unsigned mask = __ballot_sync(0xffffffffu, sat);
-      if (mask) {  // warp-uniform
-        const int pos = __popc(mask & ((1u << lane) - 1u));
-        const int count = __popc(mask);
-        if (sat) {
-          slots[pos * 4 + 0] = mlpk::norm_in(p0, a.net.lo[0], a.net.hi[0]);
-          slots[pos * 4 + 1] = mlpk::norm_in(s, a.net.lo[1], a.net.hi[1]);
-          slots[pos * 4 + 2] = mlpk::norm_in(qt, a.net.lo[2], a.net.hi[2]);
-        }
-        __syncwarp();
-        const int g = lane >> 2, t = lane & 3;
-#pragma unroll 1
-        for (int t0 = 0; t0 < count; t0 += 16) {
-          const int r0 = t0 + g, r1 = t0 + g + 8;
-          float x0[3] = {0.f, 0.f, 0.f}, x1[3] = {0.f, 0.f, 0.f};
-          if (r0 < count)
-            for (int i = 0; i < 3; ++i) x0[i] = slots[r0 * 4 + i];
-          if (r1 < count)
-            for (int i = 0; i < 3; ++i) x1[i] = slots[r1 * 4 + i];
-          float y0, y1;
-          mlpk::forward_tile<true>(*net, x0, x1, y0, y1, nullptr);
-          if (t == 0) {
-            if (r0 < count) slots[r0 * 4 + 3] = y0;
-            if (r1 < count) slots[r1 * 4 + 3] = y1;
-          }
-        }
-        __syncwarp();
-        if (sat) seed = st.T_1 + (double)a.net.out_mean + (double)a.net.out_scale * (double)slots[pos * 4 + 3];
-        __syncwarp();  // the slots are reused by the next column
-      }
+      if (kin && st.sat) seed = st.T_1 + (double)a.net.out_mean + (double)a.net.out_scale * (double)a.net.y[idx];
     }
     double T = 0.0, qv = 0.0, thr = 0.0, b = 0.0;
     if (kin) {
@@ -322,8 +274,7 @@ __global__ void thermo_dry_kernel(Geo geo, DryArgs a, long long ncols) {
 
 template <class M, bool SEED>
 cudaError_t launch_sa(const Geo& geo, const SaArgs& a, cudaStream_t st) {
-  const size_t smem = ((M::exact ? 1 : 4) * geo.n2 * sizeof(double) + 15) / 16 * 16 +
-                      (SEED ? thermo_k::seed_smem_bytes(dim3(kSaThreads, 1)) : 0);
+  const size_t smem = ((M::exact ? 1 : 4) * geo.n2 * sizeof(double) + 15) / 16 * 16;
   if (smem > 48 * 1024) {
     const cudaError_t e =
         cudaFuncSetAttribute(thermo_sa_kernel<M, SEED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

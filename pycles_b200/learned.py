@@ -71,6 +71,8 @@ class SeedMLP:
             s.in_hi[i] = IN_HI[i]
         s.out_mean = self.out_mean
         s.out_scale = self.out_scale
+        s.seed_y = None  # the per-cell seed state belongs to the thermodynamics that uses the network
+        s.seed_refresh = 0
         return s
 
     # ------------------------------------------------------------------

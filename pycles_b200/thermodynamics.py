@@ -208,6 +208,12 @@ class ThermodynamicsSA:
         self.precision = _capi.precision_of(namelist)
         self.mlp = None          # learned seed (pycles_b200.learned.SeedMLP, precision form) or None
         self.iter_stats = None   # device int64[2]: secant iterations, saturated cells
+        self._seed_y = None      # device float32[npg]: the network's output per cell
+        self._seed_for = None    # the network seed_y belongs to
+        self._seed_calls = 0
+        # updates between re-evaluations of the network (3: once per SSP-RK3
+        # time step; 1: every update)
+        self.seed_refresh_interval = max(1, int(namelist.get("gpu", {}).get("seed_refresh_interval", 3)))
 
     def initialize(self, Gr, PV, DV, NS=None, Pa=None):
         PV.add_variable("s", "J kg^-1 K^-1", "s", "specific entropy", "sym", "scalar", Pa)
@@ -239,10 +245,22 @@ class ThermodynamicsSA:
         mlp_struct = None
         if self.mlp is not None:
             # learned seed for the secant's second point (no counterpart in the
-            # reference; precision form only), evaluated inside the kernel
+            # reference; precision form only): the library refreshes the
+            # network's output per cell for the cells saturated at the
+            # previous update, then starts their secant from it
             if self.precision != _capi.PB_FP32:
                 raise ValueError("the learned seed belongs to the precision form (gpu.precision = 'fp32')")
+            npg = int(Gr.dims.npg)
+            dev = PV.values.device
+            if (self._seed_y is None or self._seed_for is not self.mlp or self._seed_y.numel() != npg
+                    or self._seed_y.device != dev):
+                self._seed_y = torch.zeros(npg, dtype=torch.float32, device=dev)
+                self._seed_for = self.mlp
+                self._seed_calls = 0
             self._mlp_struct = self.mlp.struct()
+            self._mlp_struct.seed_y = self._seed_y.data_ptr()
+            self._mlp_struct.seed_refresh = 1 if self._seed_calls % self.seed_refresh_interval == 0 else 0
+            self._seed_calls += 1
             mlp_struct = ctypes.byref(self._mlp_struct)
         table = self.CC.device_table(PV.values.device)
         rc = L.pb_thermo_sa(ctypes.byref(Gr.dims), _capi.ptr(RS.d_p0_half), _capi.ptr(RS.d_alpha0_half),

@@ -121,9 +121,11 @@ def test_trained_seed_cuts_secant_iterations():
 
 
 def test_fused_seed_in_thermodynamics():
-    """The seed evaluated inside the precision-form thermodynamics kernel:
-    same temperatures as the plain form to the secant's tolerance, fewer
-    secant iterations than the precision form without the seed."""
+    """The learned seed inside the precision-form thermodynamics update (the
+    network refreshed for the cells saturated at the previous update, then
+    the secant started from it): same temperatures as the plain form to the
+    secant's tolerance, fewer secant iterations than the precision form
+    without the seed."""
     from helpers import gpu_dv, gpu_sim, host_case
     from pycles_b200 import learned
     nl, rs, f = host_case(case="dycoms", nx=16, ny=16, nz=256, dx=35.0, dy=35.0, dz=5.0, gw=4, dt=0.25,
@@ -141,9 +143,11 @@ def test_fused_seed_in_thermodynamics():
     mlp = learned.SeedMLP(seed=0, out_mean=float(r.mean()), out_scale=2.0 * float(r.std()))
     mlp.train(P, S, Q, T, T1, epochs=8, batch=8192)
     seeded.Th.mlp = mlp
+    seeded.Th.seed_refresh_interval = 1  # re-evaluate the network at every update
     stats = {}
     for name, g in (("plain", plain), ("fast", fast), ("seeded", seeded)):
         g.PV.Update_all_bcs(g.Gr)
+        g.Th.update(g.Gr, g.RS, g.PV, g.DV)  # the condensate the seed refresh keys on
         g.Th.iter_stats = None
         g.Th.update(g.Gr, g.RS, g.PV, g.DV)
         it, nsat = g.Th.iter_stats.cpu().tolist()
