@@ -62,13 +62,14 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(FwdArgs a) {
 }
 
 // Refresh of the learned seed's per-cell network output y for the cells
-// that were saturated at the previous thermodynamics update (ql > 0 there):
-// a warp takes 32 consecutive cells (consecutive levels of a column),
-// compacts the flagged ones into per-warp shared slots and evaluates the
-// network on them 16 at a time.  Runs as its own kernel ahead of the
-// thermodynamics kernel, which then reads y: the network's code and shared
-// memory stay out of the FP64 secant kernel (whose instruction cache it
-// overflowed), and the tiles are as full as the flagged runs allow.
+// that were saturated at the previous thermodynamics update (ql > 0 there).
+// Runs as its own kernel ahead of the thermodynamics kernel, which then
+// reads y: the network's code and shared memory stay out of the FP64 secant
+// kernel (whose instruction cache it overflowed).  Each warp scans its
+// chunks of 32 consecutive cells kBatch chunks at a time (kBatch flag loads
+// in flight), appends the flagged cells to a queue in shared memory and
+// evaluates the network whenever the queue holds a full 16-row tile, so the
+// tiles are full except the warp's last one.
 struct RefreshArgs {
   const __nv_bfloat16* w1;
   const float* b1;
@@ -87,50 +88,75 @@ struct RefreshArgs {
 };
 
 constexpr int kRefreshWarps = 4;
+constexpr int kRefreshBatch = 8;                   // chunks scanned per round
+constexpr int kQueue = 32 * kRefreshBatch + 16;    // queue capacity per warp
+
+// One full tile from the head of the warp's queue q (cell indices).
+__device__ __forceinline__ void refresh_tile(const Smem& sm, const RefreshArgs& a, const int* q, int n) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2;
+  float x0[3] = {0.f, 0.f, 0.f}, x1[3] = {0.f, 0.f, 0.f};
+  long long i0 = -1, i1 = -1;
+  if (g < n) {
+    i0 = q[g];
+    x0[0] = norm_in(a.p0[(int)i0 % a.n2], a.lo[0], a.hi[0]);
+    x0[1] = norm_in(a.s[i0], a.lo[1], a.hi[1]);
+    x0[2] = norm_in(a.qt[i0], a.lo[2], a.hi[2]);
+  }
+  if (g + 8 < n) {
+    i1 = q[g + 8];
+    x1[0] = norm_in(a.p0[(int)i1 % a.n2], a.lo[0], a.hi[0]);
+    x1[1] = norm_in(a.s[i1], a.lo[1], a.hi[1]);
+    x1[2] = norm_in(a.qt[i1], a.lo[2], a.hi[2]);
+  }
+  float y0, y1;
+  forward_tile(sm, x0, x1, y0, y1, nullptr);
+  if ((lane & 3) == 0) {
+    if (i0 >= 0) a.y[i0] = y0;
+    if (i1 >= 0) a.y[i1] = y1;
+  }
+}
 
 __global__ void __launch_bounds__(32 * kRefreshWarps) mlp_seed_refresh_kernel(RefreshArgs a) {
   __shared__ Smem sm;
-  __shared__ float slots[kRefreshWarps][32 * 4];
+  __shared__ int queue[kRefreshWarps][kQueue];
   stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3, threadIdx.x, blockDim.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int g = lane >> 2;
-  float* sl = slots[wid];
+  int* q = queue[wid];
+  int nq = 0;  // warp-uniform queue length
   const long long nchunk = (a.npg + 31) / 32;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunk; c += nwarps) {
-    const long long idx = c * 32 + lane;
-    const bool sat = idx < a.npg && a.ql[idx] > 0.0;
-    const unsigned mask = __ballot_sync(0xffffffffu, sat);
-    if (!mask) continue;  // warp-uniform
-    const int pos = __popc(mask & ((1u << lane) - 1u));
-    const int count = __popc(mask);
-    if (sat) {
-      const int k = (int)(idx % a.n2);
-      sl[pos * 4 + 0] = norm_in(a.p0[k], a.lo[0], a.hi[0]);
-      sl[pos * 4 + 1] = norm_in(a.s[idx], a.lo[1], a.hi[1]);
-      sl[pos * 4 + 2] = norm_in(a.qt[idx], a.lo[2], a.hi[2]);
+  const long long first = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (long long cb = first; cb < nchunk; cb += (long long)kRefreshBatch * nwarps) {
+    unsigned masks[kRefreshBatch];
+#pragma unroll
+    for (int m = 0; m < kRefreshBatch; ++m) {
+      const long long idx = (cb + m * nwarps) * 32 + lane;
+      masks[m] = __ballot_sync(0xffffffffu, idx < a.npg && __ldg(a.ql + idx) > 0.0);
+    }
+#pragma unroll
+    for (int m = 0; m < kRefreshBatch; ++m) {
+      const long long idx = (cb + m * nwarps) * 32 + lane;
+      if ((masks[m] >> lane) & 1u) q[nq + __popc(masks[m] & ((1u << lane) - 1u))] = (int)idx;
+      nq += __popc(masks[m]);
     }
     __syncwarp();
-    for (int t0 = 0; t0 < count; t0 += 16) {
-      const int r0 = t0 + g, r1 = t0 + g + 8;
-      float x0[3] = {0.f, 0.f, 0.f}, x1[3] = {0.f, 0.f, 0.f};
-      if (r0 < count)
-        for (int i = 0; i < 3; ++i) x0[i] = sl[r0 * 4 + i];
-      if (r1 < count)
-        for (int i = 0; i < 3; ++i) x1[i] = sl[r1 * 4 + i];
-      float y0, y1;
-      forward_tile(sm, x0, x1, y0, y1, nullptr);
-      __syncwarp();
-      if ((lane & 3) == 0) {
-        if (r0 < count) sl[r0 * 4 + 3] = y0;
-        if (r1 < count) sl[r1 * 4 + 3] = y1;
-      }
-      __syncwarp();
+    int head = 0;
+    while (nq - head >= 16) {
+      refresh_tile(sm, a, q + head, 16);
+      head += 16;
     }
-    if (sat) a.y[idx] = sl[pos * 4 + 3];
-    __syncwarp();  // the slots are reused by the next chunk
+    // keep the remainder (< 16) at the front of the queue
+    __syncwarp();
+    const int rest = nq - head;
+    const int moved = lane < rest ? q[head + lane] : 0;
+    __syncwarp();
+    if (lane < rest) q[lane] = moved;
+    nq = rest;
+    __syncwarp();
   }
+  if (nq > 0) refresh_tile(sm, a, q, nq);
 }
 
 // Gradient of sum_r 0.5 (y_r - target_r)^2 over n normalised samples,
@@ -342,6 +368,7 @@ static int mlp_blocks(long long work_tiles, int warps_per_block);
 // pb_thermo_sa before its kernel; mlp validated there).
 cudaError_t pb_mlp_seed_refresh(const pb_mlp* mlp, const Geo& g, const double* p0, const double* s,
                                 const double* qt, const double* ql, cudaStream_t st) {
+  if (g.npg >= (1LL << 31)) return cudaErrorInvalidValue;  // the queue holds 32-bit cell indices
   mlpk::RefreshArgs a;
   a.w1 = static_cast<const __nv_bfloat16*>(mlp->w1);
   a.b1 = mlp->b1;
