@@ -101,7 +101,16 @@ template <> __device__ __forceinline__ float2 creal<float2>(double x) { return m
 // 8) and the odd line stride keep the strided accesses of the passes and of
 // the global loads/stores (consecutive threads on consecutive lines) free of
 // bank conflicts.
-__host__ __device__ __forceinline__ int line_ld(int N) { return N + N / 8 + 1; }
+// The stride is chosen for the transposing loads and stores: a half-warp
+// touches IC lines at 16/IC consecutive positions (IC = 4096/N lines for
+// powers of two >= 256, 16 below), so with ld = 16/IC (mod 16) its 16
+// accesses fall on distinct bank pairs; other lengths take an odd stride.
+__host__ __device__ __forceinline__ int line_ld(int N) {
+  const int base = N + N / 8;
+  if ((N & (N - 1)) != 0 || N < 256) return base + 1;
+  const int want = (N / 256) & 15;  // 16 / IC mod 16
+  return base + ((want - base % 16) + 16) % 16;
+}
 __device__ __forceinline__ int swz(int x) { return x + (x >> 3); }
 
 template <class C>
