@@ -92,24 +92,38 @@ __global__ void __launch_bounds__(256) ghost_fill_kernel(Geo g, double* __restri
     const long long js_ = (j < gw) ? j + nl1 : ((j >= n1 - gw) ? j - nl1 : j);
     const long long dst = i * g.is + j * g.js + k;
     const long long colsrc = is_ * g.is + js_ * g.js;
-    for (int v = 0; v < bc.nv; ++v) {
-      const double fac = bc.factor[v];
-      double* f = vals + (long long)v * g.npg;
-      double out;
-      if (k >= gw && k < n2 - gw) {
-        out = f[colsrc + k];
-      } else if (k >= n2 - gw) {  // top, set_bcs s = -1
-        const long long tt = k - (n2 - gw);
-        if (fac == 1.0) out = f[colsrc + (n2 - gw - 1 - tt)];
-        else if (fac == 2.0) out = f[colsrc + (n2 - gw - 1)];
-        else out = (tt == 0) ? 0.0 : fac * f[colsrc + (n2 - gw - tt)];
-      } else {  // bottom, set_bcs s = +1
-        const long long tt = gw - 1 - k;
-        if (fac == 1.0) out = f[colsrc + (gw + tt)];
-        else if (fac == 2.0) out = f[colsrc + gw];
-        else out = (tt == 0) ? 0.0 : fac * f[colsrc + (gw - 1 + tt)];
+    // reads touch interior cells only and writes ghost cells only, so the
+    // variables' loads of a batch are all issued before its stores; each
+    // variable's value is mult * f[src], or exactly 0 on the first
+    // antisymmetric level (set_bcs with factor != 1, 2)
+    constexpr int kB = 4;
+    for (int v0 = 0; v0 < bc.nv; v0 += kB) {
+      double out[kB];
+#pragma unroll
+      for (int b = 0; b < kB; ++b) {
+        const int v = v0 + b;
+        out[b] = 0.0;
+        if (v >= bc.nv) continue;
+        const double fac = bc.factor[v];
+        long long src = colsrc + k;
+        double mult = 1.0;
+        bool zero = false;
+        if (k >= n2 - gw) {  // top, set_bcs s = -1
+          const long long tt = k - (n2 - gw);
+          if (fac == 1.0) src = colsrc + (n2 - gw - 1 - tt);
+          else if (fac == 2.0) src = colsrc + (n2 - gw - 1);
+          else { src = colsrc + (n2 - gw - tt); mult = fac; zero = tt == 0; }
+        } else if (k < gw) {  // bottom, set_bcs s = +1
+          const long long tt = gw - 1 - k;
+          if (fac == 1.0) src = colsrc + (gw + tt);
+          else if (fac == 2.0) src = colsrc + gw;
+          else { src = colsrc + (gw - 1 + tt); mult = fac; zero = tt == 0; }
+        }
+        if (!zero) out[b] = mult * vals[(long long)v * g.npg + src];
       }
-      f[dst] = out;
+#pragma unroll
+      for (int b = 0; b < kB; ++b)
+        if (v0 + b < bc.nv) vals[(long long)(v0 + b) * g.npg + dst] = out[b];
     }
     (void)nl2;
   }
