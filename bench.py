@@ -55,28 +55,32 @@ def _ghost_bytes(nv, cfg):
 
 # Compulsory (algorithmic) bytes per interior cell per RK stage of each timed
 # component, FP64 storage: every array it must read once and write once.
+# fused: the precision form's stepping, the u, v, w stage inside the
+# momentum pass.
 COMPONENT_BYTES_PER_CELL = {
     # moist: read s, qt, w-tendency; write qt, T, qv, ql, qi, alpha,
     # buoyancy, theta_rho, bvf, thetali, w-tendency.  dry: read s,
     # w-tendency; write T, alpha, buoyancy, theta, bvf, w-tendency.
-    "thermo": lambda nv, cfg: 112.0 if cfg["case"] != "dry_cbl" else 64.0,
+    "thermo": lambda nv, cfg, fused: 112.0 if cfg["case"] != "dry_cbl" else 64.0,
     # read u, v, w and the scalars, read-modify-write the scalar tendencies
-    "scalar_adv": lambda nv, cfg: 8.0 * nv + 16.0 * (nv - 3),
-    # read u, v, w, read-modify-write the three momentum tendencies
-    "momentum_adv": lambda nv, cfg: 72.0,
+    "scalar_adv": lambda nv, cfg, fused: 8.0 * nv + 16.0 * (nv - 3),
+    # read u, v, w, read-modify-write the three momentum tendencies; fused:
+    # read u, v, w and the w tendency, write the new u, v, w, write (stage 0)
+    # or read the copies, clear the w tendency
+    "momentum_adv": lambda nv, cfg, fused: 88.0 if fused else 72.0,
     # SSP-RK3 stage (read value, tendency, copy; write value, copy,
-    # zeroed tendency: 40 B per variable) + ghost fill
-    "rk3+bcs": lambda nv, cfg: 40.0 * nv + _ghost_bytes(nv, cfg),
+    # zeroed tendency: 40 B per variable; fused: the scalars only) + ghost fill
+    "rk3+bcs": lambda nv, cfg, fused: 40.0 * (nv - 3 if fused else nv) + _ghost_bytes(nv, cfg),
     # read u, v, w; write u, v, w, divergence, pressure
-    "pressure": lambda nv, cfg: 64.0,
+    "pressure": lambda nv, cfg, fused: 64.0,
 }
 COMPONENT_KERNELS = {
     "thermo": "thermo_sa_kernel (saturation adjustment, buoyancy, bvf, thetali; one launch per stage)",
     "scalar_adv": "scalar_march x, y + scalar_z (WENO fluxes + divergence; 3 launches per stage and scalar "
                   "in the precision form, 3 per stage in the plain form)",
-    "momentum_adv": "momentum_fused in the precision form (1 launch per stage); momentum_march x, y + "
-                    "momentum_z in the plain form (3 launches)",
-    "rk3+bcs": "rk3_kernel + ghost_fill_kernel",
+    "momentum_adv": "momentum_tile with the u, v, w SSP-RK3 stage in the precision form (1 launch per stage); "
+                    "momentum_march x, y + momentum_z in the plain form (3 launches)",
+    "rk3+bcs": "rk3_kernel (the scalars only in the precision form) + ghost_fill_kernel",
     "pressure": "hmean, fft_x_fwd, fft_y, tdma, fft_x_inv (+ refinement), ghost_sym, correction",
 }
 
@@ -240,23 +244,14 @@ def _time_steps(sim, steps, local_rank, world):
     if world > 1:
         dist.barrier()
     t_start.record(stream)
-    Gr, PV, DV, RS = sim.Gr, sim.PV, sim.DV, sim.RS
     for _ in range(steps):
         for rk in range(3):
+            # the driver's own stage, with events at its component boundaries
+            # (thermo | scalar advection | momentum advection [+ the u, v, w
+            # RK3 stage when fused] | rest of the RK3 stage + ghost fill |
+            # pressure + its ghost fill)
             e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
-            e[0].record(stream)
-            sim.Th.update(Gr, RS, PV, DV)
-            e[1].record(stream)
-            sim.SA.update(Gr, RS, PV, DV)
-            e[2].record(stream)
-            sim.MA.update(Gr, RS, PV)
-            e[3].record(stream)
-            sim.TS.rk_step = rk
-            sim.TS.update(Gr, PV)
-            PV.Update_all_bcs(Gr)
-            e[4].record(stream)
-            sim.Pr.update(Gr, RS, DV, PV)
-            e[5].record(stream)
+            sim.stage(rk, stream, mark=lambda i, e=e: e[i].record(stream))
             ev.append(e)
     t_end.record(stream)
     torch.cuda.synchronize()
@@ -414,7 +409,7 @@ def run_ours(args, rank, world, local_rank):
     comps = {}
     for comp, ms_step in r["component_ms_per_step"].items():
         ms = ms_step / 3.0  # per RK stage
-        nbytes = COMPONENT_BYTES_PER_CELL[comp](nv, cfg)
+        nbytes = COMPONENT_BYTES_PER_CELL[comp](nv, cfg, "fp32" in head)
         ach = nbytes * npl / (ms / 1e3) / 1e9
         comps[comp] = {"ms_per_stage": round(ms, 4), "algorithmic_bytes_per_cell_stage": nbytes,
                        "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4),

@@ -138,6 +138,26 @@ int pb_momentum_advection(const pb_dims* dims, const double* rho0, const double*
                           const double* v, const double* w, double* ut, double* vt, double* wt,
                           int order, int precision, void* stream);
 
+/*
+ * The precision form's momentum advection (as pb_momentum_advection with
+ * PB_FP32) fused with the SSP-RK3 stage of u, v, w (TimeStepping.update_third,
+ * TimeStepping.pyx:131-151) for a step driver that owns the whole stage (no
+ * counterpart in the reference; PB_FP32 arithmetic).  The u and v
+ * tendencies are taken to hold nothing but the advection (they are neither
+ * read nor written); wt holds the w tendency accumulated before the call
+ * (the thermodynamics' buoyancy) and is only read (the caller clears it
+ * before the next stage's accumulation).  The new
+ * interior values go to u_new, v_new, w_new (arrays other than u, v, w:
+ * neighbouring cells are still being read), the stage-0 copies to
+ * u_copy.. at rk_step 0; ghosts of the new arrays are left for the ghost
+ * fill that follows the stage.
+ */
+int pb_momentum_advection_rk3(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                              const double* alpha0, const double* alpha0_half, const double* u,
+                              const double* v, const double* w, double* wt, double* u_new,
+                              double* v_new, double* w_new, double* u_copy, double* v_copy,
+                              double* w_copy, double dt, int rk_step, int order, void* stream);
+
 /* ------------------------------------------------------------------------
  * Thermodynamics
  * --------------------------------------------------------------------- */
@@ -243,6 +263,14 @@ int pb_mlp_adam(float* params, float* m, float* v, const float* grad, int step, 
  */
 int pb_rk3_update(double* values, double* tendencies, double* value_copy, long long n, double dt,
                   int rk_step, void* stream);
+
+/*
+ * pb_rk3_update with the new values written to values_out (which may be
+ * values itself): the out-of-place form used with
+ * pb_momentum_advection_rk3, whose new velocities go to a second buffer.
+ */
+int pb_rk3_update_to(const double* values, double* values_out, double* tendencies, double* value_copy,
+                     long long n, double dt, int rk_step, void* stream);
 
 /*
  * PrognosticVariables.update_all_bcs (PrognosticVariables.pyx:183-233) on

@@ -58,6 +58,8 @@ _DIMS = ctypes.POINTER(PbDims)
 SIGNATURES = {
     "pb_scalar_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _I, _I, _P]),
     "pb_momentum_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P]),
+    "pb_momentum_advection_rk3": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I, _I,
+                                       _P]),
     "pb_thermo_sa": (_I, [_DIMS, _P, _P, ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                           _P, _I, ctypes.POINTER(PbMlp), _P, _I, _I, _P]),
     "pb_eos_sa": (_I, [ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
@@ -67,6 +69,7 @@ SIGNATURES = {
                          ctypes.c_float, _P, _P, _P, _P, _P, _P, _P]),
     "pb_thermo_dry": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "pb_rk3_update": (_I, [_P, _P, _P, _LL, _D, _I, _P]),
+    "pb_rk3_update_to": (_I, [_P, _P, _P, _P, _LL, _D, _I, _P]),
     "pb_update_all_bcs": (_I, [_DIMS, _P, _P, _I, _P]),
     "pb_pressure_workspace_bytes": (_LL, [_DIMS]),
     "pb_pressure_init": (_I, [_DIMS, _P, _LL]),

@@ -15,6 +15,10 @@ cudaError_t momentum_fp32(int order, const Geo& g, const MomArgs& a, cudaStream_
   return order == 5 ? launch_momentum<5, true>(g, a, st) : launch_momentum<7, true>(g, a, st);
 }
 
+cudaError_t momentum_rk3_fp32(int order, const Geo& g, const MomArgs& a, cudaStream_t st) {
+  return order == 5 ? launch_momentum_rk3<5>(g, a, st) : launch_momentum_rk3<7>(g, a, st);
+}
+
 }  // namespace pbadv
 
 namespace {
@@ -100,5 +104,41 @@ extern "C" int pb_momentum_advection(const pb_dims* dims, const double* rho0, co
   cudaStream_t st = as_stream(stream);
   cudaError_t e;
   e = precision == PB_FP64 ? pbadv::momentum_fp64(order, g, a, st) : pbadv::momentum_fp32(order, g, a, st);
+  return e == cudaSuccess ? PB_OK : PB_ERR_CUDA;
+}
+
+extern "C" int pb_momentum_advection_rk3(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                                         const double* alpha0, const double* alpha0_half, const double* u,
+                                         const double* v, const double* w, double* wt, double* u_new,
+                                         double* v_new, double* w_new, double* u_copy, double* v_copy,
+                                         double* w_copy, double dt, int rk_step, int order, void* stream) {
+  int rc = pb_check_dims(dims);
+  if (rc) return rc;
+  if (!rho0 || !rho0_half || !alpha0 || !alpha0_half || !u || !v || !w || !wt || !u_new || !v_new || !w_new ||
+      !u_copy || !v_copy || !w_copy)
+    return PB_ERR_ARG;
+  if (rk_step < 0 || rk_step > 2) return PB_ERR_ARG;
+  if ((rc = check_order(dims, order))) return rc;
+  // the new values go to other arrays than the ones the stencils read
+  if (u_new == u || v_new == v || w_new == w) return PB_ERR_ARG;
+  const Geo g = make_geo(dims);
+  MomArgs a{};
+  a.vel[0] = u;
+  a.vel[1] = v;
+  a.vel[2] = w;
+  a.tend[2] = wt;
+  a.rho0 = rho0;
+  a.rho0_half = rho0_half;
+  a.alpha0 = alpha0;
+  a.alpha0_half = alpha0_half;
+  a.vnew[0] = u_new;
+  a.vnew[1] = v_new;
+  a.vnew[2] = w_new;
+  a.copy[0] = u_copy;
+  a.copy[1] = v_copy;
+  a.copy[2] = w_copy;
+  a.dt = dt;
+  a.stage = rk_step;
+  const cudaError_t e = pbadv::momentum_rk3_fp32(order, g, a, as_stream(stream));
   return e == cudaSuccess ? PB_OK : PB_ERR_CUDA;
 }

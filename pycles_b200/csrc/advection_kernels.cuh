@@ -44,6 +44,12 @@ struct MomArgs {
   const double* rho0_half;
   const double* alpha0;
   const double* alpha0_half;
+  // the SSP-RK3 stage fused into the precision form's momentum pass
+  // (momentum_tile<ORDER, true>): new values, the stage-0 copies, dt, stage
+  double* vnew[3];
+  double* copy[3];
+  double dt;
+  int stage;
 };
 
 template <int ORDER>
@@ -412,7 +418,16 @@ __device__ __forceinline__ double interp_n(const double* p) {  // p[0 .. NI-1]
     return interp_6<double>(p[0], p[1], p[2], p[3], p[4], p[5]);
 }
 
-template <int ORDER>
+// RK: the cell's SSP-RK3 stage (TimeStepping.update_third,
+// TimeStepping.pyx:131-151, the same separately rounded operations as
+// rk3_kernel) is applied here instead of a separate pass: the u and v
+// tendencies are never stored (they start from zero and are complete in
+// registers), the w tendency (the thermodynamics' buoyancy) is read, and
+// the new values go to a second buffer (neighbouring blocks still read the
+// old ones), with the stage-0 copies written here.
+// Only interior cells are written; the ghost fill that follows the stage
+// overwrites the ghosts.
+template <int ORDER, bool RK>
 __global__ void __launch_bounds__(MomTile<ORDER>::NT, 1) momentum_tile(Geo g, MomArgs a, int chunk) {
   using T = MomTile<ORDER>;
   constexpr int R = T::R, NI = T::NI, HI = T::HI, NX = T::NX, NKP = T::NKP;
@@ -474,7 +489,7 @@ __global__ void __launch_bounds__(MomTile<ORDER>::NT, 1) momentum_tile(Geo g, Mo
   // x windows: face f = c0 - 1 reads phi[f-R+1 .. f+R]
   float dl[3][ND];
   double ph[3][NX];  // phi[f-HI .. f+R]
-  double nxt[3], hv[3][T::HPT], tcur[3];
+  double nxt[3], hv[3][T::HPT], tcur[3], ccur[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     double wv[2 * R];
@@ -487,7 +502,8 @@ __global__ void __launch_bounds__(MomTile<ORDER>::NT, 1) momentum_tile(Geo g, Mo
     nxt[c] = own_ok ? a.vel[c][(c0 + R) * g.is + jk] : 0.0;
 #pragma unroll
     for (int q = 0; q < T::HPT; ++q) hv[c][q] = hg[q] >= 0 ? a.vel[c][(c0 - 1) * g.is + hg[q]] : 0.0;
-    tcur[c] = cell ? a.tend[c][c0 * g.is + jk] : 0.0;
+    tcur[c] = (cell && (!RK || c == 2)) ? a.tend[c][c0 * g.is + jk] : 0.0;
+    ccur[c] = (RK && cell && a.stage > 0) ? a.copy[c][c0 * g.is + jk] : 0.0;
   }
   double fxp[3] = {0.0, 0.0, 0.0};
 
@@ -583,13 +599,31 @@ __global__ void __launch_bounds__(MomTile<ORDER>::NT, 1) momentum_tile(Geo g, Mo
     const bool upd = cell && f >= c0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+      const long long at = f * g.is + jk;
       if (upd) {
         const double al = (c == 2) ? al_f : al_h;
         double t = fma(-al * g.dxi1, fy[c][w][lane] - fy[c][w - 1][lane], tx[c]);
         t = fma(-al * g.dxi2, dFz[c], t);
-        a.tend[c][f * g.is + jk] = t;
+        if constexpr (RK) {
+          const double val = ph[c][HI];
+          double nv;
+          if (a.stage == 0) {
+            a.copy[c][at] = val;
+            nv = add_rn(val, mul_rn(t, a.dt));
+          } else if (a.stage == 1) {
+            nv = add_rn(mul_rn(0.75, ccur[c]), mul_rn(0.25, add_rn(val, mul_rn(t, a.dt))));
+          } else {
+            nv = add_rn(mul_rn(1.0 / 3.0, ccur[c]), mul_rn(2.0 / 3.0, add_rn(val, mul_rn(t, a.dt))));
+          }
+          a.vnew[c][at] = nv;
+        } else {
+          a.tend[c][at] = t;
+        }
       }
-      if (cell && f + 1 < c1) tcur[c] = a.tend[c][(f + 1) * g.is + jk];
+      if (cell && f + 1 < c1) {
+        if (!RK || c == 2) tcur[c] = a.tend[c][at + g.is];
+        if (RK && a.stage > 0) ccur[c] = a.copy[c][at + g.is];
+      }
     }
     // (f) advance the x windows by one cell
 #pragma unroll
@@ -685,8 +719,8 @@ cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
   dim3 blk(32, 4);
   if constexpr (F32) {  // precision form: one pass for the three advecting directions
     using T = MomTile<ORDER>;
-    momentum_tile<ORDER><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, kChunk)), T::NT, 0, st>>>(
-        g, a, kChunk);
+    momentum_tile<ORDER, false><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, kChunk)), T::NT, 0,
+                                  st>>>(g, a, kChunk);
     pb_note_launch();
     return cudaGetLastError();
   } else {
@@ -702,6 +736,17 @@ cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
   }
 }
 
+// The precision form's momentum pass with the SSP-RK3 stage fused in.
+template <int ORDER>
+cudaError_t launch_momentum_rk3(const Geo& g, const MomArgs& a, cudaStream_t st) {
+  const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
+  using T = MomTile<ORDER>;
+  momentum_tile<ORDER, true><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, kChunk)), T::NT, 0, st>>>(
+      g, a, kChunk);
+  pb_note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 // FP64 plain form (advection_f64.cu) and FP32 precision form (advection.cu).
@@ -711,5 +756,6 @@ cudaError_t scalar_fp32(int order, int ns, const Geo& g, ScalarArgs base, double
                         const double* const vel[3], cudaStream_t st);
 cudaError_t momentum_fp64(int order, const Geo& g, const MomArgs& a, cudaStream_t st);
 cudaError_t momentum_fp32(int order, const Geo& g, const MomArgs& a, cudaStream_t st);
+cudaError_t momentum_rk3_fp32(int order, const Geo& g, const MomArgs& a, cudaStream_t st);
 
 }  // namespace pbadv

@@ -25,12 +25,14 @@ namespace {
 
 // TimeStepping.update_third (TimeStepping.pyx:131-151), streaming over
 // nv*npg values (ghosts included), two values per thread iteration.
+// The result goes to vout (the values array itself, or a second buffer).
 template <int STAGE>
-__global__ void __launch_bounds__(256) rk3_kernel(double* __restrict__ v, double* __restrict__ t,
+__global__ void __launch_bounds__(256) rk3_kernel(const double* v, double* vout, double* __restrict__ t,
                                                    double* __restrict__ c, long long n, double dt) {
   const long long n2 = n >> 1;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  double2* v2 = reinterpret_cast<double2*>(v);
+  const double2* v2 = reinterpret_cast<const double2*>(v);
+  double2* o2 = reinterpret_cast<double2*>(vout);
   double2* t2 = reinterpret_cast<double2*>(t);
   double2* c2 = reinterpret_cast<double2*>(c);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) {
@@ -49,18 +51,19 @@ __global__ void __launch_bounds__(256) rk3_kernel(double* __restrict__ v, double
       vv.x = add_rn(mul_rn(a, cc.x), mul_rn(b, add_rn(vv.x, mul_rn(tt.x, dt))));
       vv.y = add_rn(mul_rn(a, cc.y), mul_rn(b, add_rn(vv.y, mul_rn(tt.y, dt))));
     }
-    v2[i] = vv;
+    o2[i] = vv;
     t2[i] = make_double2(0.0, 0.0);
   }
   if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
     const long long i = n - 1;
+    const double vi = v[i];
     if (STAGE == 0) {
-      c[i] = v[i];
-      v[i] = add_rn(v[i], mul_rn(t[i], dt));
+      c[i] = vi;
+      vout[i] = add_rn(vi, mul_rn(t[i], dt));
     } else if (STAGE == 1) {
-      v[i] = add_rn(mul_rn(0.75, c[i]), mul_rn(0.25, add_rn(v[i], mul_rn(t[i], dt))));
+      vout[i] = add_rn(mul_rn(0.75, c[i]), mul_rn(0.25, add_rn(vi, mul_rn(t[i], dt))));
     } else {
-      v[i] = add_rn(mul_rn(1.0 / 3.0, c[i]), mul_rn(2.0 / 3.0, add_rn(v[i], mul_rn(t[i], dt))));
+      vout[i] = add_rn(mul_rn(1.0 / 3.0, c[i]), mul_rn(2.0 / 3.0, add_rn(vi, mul_rn(t[i], dt))));
     }
     t[i] = 0.0;
   }
@@ -156,25 +159,35 @@ static int grid_blocks(long long work, int threads) {
   return (int)b;
 }
 
-extern "C" int pb_rk3_update(double* values, double* tendencies, double* value_copy, long long n, double dt,
-                             int rk_step, void* stream) {
-  if (!values || !tendencies || !value_copy || n < 0) return PB_ERR_ARG;
+static int rk3_launch(const double* values, double* out, double* tendencies, double* value_copy, long long n,
+                      double dt, int rk_step, void* stream) {
+  if (!values || !out || !tendencies || !value_copy || n < 0) return PB_ERR_ARG;
   if (rk_step < 0 || rk_step > 2) return PB_ERR_ARG;
-  if ((reinterpret_cast<uintptr_t>(values) | reinterpret_cast<uintptr_t>(tendencies) |
-       reinterpret_cast<uintptr_t>(value_copy)) & 15)
+  if ((reinterpret_cast<uintptr_t>(values) | reinterpret_cast<uintptr_t>(out) |
+       reinterpret_cast<uintptr_t>(tendencies) | reinterpret_cast<uintptr_t>(value_copy)) & 15)
     return PB_ERR_ARG;
   if (n == 0) return PB_OK;
   cudaStream_t st = as_stream(stream);
   const int blocks = grid_blocks((n + 1) / 2, 256);
   if (rk_step == 0)
-    rk3_kernel<0><<<blocks, 256, 0, st>>>(values, tendencies, value_copy, n, dt);
+    rk3_kernel<0><<<blocks, 256, 0, st>>>(values, out, tendencies, value_copy, n, dt);
   else if (rk_step == 1)
-    rk3_kernel<1><<<blocks, 256, 0, st>>>(values, tendencies, value_copy, n, dt);
+    rk3_kernel<1><<<blocks, 256, 0, st>>>(values, out, tendencies, value_copy, n, dt);
   else
-    rk3_kernel<2><<<blocks, 256, 0, st>>>(values, tendencies, value_copy, n, dt);
+    rk3_kernel<2><<<blocks, 256, 0, st>>>(values, out, tendencies, value_copy, n, dt);
   pb_note_launch();
   PB_LAUNCH_CHECK();
   return PB_OK;
+}
+
+extern "C" int pb_rk3_update(double* values, double* tendencies, double* value_copy, long long n, double dt,
+                             int rk_step, void* stream) {
+  return rk3_launch(values, values, tendencies, value_copy, n, dt, rk_step, stream);
+}
+
+extern "C" int pb_rk3_update_to(const double* values, double* values_out, double* tendencies,
+                                double* value_copy, long long n, double dt, int rk_step, void* stream) {
+  return rk3_launch(values, values_out, tendencies, value_copy, n, dt, rk_step, stream);
 }
 
 extern "C" int pb_update_all_bcs(const pb_dims* dims, double* values, const double* bc_factor, int nv,

@@ -8,6 +8,8 @@ the components built here, in the reference's order per RK stage.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -74,6 +76,7 @@ class HotPathSimulation:
         self.SA.initialize(Gr, PV)
         self.MA.initialize(Gr, PV)
         self.TS.initialize(namelist, PV)
+        self.fuse_rk = True  # precision form: SSP-RK3 stage inside the momentum pass
         _capi.load()
 
     # state ---------------------------------------------------------------
@@ -94,20 +97,88 @@ class HotPathSimulation:
         return {n: self.PV.field(n, self.Gr).cpu().numpy() for n in self.PV.index_name}
 
     # time stepping ---------------------------------------------------------
-    def stage(self, rk_step: int, stream=None):
-        """One RK stage in the order of Simulation3d.pyx:159-178."""
+    def stage(self, rk_step: int, stream=None, mark=None):
+        """One RK stage in the order of Simulation3d.pyx:159-178.  mark(i),
+        if given, is called at the component boundaries (i = 0 before the
+        thermodynamics, 1 after it, 2 after the scalar advection, 3 after the
+        momentum advection -- with the u, v, w stage when fused --, 4 after
+        the remaining RK3 stage and the ghost fill, 5 after the pressure
+        solve and its ghost fill)."""
         Gr, PV, DV, RS = self.Gr, self.PV, self.DV, self.RS
+        m = mark if mark is not None else (lambda i: None)
+        m(0)
         self.Th.update(Gr, RS, PV, DV, stream=stream)
+        m(1)
         self.SA.update(Gr, RS, PV, DV, stream=stream)
-        self.MA.update(Gr, RS, PV, stream=stream)
-        self.TS.rk_step = rk_step
-        self.TS.update(Gr, PV, stream=stream)
+        m(2)
+        self._momentum_and_step(rk_step, stream, m)
         PV.Update_all_bcs(Gr, stream=stream)
+        m(4)
         # PressureSolver.update: the solve, then its ghost fill -- of the
         # velocities only, the one thing the correction changed (the
         # scalars' ghosts are the ones filled just above)
         self.Pr.solve(Gr, RS, DV, PV, stream=stream)
         self._fill_velocity_ghosts(stream)
+        m(5)
+
+    def _fused(self) -> bool:
+        """The precision form steps with the SSP-RK3 stage fused into the
+        momentum pass (velocities u, v, w first, as this driver adds them)
+        unless fuse_rk is off."""
+        return self.fuse_rk and self.MA.precision == _capi.PB_FP32
+
+    def _clear_w_tendency(self, stream=None):
+        """Fused stepping: the w tendency is cleared once the fused pass has
+        consumed it, as TimeStepping.update clears every tendency after the
+        stage (the other tendencies: the scalars' by their out-of-place
+        stage, u's and v's are never stored)."""
+        npg = self.Gr.dims.npg
+        w = int(self.PV.velocity_directions[2])
+        st = stream if stream is not None else torch.cuda.current_stream(self.PV.values.device)
+        with torch.cuda.stream(st):
+            self.PV.tendencies[w * npg:(w + 1) * npg].zero_()
+
+    def _momentum_and_step(self, rk_step: int, stream=None, mark=None):
+        """Momentum advection and the SSP-RK3 stage of all prognostic
+        variables (mark(3) between the two).  Fused stepping: the momentum
+        pass applies the stage to u, v, w and writes them to a second
+        buffer, the scalars' stage goes to the same buffer, and the two
+        buffers swap roles."""
+        Gr, PV, RS, TS = self.Gr, self.PV, self.RS, self.TS
+        m = mark if mark is not None else (lambda i: None)
+        TS.rk_step = rk_step
+        if not self._fused():
+            self.MA.update(Gr, RS, PV, stream=stream)
+            m(3)
+            TS.update(Gr, PV, stream=stream)
+            return
+        if [int(i) for i in PV.velocity_directions] != [0, 1, 2]:
+            raise ValueError("fused stepping expects u, v, w as the first prognostic variables")
+        npg = Gr.dims.npg
+        nxt = getattr(self, "_values_next", None)
+        if nxt is None or nxt.shape != PV.values.shape or nxt.device != PV.values.device:
+            nxt = self._values_next = torch.zeros_like(PV.values)
+        cp = TS.value_copies.view(-1)
+        L = _capi.load()
+        sh = _capi.stream_handle(stream)
+        rc = L.pb_momentum_advection_rk3(
+            ctypes.byref(Gr.dims), _capi.ptr(RS.d_rho0), _capi.ptr(RS.d_rho0_half), _capi.ptr(RS.d_alpha0),
+            _capi.ptr(RS.d_alpha0_half), _capi.ptr(PV.values[0:]), _capi.ptr(PV.values[npg:]),
+            _capi.ptr(PV.values[2 * npg:]), _capi.ptr(PV.tendencies[2 * npg:]), _capi.ptr(nxt[0:]),
+            _capi.ptr(nxt[npg:]), _capi.ptr(nxt[2 * npg:]), _capi.ptr(cp[0:]), _capi.ptr(cp[npg:]),
+            _capi.ptr(cp[2 * npg:]), TS.dt, rk_step, self.MA.order, sh)
+        _capi.check(rc, "pb_momentum_advection_rk3")
+        self._clear_w_tendency(stream)
+        m(3)
+        ns = PV.nv - 3
+        if ns > 0:
+            rc = L.pb_rk3_update_to(_capi.ptr(PV.values[3 * npg:]), _capi.ptr(nxt[3 * npg:]),
+                                    _capi.ptr(PV.tendencies[3 * npg:]), _capi.ptr(cp[3 * npg:]), ns * npg, TS.dt,
+                                    rk_step, sh)
+            _capi.check(rc, "pb_rk3_update_to")
+        PV.values, self._values_next = nxt, PV.values
+        if rk_step == 2:
+            TS.t += TS.dt
 
     def _fill_velocity_ghosts(self, stream=None):
         """Ghost fill of the velocities alone when they are the first
@@ -169,29 +240,28 @@ class HotPathSimulation:
             e_all = event(h2d)
         st.wait_event(e_sc)
         last = self.TS.n_rk_steps - 1
+        out = {}
+
+        def hooks(rk):
+            def mark(i):
+                if i == 1 and rk == 0:
+                    st.wait_event(e_all)  # the velocities' upload, overlapped with the thermodynamics
+                elif i == 4 and rk == last:
+                    # the scalars are final: download them during the pressure solve
+                    d2h.wait_event(event(st))
+                    with torch.cuda.stream(d2h):
+                        copy(host_values, PV.values, nvel, nv)
+                        out["sc"] = event(d2h)
+                elif i == 5 and rk == last:
+                    d2h.wait_event(event(st))
+                    with torch.cuda.stream(d2h):
+                        copy(host_values, PV.values, 0, nvel)
+                        out["vel"] = event(d2h)
+            return mark
+
         for rk in range(self.TS.n_rk_steps):
-            self.Th.update(Gr, RS, PV, DV, stream=st)
-            if rk == 0:
-                st.wait_event(e_all)
-            self.SA.update(Gr, RS, PV, DV, stream=st)
-            self.MA.update(Gr, RS, PV, stream=st)
-            self.TS.rk_step = rk
-            self.TS.update(Gr, PV, stream=st)
-            PV.Update_all_bcs(Gr, stream=st)
-            if rk < last:
-                self.Pr.solve(Gr, RS, DV, PV, stream=st)
-                PV.update_bcs_range(Gr, 0, nvel, stream=st)
-                continue
-            d2h.wait_event(event(st))
-            with torch.cuda.stream(d2h):
-                copy(host_values, PV.values, nvel, nv)
-                e_sc_out = event(d2h)
-            self.Pr.solve(Gr, RS, DV, PV, stream=st)
-            PV.update_bcs_range(Gr, 0, nvel, stream=st)
-            d2h.wait_event(event(st))
-            with torch.cuda.stream(d2h):
-                copy(host_values, PV.values, 0, nvel)
-                e_vel_out = event(d2h)
+            self.stage(rk, st, mark=hooks(rk))
+        e_sc_out, e_vel_out = out["sc"], out["vel"]
         self._host_events = (e_sc_out, e_vel_out)
 
     def copy_streams(self):
