@@ -62,25 +62,29 @@ COMPONENT_BYTES_PER_CELL = {
     # buoyancy, theta_rho, bvf, thetali, w-tendency.  dry: read s,
     # w-tendency; write T, alpha, buoyancy, theta, bvf, w-tendency.
     "thermo": lambda nv, cfg, fused: 112.0 if cfg["case"] != "dry_cbl" else 64.0,
-    # read u, v, w and the scalars, read-modify-write the scalar tendencies
-    "scalar_adv": lambda nv, cfg, fused: 8.0 * nv + 16.0 * (nv - 3),
+    # read u, v, w and the scalars, read-modify-write the scalar tendencies;
+    # fused: read u, v, w and the scalars, write the new scalars, write
+    # (stage 0) or read the copies
+    "scalar_adv": lambda nv, cfg, fused: 24.0 + 24.0 * (nv - 3) if fused else 8.0 * nv + 16.0 * (nv - 3),
     # read u, v, w, read-modify-write the three momentum tendencies; fused:
     # read u, v, w and the w tendency, write the new u, v, w, write (stage 0)
     # or read the copies, clear the w tendency
     "momentum_adv": lambda nv, cfg, fused: 88.0 if fused else 72.0,
     # SSP-RK3 stage (read value, tendency, copy; write value, copy,
-    # zeroed tendency: 40 B per variable; fused: the scalars only) + ghost fill
-    "rk3+bcs": lambda nv, cfg, fused: 40.0 * (nv - 3 if fused else nv) + _ghost_bytes(nv, cfg),
+    # zeroed tendency: 40 B per variable; fused: inside the advection
+    # passes) + ghost fill
+    "rk3+bcs": lambda nv, cfg, fused: (0.0 if fused else 40.0 * nv) + _ghost_bytes(nv, cfg),
     # read u, v, w; write u, v, w, divergence, pressure
     "pressure": lambda nv, cfg, fused: 64.0,
 }
 COMPONENT_KERNELS = {
     "thermo": "thermo_sa_kernel (saturation adjustment, buoyancy, bvf, thetali; one launch per stage)",
     "scalar_adv": "scalar_march x, y + scalar_z (WENO fluxes + divergence; 3 launches per stage and scalar "
-                  "in the precision form, 3 per stage in the plain form)",
+                  "in the precision form, the scalars' SSP-RK3 stage in scalar_z; 3 per stage in the plain form)",
     "momentum_adv": "momentum_tile with the u, v, w SSP-RK3 stage in the precision form (1 launch per stage); "
                     "momentum_march x, y + momentum_z in the plain form (3 launches)",
-    "rk3+bcs": "rk3_kernel (the scalars only in the precision form) + ghost_fill_kernel",
+    "rk3+bcs": "rk3_kernel + ghost_fill_kernel (the precision form: the ghost fill alone, its stage is "
+               "inside the advection passes)",
     "pressure": "hmean, fft_x_fwd, fft_y, tdma, fft_x_inv (+ refinement), ghost_sym, correction",
 }
 

@@ -126,6 +126,25 @@ int pb_scalar_advection(const pb_dims* dims, const double* rho0, const double* r
                         int order, int precision, void* stream);
 
 /*
+ * The precision form's scalar advection (as pb_scalar_advection with
+ * PB_FP32, no flux output) fused with the scalars' SSP-RK3 stage
+ * (TimeStepping.update_third, TimeStepping.pyx:131-151) for a step driver
+ * that owns the whole stage (no counterpart in the reference).  The
+ * tendencies are taken to hold nothing but the advection: the x pass stores
+ * its term, the y pass adds, the z pass applies the stage; they are left
+ * holding the x and y terms.  New interior values go to new_values[i]
+ * (arrays other than scalars[i]), the stage-0 copies to copies[i]; ghosts
+ * are left for the ghost fill that follows the stage.  HOST arrays of
+ * device pointers, as for pb_scalar_advection.
+ */
+int pb_scalar_advection_rk3(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                            const double* alpha0, const double* alpha0_half, const double* u,
+                            const double* v, const double* w, int nscalars,
+                            const double* const* scalars, double* const* tendencies,
+                            double* const* new_values, double* const* copies, double dt, int rk_step,
+                            int order, void* stream);
+
+/*
  * MomentumAdvection.update (MomentumAdvection.pyx:41-69): for advected
  * component a and advecting direction d (a, d = 0..2 in that order),
  * compute_advective_tendencies_m (Csrc/momentum_advection.h:13-93; WENO5

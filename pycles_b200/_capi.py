@@ -58,6 +58,7 @@ _DIMS = ctypes.POINTER(PbDims)
 SIGNATURES = {
     "pb_scalar_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _I, _I, _P]),
     "pb_momentum_advection": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P]),
+    "pb_scalar_advection_rk3": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _D, _I, _I, _P]),
     "pb_momentum_advection_rk3": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I, _I,
                                        _P]),
     "pb_thermo_sa": (_I, [_DIMS, _P, _P, ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,

@@ -80,6 +80,47 @@ extern "C" int pb_scalar_advection(const pb_dims* dims, const double* rho0, cons
   return PB_OK;
 }
 
+extern "C" int pb_scalar_advection_rk3(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                                       const double* alpha0, const double* alpha0_half, const double* u,
+                                       const double* v, const double* w, int nscalars,
+                                       const double* const* scalars, double* const* tendencies,
+                                       double* const* new_values, double* const* copies, double dt, int rk_step,
+                                       int order, void* stream) {
+  int rc = pb_check_dims(dims);
+  if (rc) return rc;
+  if (!rho0 || !rho0_half || !alpha0 || !alpha0_half || !u || !v || !w) return PB_ERR_ARG;
+  if (nscalars < 0 || (nscalars > 0 && (!scalars || !tendencies || !new_values || !copies))) return PB_ERR_ARG;
+  if (rk_step < 0 || rk_step > 2) return PB_ERR_ARG;
+  if ((rc = check_order(dims, order))) return rc;
+  if (nscalars == 0) return PB_OK;
+  const Geo g = make_geo(dims);
+  cudaStream_t st = as_stream(stream);
+  const double* vel[3] = {u, v, w};
+  for (int s0 = 0; s0 < nscalars; s0 += kMaxScalars) {
+    const int ns = (nscalars - s0 < kMaxScalars) ? nscalars - s0 : kMaxScalars;
+    ScalarArgs a{};
+    a.rho0 = rho0;
+    a.rho0_half = rho0_half;
+    a.alpha0_half = alpha0_half;
+    a.ns = ns;
+    a.fused = 1;
+    a.dt = dt;
+    a.stage = rk_step;
+    for (int q = 0; q < ns; ++q) {
+      const int i = s0 + q;
+      if (!scalars[i] || !tendencies[i] || !new_values[i] || !copies[i] || new_values[i] == scalars[i])
+        return PB_ERR_ARG;
+      a.s[q] = scalars[i];
+      a.t[q] = tendencies[i];
+      a.vnew[q] = new_values[i];
+      a.copy[q] = copies[i];
+    }
+    double* const* fdir[3] = {nullptr, nullptr, nullptr};
+    if (pbadv::scalar_fp32(order, ns, g, a, fdir, vel, st) != cudaSuccess) return PB_ERR_CUDA;
+  }
+  return PB_OK;
+}
+
 extern "C" int pb_momentum_advection(const pb_dims* dims, const double* rho0, const double* rho0_half,
                                      const double* alpha0, const double* alpha0_half, const double* u,
                                      const double* v, const double* w, double* ut, double* vt, double* wt,

@@ -35,6 +35,14 @@ struct ScalarArgs {
   double* t[kMaxScalars];
   double* flux[kMaxScalars];   // this direction's flux slab or nullptr
   int ns;
+  // the SSP-RK3 stage fused into the precision form's scalar passes (one
+  // scalar per launch): the x pass sets the tendency, the z pass applies
+  // the stage and writes the new value and (stage 0) the copy
+  int fused;
+  double* vnew[kMaxScalars];
+  double* copy[kMaxScalars];
+  double dt;
+  int stage;
 };
 
 struct MomArgs {
@@ -154,7 +162,10 @@ __global__ void __launch_bounds__(128) scalar_z(Geo g, ScalarArgs a) {
 // centres, now and for the next R faces); each new cell costs one FP64
 // subtraction and one rounding to FP32.  Face flux vel * phi_face * rho, the
 // tendency update t -= (alpha dxi) (F - F_prev).
-template <int D, int ORDER>
+// SET: the pass is the first to touch the tendency in the stage (fused
+// stepping), so it stores the x term instead of adding it to the stored
+// value (0 - x, as the reference's accumulation into a zeroed tendency).
+template <int D, int ORDER, bool SET>
 __global__ void __launch_bounds__(128) scalar_march_f32(Geo g, ScalarArgs a, int chunk) {
   constexpr int R = St<ORDER>::R;
   constexpr int ND = 2 * R - 1;
@@ -189,7 +200,7 @@ __global__ void __launch_bounds__(128) scalar_march_f32(Geo g, ScalarArgs a, int
   }
   double nxt = phi[(c0 + R) * sD];
   double vnxt = vel[(c0 - 1) * sD];
-  double tnxt = tend[c0 * sD];
+  double tnxt = SET ? 0.0 : tend[c0 * sD];
   double fprev = 0.0;
   for (long long f = c0 - 1; f < c1; ++f) {
     const double u = vnxt;
@@ -200,7 +211,7 @@ __global__ void __launch_bounds__(128) scalar_march_f32(Geo g, ScalarArgs a, int
     // stays in bounds)
     if (f + 1 < c1) {
       vnxt = vel[(f + 1) * sD];
-      tnxt = tend[(f + 1) * sD];
+      if (!SET) tnxt = tend[(f + 1) * sD];
     }
     if (f + 2 < c1) nxt = phi[(f + 2 + R) * sD];
     const bool pos = u >= 0.0;
@@ -220,7 +231,12 @@ __global__ void __launch_bounds__(128) scalar_march_f32(Geo g, ScalarArgs a, int
 
 // z: lane L takes face f = k0 - 1 + L from the 2R values around it (L1
 // hits: the warp's lanes overlap) and the lower face's flux from lane L-1.
-template <int ORDER>
+// RK: the last pass over the tendency in fused stepping -- the cell's
+// SSP-RK3 stage (the separately rounded operations of rk3_kernel) is
+// applied here, the new value written to a.vnew (the stencils of other
+// warps still read the current values) and, at stage 0, the copy; the
+// tendency is not stored.
+template <int ORDER, bool RK>
 __global__ void __launch_bounds__(128) scalar_z_f32(Geo g, ScalarArgs a) {
   constexpr int R = St<ORDER>::R;
   constexpr int ND = 2 * R - 1;
@@ -233,7 +249,7 @@ __global__ void __launch_bounds__(128) scalar_z_f32(Geo g, ScalarArgs a) {
   const long long f = g.gw + seg * 31 - 1 + lane;
   const bool valid = f <= g.n2 - g.gw - 1;
   const long long col = i * g.is + j * g.js;
-  double F = 0.0;
+  double F = 0.0, val = 0.0;
   if (valid) {
     const double* s = a.s[0] + col + f - (R - 1);
     double w[2 * R];
@@ -246,9 +262,27 @@ __global__ void __launch_bounds__(128) scalar_z_f32(Geo g, ScalarArgs a) {
     const bool pos = u >= 0.0;
     F = u * ((pos ? w[R - 1] : w[R]) + (double)weno_delta<ORDER>(pos, d)) * a.rho0[f];
     if (a.flux[0] != nullptr) a.flux[0][col + f] = F;
+    val = w[R - 1];
   }
   const double Fm = __shfl_up_sync(0xffffffffu, F, 1);
-  if (valid && lane > 0) a.t[0][col + f] = fma(-a.alpha0_half[f] * g.dxi2, F - Fm, a.t[0][col + f]);
+  if (valid && lane > 0) {
+    const long long at = col + f;
+    const double t = fma(-a.alpha0_half[f] * g.dxi2, F - Fm, a.t[0][at]);
+    if constexpr (RK) {
+      double nv;
+      if (a.stage == 0) {
+        a.copy[0][at] = val;
+        nv = add_rn(val, mul_rn(t, a.dt));
+      } else if (a.stage == 1) {
+        nv = add_rn(mul_rn(0.75, a.copy[0][at]), mul_rn(0.25, add_rn(val, mul_rn(t, a.dt))));
+      } else {
+        nv = add_rn(mul_rn(1.0 / 3.0, a.copy[0][at]), mul_rn(2.0 / 3.0, add_rn(val, mul_rn(t, a.dt))));
+      }
+      a.vnew[0][at] = nv;
+    } else {
+      a.t[0][at] = t;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -650,10 +684,14 @@ cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* fl
     a.vel = vel[0];
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[0] ? flux_dir[0][q] : nullptr;
     dim3 grd(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, kChunk));
-    if constexpr (F32 && NS == 1)
-      scalar_march_f32<0, ORDER><<<grd, blk, 0, st>>>(g, a, kChunk);
-    else
+    if constexpr (F32 && NS == 1) {
+      if (a.fused)
+        scalar_march_f32<0, ORDER, true><<<grd, blk, 0, st>>>(g, a, kChunk);
+      else
+        scalar_march_f32<0, ORDER, false><<<grd, blk, 0, st>>>(g, a, kChunk);
+    } else {
       scalar_march<0, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
+    }
     pb_note_launch();
   }
   {
@@ -662,7 +700,7 @@ cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* fl
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[1] ? flux_dir[1][q] : nullptr;
     dim3 grd(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, kChunk));
     if constexpr (F32 && NS == 1)
-      scalar_march_f32<1, ORDER><<<grd, blk, 0, st>>>(g, a, kChunk);
+      scalar_march_f32<1, ORDER, false><<<grd, blk, 0, st>>>(g, a, kChunk);
     else
       scalar_march<1, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
     pb_note_launch();
@@ -672,10 +710,14 @@ cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* fl
     a.vel = vel[2];
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[2] ? flux_dir[2][q] : nullptr;
     const dim3 grd(ceil_div(nl2, 31), ceil_div(nl1, 4), (unsigned)nl0);
-    if constexpr (F32 && NS == 1)
-      scalar_z_f32<ORDER><<<grd, 128, 0, st>>>(g, a);
-    else
+    if constexpr (F32 && NS == 1) {
+      if (a.fused)
+        scalar_z_f32<ORDER, true><<<grd, 128, 0, st>>>(g, a);
+      else
+        scalar_z_f32<ORDER, false><<<grd, 128, 0, st>>>(g, a);
+    } else {
       scalar_z<ORDER, F32, NS><<<grd, 128, 0, st>>>(g, a);
+    }
     pb_note_launch();
   }
   return cudaGetLastError();
@@ -692,6 +734,8 @@ cudaError_t launch_scalar_ns(int ns, const Geo& g, ScalarArgs base, double* cons
       ScalarArgs a = base;
       a.s[0] = base.s[q];
       a.t[0] = base.t[q];
+      a.vnew[0] = base.vnew[q];
+      a.copy[0] = base.copy[q];
       a.ns = 1;
       double* fq[3][1];
       double* const* fd[3];

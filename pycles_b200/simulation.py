@@ -109,7 +109,10 @@ class HotPathSimulation:
         m(0)
         self.Th.update(Gr, RS, PV, DV, stream=stream)
         m(1)
-        self.SA.update(Gr, RS, PV, DV, stream=stream)
+        if self._fused():
+            self._scalars_and_step(rk_step, stream)
+        else:
+            self.SA.update(Gr, RS, PV, DV, stream=stream)
         m(2)
         self._momentum_and_step(rk_step, stream, m)
         PV.Update_all_bcs(Gr, stream=stream)
@@ -138,11 +141,39 @@ class HotPathSimulation:
         with torch.cuda.stream(st):
             self.PV.tendencies[w * npg:(w + 1) * npg].zero_()
 
+    def _next_values(self):
+        """The second value buffer of fused stepping."""
+        PV = self.PV
+        nxt = getattr(self, "_values_next", None)
+        if nxt is None or nxt.shape != PV.values.shape or nxt.device != PV.values.device:
+            nxt = self._values_next = torch.zeros_like(PV.values)
+        return nxt
+
+    def _scalars_and_step(self, rk_step: int, stream=None):
+        """Fused stepping: scalar advection with the scalars' SSP-RK3 stage,
+        new values into the second buffer."""
+        Gr, PV, RS, TS = self.Gr, self.PV, self.RS, self.TS
+        scal = [i for i in range(PV.nv) if PV.var_type[i] == 1]
+        if not scal:
+            return
+        npg = Gr.dims.npg
+        nxt = self._next_values()
+        cp = TS.value_copies.view(-1)
+        n = len(scal)
+        arr = lambda t: (ctypes.c_void_p * n)(*[_capi.ptr(t[i * npg:]) for i in scal])
+        vel = [PV.values[int(PV.velocity_directions[d]) * npg:] for d in range(3)]
+        rc = _capi.load().pb_scalar_advection_rk3(
+            ctypes.byref(Gr.dims), _capi.ptr(RS.d_rho0), _capi.ptr(RS.d_rho0_half), _capi.ptr(RS.d_alpha0),
+            _capi.ptr(RS.d_alpha0_half), _capi.ptr(vel[0]), _capi.ptr(vel[1]), _capi.ptr(vel[2]), n,
+            arr(PV.values), arr(PV.tendencies), arr(nxt), arr(cp), TS.dt, rk_step, self.SA.order,
+            _capi.stream_handle(stream))
+        _capi.check(rc, "pb_scalar_advection_rk3")
+
     def _momentum_and_step(self, rk_step: int, stream=None, mark=None):
         """Momentum advection and the SSP-RK3 stage of all prognostic
         variables (mark(3) between the two).  Fused stepping: the momentum
-        pass applies the stage to u, v, w and writes them to a second
-        buffer, the scalars' stage goes to the same buffer, and the two
+        pass applies the stage to u, v, w and writes them to the second
+        buffer (the scalar pass has written the scalars there), and the two
         buffers swap roles."""
         Gr, PV, RS, TS = self.Gr, self.PV, self.RS, self.TS
         m = mark if mark is not None else (lambda i: None)
@@ -155,9 +186,7 @@ class HotPathSimulation:
         if [int(i) for i in PV.velocity_directions] != [0, 1, 2]:
             raise ValueError("fused stepping expects u, v, w as the first prognostic variables")
         npg = Gr.dims.npg
-        nxt = getattr(self, "_values_next", None)
-        if nxt is None or nxt.shape != PV.values.shape or nxt.device != PV.values.device:
-            nxt = self._values_next = torch.zeros_like(PV.values)
+        nxt = self._next_values()
         cp = TS.value_copies.view(-1)
         L = _capi.load()
         sh = _capi.stream_handle(stream)
@@ -170,12 +199,6 @@ class HotPathSimulation:
         _capi.check(rc, "pb_momentum_advection_rk3")
         self._clear_w_tendency(stream)
         m(3)
-        ns = PV.nv - 3
-        if ns > 0:
-            rc = L.pb_rk3_update_to(_capi.ptr(PV.values[3 * npg:]), _capi.ptr(nxt[3 * npg:]),
-                                    _capi.ptr(PV.tendencies[3 * npg:]), _capi.ptr(cp[3 * npg:]), ns * npg, TS.dt,
-                                    rk_step, sh)
-            _capi.check(rc, "pb_rk3_update_to")
         PV.values, self._values_next = nxt, PV.values
         if rk_step == 2:
             TS.t += TS.dt
