@@ -350,6 +350,8 @@ def run_ours(args, rank, world, local_rank):
                 trained = _train_seed(sim, fields, log)
             if trained is not None:
                 sim.Th.mlp, seed_info = trained
+                if args.seed_refresh_interval:
+                    sim.Th.seed_refresh_interval = args.seed_refresh_interval
         sim.run(0)  # ghost fill + first thermodynamics update, as Simulation3d.run
         _capi.clear_error()
         for _ in range(args.warmup):
@@ -496,6 +498,8 @@ def run_accuracy(args, cfg):
             trained = trained or _train_seed(sim, fields, log)
             if trained is not None:
                 sim.Th.mlp = trained[0]
+                if args.seed_refresh_interval:
+                    sim.Th.seed_refresh_interval = args.seed_refresh_interval
         sim.run(0)
         sim.step()
         snaps[form] = {1: sim.host_fields()}
@@ -558,6 +562,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cores", type=int, default=None)
+    ap.add_argument("--seed-refresh-interval", type=int, default=0,
+                    help="thermodynamics updates between refreshes of the learned seed (default: the "
+                         "library's, gpu.seed_refresh_interval)")
     ap.add_argument("--accuracy-steps", type=int, default=0,
                     help="instead of timing: run every form N steps from the same state and report each "
                          "field's relative L2 error against the FP64 plain form after 1 and N steps")

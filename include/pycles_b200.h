@@ -198,10 +198,11 @@ int pb_momentum_advection_rk3(const pb_dims* dims, const double* rho0, const dou
  *                           out_scale * seed_y, clamped to the bracket
  *                           [T_1 + (T_2r - T_1)/16, T_2r] of the root (T_1
  *                           the first point :22-24, T_2r the reference's
- *                           second point :39).  Cells newly saturated
- *                           start from an older or zero y: the clamp keeps
- *                           any start safe and the secant's stopping test
- *                           decides the result.
+ *                           second point :39).  The refresh sets seed_y to
+ *                           NaN for the cells it does not evaluate: those
+ *                           (saturated since the last refresh) start from
+ *                           T_2r.  The secant's stopping test decides every
+ *                           result.
  *   secant_iters (nullable): device long long[2]; receives
  *                           {sum of secant iterations, saturated cells}.
  *   max_iter              : secant iteration cap (the reference has none);

@@ -69,7 +69,9 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(FwdArgs a) {
 // chunks of 32 consecutive cells kBatch chunks at a time (kBatch flag loads
 // in flight), appends the flagged cells to a queue in shared memory and
 // evaluates the network whenever the queue holds a full 16-row tile, so the
-// tiles are full except the warp's last one.
+// tiles are full except the warp's last one.  Cells not flagged get NaN: a
+// cell that saturates between refreshes starts its secant from the
+// reference's second point, not from a stale output.
 struct RefreshArgs {
   const __nv_bfloat16* w1;
   const float* b1;
@@ -138,7 +140,11 @@ __global__ void __launch_bounds__(32 * kRefreshWarps) mlp_seed_refresh_kernel(Re
 #pragma unroll
     for (int m = 0; m < kRefreshBatch; ++m) {
       const long long idx = (cb + m * nwarps) * 32 + lane;
-      if ((masks[m] >> lane) & 1u) q[nq + __popc(masks[m] & ((1u << lane) - 1u))] = (int)idx;
+      if ((masks[m] >> lane) & 1u) {
+        q[nq + __popc(masks[m] & ((1u << lane) - 1u))] = (int)idx;
+      } else if (idx < a.npg) {
+        a.y[idx] = __int_as_float(0x7fc00000);  // not evaluated: NaN, the secant takes its own start
+      }
       nq += __popc(masks[m]);
     }
     __syncwarp();

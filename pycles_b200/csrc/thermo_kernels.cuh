@@ -89,7 +89,9 @@ using thermo_k::SaArgs;
 //
 // SEED: each saturated cell starts the secant from
 //   T_2 = T_1 + out_mean + out_scale * y[cell]
-// (clamped in eos_finish), y refreshed by the network kernel beforehand.
+// (clamped in eos_finish), y refreshed by the network kernel beforehand;
+// a cell whose y is NaN (not saturated at the last refresh) takes the
+// reference's second point.
 constexpr int kSeg = 30;
 constexpr int kSaThreads = 256;
 
@@ -138,12 +140,17 @@ __global__ void __launch_bounds__(kSaThreads, 4) thermo_sa_kernel(Geo geo, SaArg
       st = eos_start<M>(a.LT, p0, s, qt, a.err);
     }
     double seed = 0.0;
+    bool seeded = false;
     if constexpr (SEED) {
-      if (kin && st.sat) seed = st.T_1 + (double)a.net.out_mean + (double)a.net.out_scale * (double)a.net.y[idx];
+      if (kin && st.sat) {
+        const float y = a.net.y[idx];  // NaN: not evaluated at the last refresh
+        seeded = isfinite(y);
+        seed = st.T_1 + (double)a.net.out_mean + (double)a.net.out_scale * (double)y;
+      }
     }
     double T = 0.0, qv = 0.0, thr = 0.0, b = 0.0;
     if (kin) {
-      const EosOut e = eos_finish<M>(a.LT, st, p0, s, qt, a.max_iter, SEED && st.sat, seed, a.err);
+      const EosOut e = eos_finish<M>(a.LT, st, p0, s, qt, a.max_iter, SEED && st.sat && seeded, seed, a.err);
       T = e.T;
       qv = e.qv;
       double al;
