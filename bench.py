@@ -312,6 +312,46 @@ def _train_seed(sim, fields, log):
     return mlp, info
 
 
+# surface scheme of each configuration's case (Surface.pyx:39-74)
+SURFACE_OF_CASE = {"dry_cbl": "SullivanPatton", "bomex": "Bomex", "dycoms": "DYCOMS_RF01"}
+
+
+def _time_surface(sim, cfg, peak, calls=50, warm=3):
+    """The surface scheme of the configuration's case on the timed state:
+    CUDA-event time of pb_surface_update (its two kernels) over `calls`
+    calls.  Algorithmic bytes per column: read u, v, T, qt, ql (qt, ql for
+    the moist schemes); write the nine surface arrays and the wind speed;
+    read and write the first-level tendencies of u, v, s (and qt).  Each 3-D
+    field contributes one 8-byte value per column at k = gw, a strided
+    access that moves a 32-byte sector per value."""
+    import torch
+
+    from pycles_b200.surface import SurfaceFactory
+    scheme = SURFACE_OF_CASE[cfg["case"]]
+    sur = SurfaceFactory({"meta": {"casename": scheme}})
+    sur.initialize(sim.Gr, sim.RS)
+    args = (sim.Gr, sim.RS, sim.PV, sim.DV)
+    tend = sim.PV.tendencies.clone()
+    for _ in range(warm):
+        sur.update(*args)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(calls):
+        sur.update(*args)
+    b.record(stream)
+    torch.cuda.synchronize()
+    sim.PV.tendencies.copy_(tend)
+    us = a.elapsed_time(b) * 1e3 / calls
+    moist = scheme != "SullivanPatton"
+    cols = sim.Gr.dims.nlg[0] * sim.Gr.dims.nlg[1]
+    nbytes_col = 8 * (5 if moist else 3) + 8 * 10 + 16 * (4 if moist else 3)
+    ach = nbytes_col * cols / (us * 1e-6) / 1e9
+    return {"scheme": scheme, "us_per_call": round(us, 2), "kernels_per_call": 2, "columns": cols,
+            "algorithmic_bytes_per_column": nbytes_col, "achieved_gbs": round(ach, 1),
+            "frac": round(ach / peak, 4)}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -410,6 +450,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- roofline per component; the headline is the largest one ----------
     peak, peak_kind = _peaks()
+    surface = _time_surface(sim, cfg, peak) if not args.no_surface else None
     r = results[head]
     nv = PV.nv
     comps = {}
@@ -461,6 +502,7 @@ def run_ours(args, rank, world, local_rank):
             "component_ms_per_step": r["component_ms_per_step"],
             "roofline": roofline,
             "e2e": e2e,
+            "surface": surface,
             "gpu_launches": r["gpu_launches"],
             "clocks": r["clocks"],
             "device_error_word": r["device_error_word"],
@@ -561,6 +603,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surface", action="store_true",
+                    help="skip the timing of the case's surface scheme (reported beside the step)")
     ap.add_argument("--cpu-cores", type=int, default=None)
     ap.add_argument("--seed-refresh-interval", type=int, default=0,
                     help="thermodynamics updates between refreshes of the learned seed (default: the "

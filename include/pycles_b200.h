@@ -372,6 +372,86 @@ int pb_pressure_solve_noalloc(const pb_dims* dims, const double* rho0, const dou
                               double* w, double* divergence, double* dynamic_pressure, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Surface fluxes (lowest model level)
+ * --------------------------------------------------------------------- */
+
+/* Surface schemes, as SurfaceFactory (Surface.pyx:39-74) picks them by case. */
+enum pb_surface_scheme {
+  PB_SURFACE_NONE = 0,             /* SurfaceNone (Surface.pyx:203-213)             */
+  PB_SURFACE_SULLIVAN_PATTON = 1,  /* SurfaceSullivanPatton (Surface.pyx:216-294)   */
+  PB_SURFACE_BOMEX = 2,            /* SurfaceBomex (Surface.pyx:297-377)            */
+  PB_SURFACE_DYCOMS_RF01 = 3       /* SurfaceDYCOMS_RF01 (Surface.pyx:474-561)      */
+};
+
+/*
+ * The scheme's constants (the attributes its __init__/initialize set).
+ *   theta_flux : SullivanPatton 0.24, Bomex 8.0e-3 (K m/s)
+ *   z0         : roughness length (SullivanPatton 0.1 m)
+ *   gustiness  : minimum wind speed of compute_windspeed (SullivanPatton
+ *                0.001 m/s, Bomex and DYCOMS_RF01 0)
+ *   ustar      : Bomex's fixed friction velocity ustar_ (0.28 m/s)
+ *   cm, ft, fq : DYCOMS_RF01's bulk drag coefficient (0.0011), sensible and
+ *                latent heat fluxes (15, 115 W/m^2)
+ *   u0, v0     : the reference state's Galilean shift (Ref.u0, Ref.v0)
+ */
+typedef struct pb_surface {
+  int scheme;
+  double theta_flux;
+  double z0;
+  double gustiness;
+  double ustar;
+  double cm, ft, fq;
+  double u0, v0;
+} pb_surface;
+
+/*
+ * The surface arrays of SurfaceBase (Surface.pyx:84-94), device, nlg0*nlg1
+ * doubles each, indexed i*nlg1 + j, owned by the caller and zeroed at
+ * set-up as SurfaceBase.initialize does (Bomex also sets qt_flux to
+ * 5.2e-5, Surface.pyx:305).  windspeed holds compute_windspeed's output;
+ * scratch is PB_SURFACE_SCRATCH doubles for the horizontal mean of the
+ * lowest-level temperature.
+ */
+#define PB_SURFACE_SCRATCH 512
+typedef struct pb_surface_fields {
+  double* u_flux;
+  double* v_flux;
+  double* qt_flux;
+  double* s_flux;
+  double* obukhov_length;
+  double* friction_velocity;
+  double* shf;
+  double* lhf;
+  double* b_flux;
+  double* windspeed;
+  double* scratch;
+} pb_surface_fields;
+
+/*
+ * Surface<scheme>.update followed by SurfaceBase.update (Surface.pyx:116-
+ * 178): wind speed at the lowest level (compute_windspeed,
+ * Csrc/surface.h:157-185), friction velocity (SullivanPatton: the
+ * Monin-Obukhov secant compute_ustar, Csrc/surface.h:34-93; Bomex: fixed;
+ * DYCOMS_RF01: sqrt(cm) * wind speed), entropy and moisture fluxes, momentum
+ * fluxes, then sensible / latent / buoyancy fluxes, Obukhov length and the
+ * tendencies of the first interior level: u, v, s, and qt for the moist
+ * schemes, += flux * alpha0_half[gw] / alpha0[gw-1] / dz.
+ *   T, qt, qv, ql: DiagnosticVariables temperature, qv, ql and the
+ *                  prognostic qt (qt, qv, ql, qt_tend NULL for
+ *                  SullivanPatton, which is dry).
+ * FP64 in both arithmetic forms: the work is one horizontal plane.
+ * compute_ustar returns its first fixed-point iterate from the neutral guess
+ * (`ustar` is assigned before its secant loop, Csrc/surface.h:52,73, and the
+ * loop's result is not used); this computes that value and runs no loop.
+ * PB_SURFACE_NONE returns PB_OK without work.
+ */
+int pb_surface_update(const pb_dims* dims, const pb_surface* surface, const double* p0_half,
+                      const double* alpha0, const double* alpha0_half, const double* rho0_half,
+                      const double* u, const double* v, const double* T, const double* qt, const double* qv,
+                      const double* ql, double* u_tend, double* v_tend, double* s_tend, double* qt_tend,
+                      const pb_surface_fields* fields, void* stream);
+
+/* ------------------------------------------------------------------------
  * Errors
  * --------------------------------------------------------------------- */
 

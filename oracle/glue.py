@@ -3,8 +3,8 @@ TEST INFRASTRUCTURE ONLY.
 
 ``OracleSim`` reproduces one rank of ``Simulation3d.run`` (Simulation3d.pyx:
 140-189) restricted to the hot-path components, in the reference's order per
-RK stage: Th.update, SA.update, MA.update, TS.update, PV.Update_all_bcs,
-Pr.update.  The kernels come from one of two backends:
+RK stage: Th.update, SA.update, MA.update, [Sur.update,] TS.update,
+PV.Update_all_bcs, Pr.update.  The kernels come from one of two backends:
 
 * ``"ref"``  -- the reference's own C (oracle/ref.py), TDMA from the
                reference's cythonized SparseSolvers when it was built;
@@ -157,6 +157,7 @@ class OracleSim:
         self.nscalars = self.nv - 3
         self.flux = np.zeros(self.nscalars * 3 * npg)
         self.secant_iters = None
+        self.surface = None  # an oracle.surface.OracleSurface, updated after MA as Simulation3d.pyx:167
         if moist:
             x, y = table_xy if table_xy is not None else cc_table()
             self.table_xy = (x, y)
@@ -315,6 +316,8 @@ class OracleSim:
         self.th_update()
         self.sa_update()
         self.ma_update()
+        if self.surface is not None:
+            self.surface.update(self)
         self.ts_update(rk_step)
         self.update_all_bcs()
         self.pr_update()

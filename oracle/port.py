@@ -700,3 +700,66 @@ def pressure_correction(d: Dims, p, u, v, w):
     u.reshape(sh)[reg] -= (_sh(P, reg, 0, 1) - Pc) * d.dxi[0]
     v.reshape(sh)[reg] -= (_sh(P, reg, 1, 1) - Pc) * d.dxi[1]
     w.reshape(sh)[reg] -= (_sh(P, reg, 2, 1) - Pc) * d.dxi[2]
+
+
+# ---------------------------------------------------------------------------
+# surface layer, Csrc/surface.h (constants generate_parameters.py:44-49)
+# ---------------------------------------------------------------------------
+vkb = 0.35
+Pr0 = 0.74
+beta_m = 4.7
+beta_h = beta_m / Pr0
+gamma_m = 15.0
+gamma_h = 9.0
+
+
+def psi_m_unstable(zeta, zeta0):
+    """Csrc/surface.h:6-12 (scalars)."""
+    x = math.pow((1.0 - gamma_m * zeta), 0.25)
+    x0 = math.pow((1.0 - gamma_m * zeta0), 0.25)
+    return (2.0 * math.log((1.0 + x) / (1.0 + x0)) + math.log((1.0 + x * x) / (1.0 + x0 * x0))
+            - 2.0 * math.atan(x) + 2.0 * math.atan(x0))
+
+
+def psi_m_stable(zeta, zeta0):
+    """Csrc/surface.h:22-25."""
+    return -beta_m * (zeta - zeta0)
+
+
+def compute_ustar(windspeed, buoyancy_flux, z0, zb):
+    """Csrc/surface.h:34-93 (scalars).  The reference returns ``ustar``, which
+    it sets to the first iterate ustar1 = windspeed vkb / (log(zb/z0) - psi_m)
+    from the neutral guess before its secant loop (:52, :73) and does not
+    update inside it; the loop's iterates never reach the result, so this
+    restatement stops at that iterate."""
+    logz = math.log(zb / z0)
+    ustar0 = windspeed * vkb / logz
+    if not (math.fabs(buoyancy_flux) > 1.0e-20):
+        return ustar0
+    lmo = -ustar0 * ustar0 * ustar0 / (buoyancy_flux * vkb)
+    zeta = zb / lmo
+    zeta0 = z0 / lmo
+    psi = psi_m_stable(zeta, zeta0) if zeta >= 0.0 else psi_m_unstable(zeta, zeta0)
+    return windspeed * vkb / (logz - psi)
+
+
+def compute_windspeed(d: Dims, u, v, speed, u0, v0, gustiness):
+    """Csrc/surface.h:157-185: speed[i*nlg1+j] over i, j >= 1 from the
+    lowest interior level k = gw."""
+    U = u.reshape(d.shape)[:, :, d.gw]
+    V = v.reshape(d.shape)[:, :, d.gw]
+    S = speed.reshape(d.nlg[0], d.nlg[1])
+    ui = interp_2(U[:-1, 1:], U[1:, 1:]) + u0
+    vi = interp_2(V[1:, :-1], V[1:, 1:]) + v0
+    S[1:, 1:] = np.fmax(np.sqrt(ui * ui + vi * vi), gustiness)
+
+
+def entropyflux_from_thetaflux_qtflux(thetaflux, qtflux, p0_b, T_b, qt_b, qv_b):
+    """Csrc/surface.h:95-106 (arrays)."""
+    exner_b = exner_c(p0_b)
+    pd_b = pd_c(p0_b, qt_b, qv_b)
+    pv_b = pv_c(p0_b, qt_b, qv_b)
+    sd_b = sd_c(pd_b, T_b)
+    sv_b = sv_c(pv_b, T_b)
+    cp_b = cpm_c(qt_b)
+    return cp_b * thetaflux * exner_b / T_b + qtflux * (sv_b - sd_b)

@@ -186,3 +186,30 @@ def eos_c(table: Table, p0, s, qt):
 
 def entropy_sa(p0, T, qt, ql, qi):
     return lib().ref_entropy_sa(p0, T, qt, ql, qi)
+
+
+# ---- surface layer (Csrc/surface.h) ---------------------------------------
+def compute_ustar(windspeed, buoyancy_flux, z0, zb):
+    f = lib().ref_compute_ustar
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double] * 4
+    return f(windspeed, buoyancy_flux, z0, zb)
+
+
+def compute_windspeed(d: Dims, u, v, speed, u0, v0, gustiness):
+    dc = d.c()
+    f = lib().ref_compute_windspeed
+    f.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    f(ctypes.byref(dc), _p(u), _p(v), _p(speed), u0, v0, gustiness)
+
+
+def entropyflux_from_thetaflux_qtflux(thetaflux, qtflux, p0_b, T_b, qt_b, qv_b):
+    f = lib().ref_entropyflux
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double] * 6
+    b = np.broadcast_arrays(*[np.asarray(x, dtype=np.float64) for x in (thetaflux, qtflux, p0_b, T_b, qt_b,
+                                                                         qv_b)])
+    out = np.empty(b[0].shape)
+    for idx in np.ndindex(out.shape):
+        out[idx] = f(*[float(x[idx]) for x in b])
+    return out

@@ -15,7 +15,8 @@
  *  - wrappers that pass those pointers, so ctypes can call eos_update,
  *    bvf_sa and thetali_update with plain pointers;
  *  - a LookupStruct constructor (init_table, Csrc/lookup.h:16-40) callable
- *    from ctypes.
+ *    from ctypes;
+ *  - wrappers of the surface-layer functions of Csrc/surface.h.
  * The dry-thermodynamics header defines eos_c/eos_update under the same
  * names as the saturation-adjustment header, so it is included with those
  * two names remapped.
@@ -34,6 +35,7 @@
 #include "momentum_advection.h"
 #include "thermodynamics_sa.h"
 #include "prognostic_variables.h"
+#include "surface.h"
 
 #define eos_c dry_eos_c
 #define eos_update dry_eos_update
@@ -93,3 +95,15 @@ double ref_entropy_sa(double p0, double T, double qt, double ql, double qi) {
 
 double ref_exner(double p0) { return exner_c(p0); }
 double ref_dry_eos(double pd, double s) { return dry_eos_c(pd, s); }
+
+/* ---- surface fluxes (Csrc/surface.h) --------------------------------- */
+double ref_compute_ustar(double windspeed, double buoyancy_flux, double z0, double zb) {
+    return compute_ustar(windspeed, buoyancy_flux, z0, zb);
+}
+void ref_compute_windspeed(struct DimStruct* dims, double* u, double* v, double* speed, double u0, double v0,
+                           double gustiness) {
+    compute_windspeed(dims, u, v, speed, u0, v0, gustiness);
+}
+double ref_entropyflux(double thetaflux, double qtflux, double p0_b, double T_b, double qt_b, double qv_b) {
+    return entropyflux_from_thetaflux_qtflux(thetaflux, qtflux, p0_b, T_b, qt_b, qv_b);
+}

@@ -40,8 +40,25 @@ class PbMlp(ctypes.Structure):
                 ("seed_refresh", ctypes.c_int)]
 
 
+class PbSurface(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("theta_flux", ctypes.c_double), ("z0", ctypes.c_double),
+                ("gustiness", ctypes.c_double), ("ustar", ctypes.c_double), ("cm", ctypes.c_double),
+                ("ft", ctypes.c_double), ("fq", ctypes.c_double), ("u0", ctypes.c_double),
+                ("v0", ctypes.c_double)]
+
+
+SURFACE_FIELDS = ("u_flux", "v_flux", "qt_flux", "s_flux", "obukhov_length", "friction_velocity", "shf",
+                  "lhf", "b_flux", "windspeed", "scratch")
+
+
+class PbSurfaceFields(ctypes.Structure):
+    _fields_ = [(n, _vp) for n in SURFACE_FIELDS]
+
+
 PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_UNSUPPORTED, PB_ERR_WORKSPACE = 0, 1, 2, 3, 4
 PB_FP64, PB_FP32 = 0, 1
+PB_SURFACE_NONE, PB_SURFACE_SULLIVAN_PATTON, PB_SURFACE_BOMEX, PB_SURFACE_DYCOMS_RF01 = 0, 1, 2, 3
+PB_SURFACE_SCRATCH = 512
 
 
 def precision_of(namelist) -> int:
@@ -76,6 +93,8 @@ SIGNATURES = {
     "pb_pressure_init": (_I, [_DIMS, _P, _LL]),
     "pb_pressure_solve": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _I, _P]),
     "pb_pressure_solve_noalloc": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pb_surface_update": (_I, [_DIMS, ctypes.POINTER(PbSurface), _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                               _P, _P, ctypes.POINTER(PbSurfaceFields), _P]),
     "pb_get_error": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "pb_clear_error": (_I, [_P]),
     "pb_status_string": (ctypes.c_char_p, [_I]),

@@ -47,12 +47,12 @@ def nvcc() -> str:
     return "nvcc"
 
 
-# Translation units and their extra flags.  The thermodynamics and the FP64
-# plain-form advection are compiled without FMA contraction so that they
+# Translation units and their extra flags.  The thermodynamics, the FP64
+# plain-form advection and the surface fluxes are compiled without FMA contraction so that they
 # follow the reference's separately rounded arithmetic (see csrc/crmath.cuh
 # and csrc/advection_f64.cu).
 UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"]), ("advection_f64.cu", ["-fmad=false"]),
-         ("thermo_fast.cu", [])]
+         ("thermo_fast.cu", []), ("surface.cu", ["-fmad=false"])]
 
 
 def _run(cmd):

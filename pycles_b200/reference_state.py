@@ -63,9 +63,13 @@ class ReferenceState:
         self.to_device(device)
 
     def set_profiles(self, profiles: dict, device="cuda"):
-        """Install precomputed profiles (e.g. from a restart dict)."""
+        """Install precomputed profiles (e.g. from a restart dict), and the
+        Galilean shift u0, v0 when the dict carries it."""
         for k in ("p0", "p0_half", "alpha0", "alpha0_half", "rho0", "rho0_half"):
             setattr(self, k, np.ascontiguousarray(profiles[k], dtype=np.float64))
+        for k in ("u0", "v0"):
+            if k in profiles:
+                setattr(self, k, float(profiles[k]))
         self.to_device(device)
 
     def to_device(self, device="cuda"):
@@ -73,5 +77,8 @@ class ReferenceState:
             setattr(self, "d_" + k, torch.as_tensor(getattr(self, k), dtype=torch.float64, device=device).contiguous())
 
     def profiles(self) -> dict:
-        return {k: np.array(getattr(self, k)) for k in ("p0", "p0_half", "alpha0", "alpha0_half", "rho0",
-                                                        "rho0_half")}
+        """The six profiles (arrays of nlg2) and the Galilean shift u0, v0."""
+        out = {k: np.array(getattr(self, k)) for k in ("p0", "p0_half", "alpha0", "alpha0_half", "rho0",
+                                                       "rho0_half")}
+        out["u0"], out["v0"] = float(self.u0), float(self.v0)
+        return out

@@ -18,6 +18,7 @@ from .advection import MomentumAdvection, ScalarAdvection
 from .grid import Grid
 from .pressure import PressureSolver
 from .reference_state import ReferenceState
+from .surface import SurfaceFactory
 from .thermodynamics import ThermodynamicsDry, ThermodynamicsSA
 from .time_stepping import TimeStepping
 from .variables import DiagnosticVariables, PrognosticVariables
@@ -62,6 +63,7 @@ class HotPathSimulation:
         self.Pr = PressureSolver(namelist)
         self.TS = TimeStepping()
         self.RS = ReferenceState(Gr)
+        self.Sur = SurfaceFactory(namelist)
         PV = self.PV
         PV.add_variable("u", "m/s", "u", "u velocity component", "sym", "velocity")
         PV.set_velocity_direction("u", 0)
@@ -73,6 +75,7 @@ class HotPathSimulation:
         self.Pr.initialize(namelist, Gr, self.RS, self.DV)
         PV.initialize(Gr, device=self.device)
         self.DV.initialize(Gr, device=self.device)
+        self.Sur.initialize(Gr, self.RS)
         self.SA.initialize(Gr, PV)
         self.MA.initialize(Gr, PV)
         self.TS.initialize(namelist, PV)
@@ -101,7 +104,8 @@ class HotPathSimulation:
         """One RK stage in the order of Simulation3d.pyx:159-178.  mark(i),
         if given, is called at the component boundaries (i = 0 before the
         thermodynamics, 1 after it, 2 after the scalar advection, 3 after the
-        momentum advection -- with the u, v, w stage when fused --, 4 after
+        momentum advection -- with the u, v, w stage when fused, with the
+        surface fluxes when a surface scheme is set --, 4 after
         the remaining RK3 stage and the ghost fill, 5 after the pressure
         solve and its ghost fill)."""
         Gr, PV, DV, RS = self.Gr, self.PV, self.DV, self.RS
@@ -127,8 +131,10 @@ class HotPathSimulation:
     def _fused(self) -> bool:
         """The precision form steps with the SSP-RK3 stage fused into the
         momentum pass (velocities u, v, w first, as this driver adds them)
-        unless fuse_rk is off."""
-        return self.fuse_rk and self.MA.precision == _capi.PB_FP32
+        unless fuse_rk is off or a surface scheme adds tendencies between the
+        advection and the stage."""
+        return (self.fuse_rk and self.MA.precision == _capi.PB_FP32
+                and self.Sur.scheme == _capi.PB_SURFACE_NONE)
 
     def _clear_w_tendency(self, stream=None):
         """Fused stepping: the w tendency is cleared once the fused pass has
@@ -180,6 +186,8 @@ class HotPathSimulation:
         TS.rk_step = rk_step
         if not self._fused():
             self.MA.update(Gr, RS, PV, stream=stream)
+            # Sur.update comes next in Simulation3d.pyx:167
+            self.Sur.update(Gr, RS, PV, self.DV, stream=stream)
             m(3)
             TS.update(Gr, PV, stream=stream)
             return

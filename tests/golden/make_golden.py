@@ -1,13 +1,15 @@
 """Generate the golden fixtures of the hot path from the reference's own C.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]
 
 Needs oracle/_ref (the reference's C kernels and its Cython TDMA compiled
 from the reference tree by oracle/build_ref.py).  For each case it stores
 the seeded input state and reference-state profiles, and the outputs of the
 reference kernels driven by the restated glue (oracle.glue, backend "ref"):
 thermodynamics, scalar advection, momentum advection, pressure, one full
-time step, and Simulation3d.run's prologue + one step.
+time step, and Simulation3d.run's prologue + one step.  The surface
+fixtures hold, per surface scheme, the scheme's update after the
+thermodynamics and one time step with the scheme in the stage.
 """
 from __future__ import annotations
 
@@ -93,11 +95,63 @@ def make(name, cfg):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=meta, **out)
 
 
-def main():
+# surface schemes (Surface.pyx) on the case each belongs to
+SURFACE_CASES = {
+    "surface_sullivan_patton": ("SullivanPatton", dict(case="dry_cbl", nx=8, ny=8, nz=12, dx=50.0, dy=50.0,
+                                                       dz=50.0, gw=3, dt=0.5)),
+    "surface_bomex": ("Bomex", dict(case="bomex", nx=12, ny=10, nz=16, dx=100.0, dy=100.0, dz=40.0, gw=3,
+                                    dt=1.0)),
+    "surface_dycoms_rf01": ("DYCOMS_RF01", dict(case="dycoms", nx=8, ny=10, nz=16, dx=35.0, dy=35.0, dz=60.0,
+                                                gw=4, dt=0.25, scalar_order=7, momentum_order=5)),
+}
+
+
+def make_surface(name, scheme, cfg):
+    """The surface scheme's update after the thermodynamics (fluxes and the
+    tendencies of the first interior level), and one time step with the
+    scheme in the stage, from the reference's C driven by the restated glue."""
+    from helpers import host_case, oracle_dims, oracle_sim
+    from oracle import ref
+    from oracle.surface import OracleSurface
+    assert ref.available(), "oracle/_ref missing: run oracle/build_ref.py"
+    nl, rs, f0 = host_case(**cfg)
+    f = stir(f0)
+    d = oracle_dims(nl)
+    out = {"rs_" + k: np.asarray(v) for k, v in rs.items()}
+    for k, v in f.items():
+        out["in_" + k] = v
+    for k, v in f0.items():
+        out["in0_" + k] = v
+    s = oracle_sim(nl, rs, f, backend="ref")
+    s.update_all_bcs()
+    s.th_update()
+    s.tendencies[:] = 0.0
+    s.surface = OracleSurface(scheme, d, u0=rs["u0"], v0=rs["v0"])
+    s.surface.update(s)
+    for n in OracleSurface.NAMES:
+        out["sur_" + n] = getattr(s.surface, n).copy()
+    for k in s.names:
+        out["surtend_" + k] = s.tend(k).copy()
+    s = oracle_sim(nl, rs, f0, backend="ref")
+    s.surface = OracleSurface(scheme, d, u0=rs["u0"], v0=rs["v0"])
+    s.update_all_bcs()
+    s.step()
+    for k in s.names:
+        out["step_" + k] = s.var(k).copy()
+    meta = np.array([repr(cfg), scheme])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=meta, **out)
+
+
+def main(names=None):
     for name, cfg in CASES.items():
-        make(name, cfg)
-        print("wrote", name)
+        if not names or name in names:
+            make(name, cfg)
+            print("wrote", name)
+    for name, (scheme, cfg) in SURFACE_CASES.items():
+        if not names or name in names:
+            make_surface(name, scheme, cfg)
+            print("wrote", name)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

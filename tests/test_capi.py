@@ -43,6 +43,9 @@ def test_every_declared_symbol_is_exported():
 def test_dims_struct_matches_reference_layout():
     # DimStruct (Csrc/grid.h): 1 + 4*3 + 4 + 4*3 longs, then 6 doubles
     assert ctypes.sizeof(_capi.PbDims) == (1 + 12 + 4 + 12) * 8 + 6 * 8
+    # pb_surface: int (padded to 8) + 9 doubles; pb_surface_fields: 11 pointers
+    assert ctypes.sizeof(_capi.PbSurface) == 8 + 9 * 8
+    assert ctypes.sizeof(_capi.PbSurfaceFields) == 11 * 8
 
 
 def test_workspace_size_and_dims_validation():
@@ -70,6 +73,18 @@ def test_invalid_arguments_rejected_without_device():
     assert L.pb_rk3_update(p, p, p, 10, 1.0, 3, None) == _capi.PB_ERR_ARG
     assert L.pb_pressure_solve(d, p, p, p, p, p, p, p, p, p, None, 0, 0, 0, None) == _capi.PB_ERR_WORKSPACE
     assert L.pb_status_string(3) == b"unsupported configuration"
+    sc = _capi.PbSurface(_capi.PB_SURFACE_NONE)
+    assert L.pb_surface_update(d, ctypes.byref(sc), *([None] * 14), None, None) == _capi.PB_OK
+    sc.scheme = 9
+    assert L.pb_surface_update(d, ctypes.byref(sc), *([p] * 14), None, None) == _capi.PB_ERR_ARG
+    fields = _capi.PbSurfaceFields(*([16] * len(_capi.SURFACE_FIELDS)))
+    sc.scheme = _capi.PB_SURFACE_BOMEX  # moist: needs qt, qv, ql and the qt tendency
+    args = [p] * 14
+    args[7] = None  # qt
+    assert L.pb_surface_update(d, ctypes.byref(sc), *args, ctypes.byref(fields), None) == _capi.PB_ERR_ARG
+    fields.scratch = None
+    sc.scheme = _capi.PB_SURFACE_SULLIVAN_PATTON
+    assert L.pb_surface_update(d, ctypes.byref(sc), *([p] * 14), ctypes.byref(fields), None) == _capi.PB_ERR_ARG
 
 
 def test_no_cpu_fallback():

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import GOLDEN, host_case, oracle_sim, rel_l2
+from helpers import GOLDEN, host_case, oracle_dims, oracle_sim, rel_l2
 
 from oracle import port, ref
 
@@ -180,3 +180,87 @@ def test_golden_fixtures_port(name):
     s.step()
     for k in s.names:
         assert np.array_equal(s.var(k), z["run1_" + k]), k
+
+
+# ---- surface fluxes (Surface.pyx, Csrc/surface.h) --------------------------
+SURFACE_FIXTURES = ["surface_sullivan_patton", "surface_bomex", "surface_dycoms_rf01"]
+
+
+@needs_ref
+def test_surface_layer_functions_port_vs_reference():
+    """compute_ustar (the reference runs its secant loop; the restatement
+    returns the first iterate the reference returns), compute_windspeed and
+    entropyflux_from_thetaflux_qtflux, bit for bit against the reference C."""
+    rng = np.random.default_rng(11)
+    n_stable = 0
+    for t in range(2000):
+        ws = 10 ** rng.uniform(-3, 1.3)
+        bf = 0.0 if t % 40 == 0 else rng.choice([-1.0, 1.0]) * 10 ** rng.uniform(-6, -1)
+        z0, zb = 10 ** rng.uniform(-4, -0.5), rng.uniform(1.0, 30.0)
+        n_stable += bf < 0
+        assert port.compute_ustar(ws, bf, z0, zb) == ref.compute_ustar(ws, bf, z0, zb), (ws, bf, z0, zb)
+    assert 500 < n_stable < 1500  # both stability branches exercised
+    nl, rs, f = _stirred(SMALL)
+    d = oracle_dims(nl)
+    a, b = np.zeros(d.nlg[0] * d.nlg[1]), np.zeros(d.nlg[0] * d.nlg[1])
+    port.compute_windspeed(d, f["u"], f["v"], a, 0.7, -0.3, 0.001)
+    ref.compute_windspeed(d, f["u"], f["v"], b, 0.7, -0.3, 0.001)
+    assert np.array_equal(a, b)
+    T = rng.uniform(280.0, 305.0, 64)
+    qt = rng.uniform(1e-3, 2e-2, 64)
+    qv = qt * rng.uniform(0.9, 1.0, 64)
+    assert np.array_equal(port.entropyflux_from_thetaflux_qtflux(8e-3, 5.2e-5, 1.0e5, T, qt, qv),
+                          ref.entropyflux_from_thetaflux_qtflux(8e-3, 5.2e-5, 1.0e5, T, qt, qv))
+
+
+def _surface_fixture(name):
+    from pycles_b200.simulation import namelist_for
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    cfg = eval(str(z["meta"][0]))  # dict literal written by make_golden.py
+    scheme = str(z["meta"][1])
+    nl = namelist_for(**cfg)
+    rs = {k[3:]: z[k] for k in z.files if k.startswith("rs_")}
+    f = {k[3:]: z[k] for k in z.files if k.startswith("in_")}
+    f0 = {k[4:]: z[k] for k in z.files if k.startswith("in0_")}
+    return z, scheme, nl, rs, f, f0
+
+
+@pytest.mark.parametrize("name", SURFACE_FIXTURES)
+def test_surface_golden_port(name):
+    """The restated surface glue on the numpy restatement reproduces the
+    reference-generated surface fixtures: the fluxes and tendencies bit for
+    bit, one time step with the scheme to 1e-13."""
+    from oracle.surface import OracleSurface
+    z, scheme, nl, rs, f, f0 = _surface_fixture(name)
+    d = oracle_dims(nl)
+    s = oracle_sim(nl, rs, f, "port")
+    s.update_all_bcs()
+    s.th_update()
+    s.tendencies[:] = 0.0
+    s.surface = OracleSurface(scheme, d, u0=float(rs["u0"]), v0=float(rs["v0"]))
+    s.surface.update(s)
+    for n in OracleSurface.NAMES:
+        assert np.array_equal(getattr(s.surface, n), z["sur_" + n]), n
+    for k in s.names:
+        assert np.array_equal(s.tend(k), z["surtend_" + k]), k
+    s = oracle_sim(nl, rs, f0, "port")
+    s.surface = OracleSurface(scheme, d, u0=float(rs["u0"]), v0=float(rs["v0"]))
+    s.update_all_bcs()
+    s.step()
+    for k in s.names:
+        assert rel_l2(s.var(k), z["step_" + k]) < 1e-13, k
+
+
+def test_surface_changes_the_step():
+    """The surface fluxes reach the state: a step with the scheme differs
+    from one without it at the first interior level (a planted omission of
+    the surface update would pass the other checks of an unchanged field)."""
+    z, scheme, nl, rs, f, f0 = _surface_fixture("surface_bomex")
+    s = oracle_sim(nl, rs, f0, "port")
+    s.update_all_bcs()
+    s.step()
+    d = oracle_dims(nl)
+    for k in ("u", "s", "qt"):
+        a = s.var(k).reshape(d.shape)[d.gw:-d.gw, d.gw:-d.gw, d.gw]
+        b = z["step_" + k].reshape(d.shape)[d.gw:-d.gw, d.gw:-d.gw, d.gw]
+        assert rel_l2(a, b) > 1e-9, k
