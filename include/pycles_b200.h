@@ -452,6 +452,81 @@ int pb_surface_update(const pb_dims* dims, const pb_surface* surface, const doub
                       const pb_surface_fields* fields, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Subgrid scale and diffusion
+ * --------------------------------------------------------------------- */
+
+/* SGS schemes (SGS.pyx:35-44) and the Smagorinsky length scale (:101-145). */
+enum pb_sgs_scheme {
+  PB_SGS_UNIFORM = 1,       /* UniformViscosity (SGS.pyx:57-97)              */
+  PB_SGS_SMAGORINSKY = 2    /* Smagorinsky (SGS.pyx:101-149)                 */
+};
+enum pb_sgs_length {
+  PB_SGS_LENGTH_GRID = 0,   /* smagorinsky_update (Csrc/sgs.h:4-18)          */
+  PB_SGS_LENGTH_WALL = 1,   /* smagorinsky_update_wall (Csrc/sgs.h:21-54)    */
+  PB_SGS_LENGTH_ILES = 2    /* smagorinsky_update_iles (Csrc/sgs.h:56-89)    */
+};
+/* cs, prt: Smagorinsky constant and turbulent Prandtl number (defaults
+ * 0.17, 1/3); viscosity, diffusivity: UniformViscosity's constants. */
+typedef struct pb_sgs {
+  int scheme;
+  int length;
+  double cs, prt;
+  double viscosity, diffusivity;
+} pb_sgs;
+
+/*
+ * Kinematics.update (Kinematics.pyx:42-58) followed by SGS.update
+ * (SGS.pyx:48-53): the strain-rate magnitude of compute_strain_rate_mag
+ * (Csrc/kinematics.h:72-131, from the velocity gradients :6-34 and strain
+ * rates :37-69, formed in registers, not stored), then the eddy viscosity
+ * and diffusivity over all cells.  The velocity gradients and the nine
+ * strain-rate components the reference stores are not materialised.
+ * sgs == NULL: Kinematics.update alone (the strain-rate magnitude; the
+ * viscosity, diffusivity, buoyancy_frequency and zl_half are not used).
+ *   buoyancy_frequency: DiagnosticVariables 'buoyancy_frequency' (Smagorinsky)
+ *   zl_half           : Grid.zl_half, nlg2 doubles (wall / ILES length scale)
+ * Where the reference's strain-magnitude stencil leaves the computed strain
+ * field (the (x,x) pair on the plane i = 1 reads before the array, the (y,y)
+ * pair on j = 1 wraps into the previous row), the term is 0; no interior
+ * tendency reads those planes' viscosity when gw >= 3.
+ */
+int pb_kinematics_sgs(const pb_dims* dims, const pb_sgs* sgs, const double* u, const double* v,
+                      const double* w, const double* buoyancy_frequency, const double* zl_half,
+                      double* strain_rate_mag, double* viscosity, double* diffusivity, void* stream);
+
+/*
+ * ScalarDiffusion.update (ScalarDiffusion.pyx:112-150): for every scalar and
+ * direction the second-order diffusive flux (Csrc/scalar_diffusion.h:6-57,
+ * formed in registers) and its divergence (scalar_flux_divergence,
+ * Csrc/flux_divergence.h:4-32) subtracted from the scalar's tendency over
+ * the interior; factors (HOST, nscalars doubles, NULL = all 1) as the
+ * reference's flux_factor.  qt_index >= 0 adds the qt-diffusion entropy
+ * source (compute_qt_diffusion_s_source, Csrc/scalar_diffusion.h:70-113;
+ * namelist diffusion.qt_entropy_source) to the tendency of scalar s_index,
+ * with p0_half, qv (DV) and T (DV).  scalars / tendencies: HOST arrays of
+ * device pointers.  Needs gw >= 2.
+ */
+int pb_scalar_diffusion(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                        const double* alpha0_half, const double* diffusivity, int nscalars,
+                        const double* const* scalars, double* const* tendencies, const double* factors,
+                        int qt_index, int s_index, const double* p0_half, const double* qv, const double* T,
+                        void* stream);
+
+/*
+ * MomentumDiffusion.update (MomentumDiffusion.pyx:52-78): the nine stress
+ * fluxes (compute_diffusive_flux_m, Csrc/momentum_diffusion.h:5-96, formed
+ * in registers from the velocities and the viscosity) and their divergence
+ * (momentum_flux_divergence, Csrc/flux_divergence.h:34-60) into the u, v, w
+ * tendencies, then the entropy source S^2 nu / T into s_tend
+ * (compute_entropy_source, :98-118).  strain_rate_mag as pb_kinematics_sgs
+ * leaves it.  Needs gw >= 2.
+ */
+int pb_momentum_diffusion(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                          const double* alpha0, const double* alpha0_half, const double* u, const double* v,
+                          const double* w, const double* viscosity, const double* strain_rate_mag,
+                          const double* T, double* ut, double* vt, double* wt, double* s_tend, void* stream);
+
+/* ------------------------------------------------------------------------
  * Errors
  * --------------------------------------------------------------------- */
 

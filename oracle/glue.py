@@ -3,8 +3,9 @@ TEST INFRASTRUCTURE ONLY.
 
 ``OracleSim`` reproduces one rank of ``Simulation3d.run`` (Simulation3d.pyx:
 140-189) restricted to the hot-path components, in the reference's order per
-RK stage: Th.update, SA.update, MA.update, [Sur.update,] TS.update,
-PV.Update_all_bcs, Pr.update.  The kernels come from one of two backends:
+RK stage: [Ke.update,] Th.update, SA.update, MA.update, [Sur.update,]
+[SGS.update, SD.update, MD.update,] TS.update, PV.Update_all_bcs,
+Pr.update.  The kernels come from one of two backends:
 
 * ``"ref"``  -- the reference's own C (oracle/ref.py), TDMA from the
                reference's cythonized SparseSolvers when it was built;
@@ -158,6 +159,7 @@ class OracleSim:
         self.flux = np.zeros(self.nscalars * 3 * npg)
         self.secant_iters = None
         self.surface = None  # an oracle.surface.OracleSurface, updated after MA as Simulation3d.pyx:167
+        self.sgs = None  # an oracle.sgs.OracleSGS: Ke at the stage start, SGS/SD/MD after Sur (:159-172)
         if moist:
             x, y = table_xy if table_xy is not None else cc_table()
             self.table_xy = (x, y)
@@ -313,11 +315,17 @@ class OracleSim:
     # driver ------------------------------------------------------------------
     def stage(self, rk_step):
         """One RK stage of Simulation3d.run (:158-180) over the hot path."""
+        if self.sgs is not None:
+            self.sgs.ke_update(self)
         self.th_update()
         self.sa_update()
         self.ma_update()
         if self.surface is not None:
             self.surface.update(self)
+        if self.sgs is not None:
+            self.sgs.sgs_update(self)
+            self.sgs.sd_update(self)
+            self.sgs.md_update(self)
         self.ts_update(rk_step)
         self.update_all_bcs()
         self.pr_update()

@@ -763,3 +763,182 @@ def entropyflux_from_thetaflux_qtflux(thetaflux, qtflux, p0_b, T_b, qt_b, qv_b):
     sv_b = sv_c(pv_b, T_b)
     cp_b = cpm_c(qt_b)
     return cp_b * thetaflux * exner_b / T_b + qtflux * (sv_b - sd_b)
+
+
+# ---------------------------------------------------------------------------
+# kinematics, Csrc/kinematics.h
+# ---------------------------------------------------------------------------
+def compute_velocity_gradient(d: Dims, v, vgrad, direction):
+    """Csrc/kinematics.h:6-34: vgrad = (v[ijk + s_d] - v[ijk]) dxi_d over
+    [0, nlg-1) in every dimension."""
+    sh = d.shape
+    V = v.reshape(sh)
+    G = vgrad.reshape(sh)
+    reg = _region(sh, 0, 1)
+    G[reg] = (_sh(V, reg, direction, 1) - V[reg]) * d.dxi[direction]
+
+
+def compute_strain_rate(d: Dims, vgrad, strain_rate):
+    """Csrc/kinematics.h:37-69: S[3 vi1 + d] = (vgrad[vi1][d] + vgrad[d][vi1]) / 2."""
+    sh = d.shape
+    npg = d.npg
+    reg = _region(sh, 0, 1)
+    for vi1 in range(3):
+        for dd in range(3):
+            a = vgrad[(3 * vi1 + dd) * npg:(3 * vi1 + dd + 1) * npg].reshape(sh)
+            b = vgrad[(3 * dd + vi1) * npg:(3 * dd + vi1 + 1) * npg].reshape(sh)
+            S = strain_rate[(3 * vi1 + dd) * npg:(3 * vi1 + dd + 1) * npg].reshape(sh)
+            S[reg] = 0.5 * (a[reg] + b[reg])
+
+
+def compute_strain_rate_mag(d: Dims, strain_rate, strain_rate_mag):
+    """Csrc/kinematics.h:72-131: zero everywhere; over [1, nlg-1) add the
+    diagonal components S_dd at ijk - s_d, then for the pairs (vi1, d) with
+    vi1 in {0, 1} and d >= vi1 -- (0,0), (0,1), (0,2), (1,1), (1,2), as the
+    reference loops run -- twice the square of S averaged over ijk, ijk -
+    s_vi1, ijk - s_d, ijk - s_d - s_vi1; finally sqrt(2 sum) over all
+    cells."""
+    sh = d.shape
+    npg = d.npg
+    M = strain_rate_mag.reshape(sh)
+    M[...] = 0.0
+    reg = _region(sh, 1, 1)
+
+    def comp(c):
+        return strain_rate[c * npg:(c + 1) * npg].reshape(sh)
+
+    for dd in range(3):
+        S = comp(4 * dd)
+        t = _sh(S, reg, dd, -1)
+        M[reg] += t * t
+    strides = (d.nlg[1] * d.nlg[2], d.nlg[2], 1)
+    ii, jj, kk = np.meshgrid(*[np.arange(r.start, r.stop) for r in reg], indexing="ij")
+    flat = ii * strides[0] + jj * strides[1] + kk
+    for vi1 in range(2):
+        for dd in range(vi1, 3):
+            c = 3 * vi1 + dd
+            S = comp(c)
+            p2 = _sh(S, reg, vi1, -1)
+            p3 = _sh(S, reg, dd, -1)
+            # the fourth point by its flat offset, as the reference indexes it:
+            # for vi1 = d it is two cells back along vi1, which from j = 1
+            # wraps to the previous x row (a cell the strain rate is never
+            # computed on: 0) and from i = 1 falls before the array (read
+            # as 0 here; no interior tendency depends on it when gw >= 3)
+            q = flat - strides[vi1] - strides[dd]
+            Sf = strain_rate[c * npg:(c + 1) * npg]
+            p4 = np.where(q >= 0, Sf[np.clip(q, 0, None)], 0.0)
+            s_interp = 0.25 * (S[reg] + p2 + p3 + p4)
+            M[reg] += 2.0 * s_interp * s_interp
+    M[...] = np.sqrt(2.0 * M)
+
+
+# ---------------------------------------------------------------------------
+# Smagorinsky, Csrc/sgs.h
+# ---------------------------------------------------------------------------
+def smagorinsky_update(d: Dims, visc, diff, buoy_freq, strain_rate_mag, cs, prt, variant="plain", zl_half=None):
+    """Csrc/sgs.h:4-18 (plain), :21-54 (wall), :56-89 (iles), over all npg
+    cells; delta = cbrt(dx dy dz)."""
+    sh = d.shape
+    delta = _cbrt(d.dx[0] * d.dx[1] * d.dx[2])
+    S = strain_rate_mag.reshape(sh)
+    N2 = buoy_freq.reshape(sh)
+    if variant == "plain":
+        nu = cs * cs * delta * delta * S
+    else:
+        z = np.asarray(zl_half, dtype=np.float64)[None, None, :]
+        if variant == "wall":
+            ell = delta * vkb * z / (delta + vkb * z)
+        else:
+            ell = np.fmax(0.0, delta - vkb * z)
+        nu = cs * cs * ell * ell * S
+    pos = N2 > 0.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fb = np.sqrt(np.fmax(1.0 - N2 / (prt * S * S), 0.0))
+        nu = np.where(pos, nu * fb, nu)
+    visc.reshape(sh)[...] = nu
+    diff.reshape(sh)[...] = nu / prt
+
+
+def _cbrt(x):
+    """C's cbrt (the reference's delta); Python's math.cbrt is the C library's."""
+    return math.cbrt(x)
+
+
+# ---------------------------------------------------------------------------
+# scalar diffusion, Csrc/scalar_diffusion.h
+# ---------------------------------------------------------------------------
+def compute_diffusive_flux(d: Dims, rho0, rho0_half, diffusivity, scalar, flux, dx, direction, factor):
+    """Csrc/scalar_diffusion.h:6-57 (second_order_diffusion): over [gw-1,
+    nlg-gw) in every dimension F = -factor interp_2(D, D[+s]) (phi[+s] -
+    phi) rho dxi, rho = rho0[k] for d = 2 else rho0_half[k]; then F = 0 on
+    the level k = gw-1."""
+    sh = d.shape
+    D = diffusivity.reshape(sh)
+    P = scalar.reshape(sh)
+    F = flux.reshape(sh)
+    reg = tuple(slice(d.gw - 1, n - d.gw) for n in sh)
+    rho = _kvec(rho0 if direction == 2 else rho0_half, reg)
+    dxi = 1.0 / dx
+    F[reg] = (-factor * interp_2(D[reg], _sh(D, reg, direction, 1)) * (_sh(P, reg, direction, 1) - P[reg])
+              * rho * dxi)
+    F[reg[0], reg[1], d.gw - 1] = 0.0
+
+
+def compute_qt_diffusion_s_source(d: Dims, p0_half, alpha0, alpha0_half, flux, qt, qv, T, tendency, dx, direction):
+    """Csrc/scalar_diffusion.h:70-113: the entropy tendency of the qt
+    diffusion, -(sw - sd) alpha0_half (F[+s] - F) dxi over the interior."""
+    sh = d.shape
+    reg = _region(sh, d.gw, d.gw)
+    F = flux.reshape(sh)
+    Q = qt.reshape(sh)[reg]
+    V = qv.reshape(sh)[reg]
+    Tm = T.reshape(sh)[reg]
+    p0 = _kvec(p0_half, reg)
+    pd = pd_c(p0, Q, V)
+    sd = sd_c(pd, Tm)
+    pv = pv_c(p0, Q, V)
+    sv = sv_c(pv, Tm)
+    L = latent_heat_variable(Tm)
+    sw = sv - (((Q - V) / Q) * L / Tm)
+    dxi = 1.0 / dx
+    tendency.reshape(sh)[reg] -= (sw - sd) * _kvec(alpha0_half, reg) * (_sh(F, reg, direction, 1) - F[reg]) * dxi
+
+
+# ---------------------------------------------------------------------------
+# momentum diffusion, Csrc/momentum_diffusion.h
+# ---------------------------------------------------------------------------
+def compute_diffusive_flux_m(d: Dims, strain_rate, viscosity, flux, rho0, rho0_half, i1, i2):
+    """Csrc/momentum_diffusion.h:5-96: F = -2 S_{i1 i2} nu rho over [gw-1,
+    nlg-gw); nu at ijk + s_i1 for the diagonal components, else averaged
+    over the four cells around the edge; rho = rho0_half[k] (i1, i2 != 2),
+    rho0_half[k+1] (i1 = i2 = 2), rho0[k] (one of them 2); F = 0 on the
+    level k = gw-1."""
+    sh = d.shape
+    S = strain_rate.reshape(sh)
+    N = viscosity.reshape(sh)
+    F = flux.reshape(sh)
+    reg = tuple(slice(d.gw - 1, n - d.gw) for n in sh)
+    if i1 == i2:
+        nu = _sh(N, reg, i1, 1)
+    else:
+        s4 = list(reg)
+        s4[i1] = slice(reg[i1].start + 1, reg[i1].stop + 1)
+        s4[i2] = slice(reg[i2].start + 1, reg[i2].stop + 1)
+        nu = 0.25 * (N[reg] + _sh(N, reg, i1, 1) + _sh(N, reg, i2, 1) + N[tuple(s4)])
+    if i1 != 2 and i2 != 2:
+        rho = _kvec(rho0_half, reg)
+    elif i1 == 2 and i2 == 2:
+        rho = _kvec(rho0_half, reg, 1)
+    else:
+        rho = _kvec(rho0, reg)
+    F[reg] = -2.0 * S[reg] * nu * rho
+    F[reg[0], reg[1], d.gw - 1] = 0.0
+
+
+def compute_entropy_source(d: Dims, viscosity, strain_rate_mag, temperature, entropy_tendency):
+    """Csrc/momentum_diffusion.h:98-118: s tendency += S^2 nu / T over the interior."""
+    sh = d.shape
+    reg = _region(sh, d.gw, d.gw)
+    S = strain_rate_mag.reshape(sh)[reg]
+    entropy_tendency.reshape(sh)[reg] += S * S * viscosity.reshape(sh)[reg] / temperature.reshape(sh)[reg]

@@ -213,3 +213,71 @@ def entropyflux_from_thetaflux_qtflux(thetaflux, qtflux, p0_b, T_b, qt_b, qv_b):
     for idx in np.ndindex(out.shape):
         out[idx] = f(*[float(x[idx]) for x in b])
     return out
+
+
+# ---- subgrid scale and diffusion (Csrc/kinematics.h, sgs.h, *_diffusion.h) --
+def _fn(name, argtypes, restype=None):
+    f = getattr(lib(), name)
+    f.argtypes = argtypes
+    f.restype = restype
+    return f
+
+
+def compute_velocity_gradient(d: Dims, v, vgrad, direction):
+    dc = d.c()
+    _fn("compute_velocity_gradient", [ctypes.c_void_p, _dp, _dp, ctypes.c_ssize_t])(
+        ctypes.byref(dc), _p(v), _p(vgrad), direction)
+
+
+def compute_strain_rate(d: Dims, vgrad, strain_rate):
+    dc = d.c()
+    _fn("compute_strain_rate", [ctypes.c_void_p, _dp, _dp])(ctypes.byref(dc), _p(vgrad), _p(strain_rate))
+
+
+def compute_strain_rate_mag(d: Dims, strain_rate, strain_rate_mag):
+    dc = d.c()
+    _fn("compute_strain_rate_mag", [ctypes.c_void_p, _dp, _dp])(ctypes.byref(dc), _p(strain_rate),
+                                                               _p(strain_rate_mag))
+
+
+def smagorinsky_update(d: Dims, visc, diff, buoy_freq, strain_rate_mag, cs, prt, variant="plain", zl_half=None):
+    dc = d.c()
+    if variant == "plain":
+        _fn("smagorinsky_update", [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double])(
+            ctypes.byref(dc), _p(visc), _p(diff), _p(buoy_freq), _p(strain_rate_mag), cs, prt)
+    else:
+        name = "smagorinsky_update_wall" if variant == "wall" else "smagorinsky_update_iles"
+        _fn(name, [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double])(
+            ctypes.byref(dc), _p(zl_half), _p(visc), _p(diff), _p(buoy_freq), _p(strain_rate_mag), cs, prt)
+
+
+def compute_diffusive_flux(d: Dims, rho0, rho0_half, diffusivity, scalar, flux, dx, direction, factor):
+    dc = d.c()
+    _fn("compute_diffusive_flux", [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_ssize_t,
+                                   ctypes.c_ssize_t, ctypes.c_double])(
+        ctypes.byref(dc), _p(rho0), _p(rho0_half), _p(diffusivity), _p(scalar), _p(flux), dx, direction, 2, factor)
+
+
+def compute_qt_diffusion_s_source(d: Dims, p0_half, alpha0, alpha0_half, flux, qt, qv, T, tendency, dx, direction):
+    dc = d.c()
+    _fn("ref_compute_qt_diffusion_s_source", [ctypes.c_void_p] + [_dp] * 8 + [ctypes.c_double, ctypes.c_ssize_t])(
+        ctypes.byref(dc), _p(p0_half), _p(alpha0), _p(alpha0_half), _p(flux), _p(qt), _p(qv), _p(T), _p(tendency),
+        dx, direction)
+
+
+def compute_diffusive_flux_m(d: Dims, strain_rate, viscosity, flux, rho0, rho0_half, i1, i2):
+    dc = d.c()
+    _fn("compute_diffusive_flux_m", [ctypes.c_void_p] + [_dp] * 5 + [ctypes.c_ssize_t, ctypes.c_ssize_t])(
+        ctypes.byref(dc), _p(strain_rate), _p(viscosity), _p(flux), _p(rho0), _p(rho0_half), i1, i2)
+
+
+def momentum_flux_divergence(d: Dims, alpha0, alpha0_half, flux, tendency, d_advected, d_advecting):
+    dc = d.c()
+    _fn("momentum_flux_divergence", [ctypes.c_void_p] + [_dp] * 4 + [ctypes.c_ssize_t, ctypes.c_ssize_t])(
+        ctypes.byref(dc), _p(alpha0), _p(alpha0_half), _p(flux), _p(tendency), d_advected, d_advecting)
+
+
+def compute_entropy_source(d: Dims, viscosity, strain_rate_mag, temperature, entropy_tendency):
+    dc = d.c()
+    _fn("compute_entropy_source", [ctypes.c_void_p] + [_dp] * 4)(
+        ctypes.byref(dc), _p(viscosity), _p(strain_rate_mag), _p(temperature), _p(entropy_tendency))

@@ -16,7 +16,9 @@
  *    bvf_sa and thetali_update with plain pointers;
  *  - a LookupStruct constructor (init_table, Csrc/lookup.h:16-40) callable
  *    from ctypes;
- *  - wrappers of the surface-layer functions of Csrc/surface.h.
+ *  - wrappers of the surface-layer functions of Csrc/surface.h and of the
+ *    qt-diffusion entropy source (Csrc/scalar_diffusion.h), which takes the
+ *    latent-heat function pointers.
  * The dry-thermodynamics header defines eos_c/eos_update under the same
  * names as the saturation-adjustment header, so it is included with those
  * two names remapped.
@@ -36,6 +38,10 @@
 #include "thermodynamics_sa.h"
 #include "prognostic_variables.h"
 #include "surface.h"
+#include "kinematics.h"
+#include "sgs.h"
+#include "scalar_diffusion.h"
+#include "momentum_diffusion.h"
 
 #define eos_c dry_eos_c
 #define eos_update dry_eos_update
@@ -106,4 +112,12 @@ void ref_compute_windspeed(struct DimStruct* dims, double* u, double* v, double*
 }
 double ref_entropyflux(double thetaflux, double qtflux, double p0_b, double T_b, double qt_b, double qv_b) {
     return entropyflux_from_thetaflux_qtflux(thetaflux, qtflux, p0_b, T_b, qt_b, qv_b);
+}
+
+/* ---- subgrid scale and diffusion (Csrc/kinematics.h, sgs.h, *_diffusion.h) */
+void ref_compute_qt_diffusion_s_source(struct DimStruct* dims, double* p0_half, double* alpha0, double* alpha0_half,
+                                       double* flux, double* qt, double* qv, double* T, double* tendency,
+                                       double dx, ssize_t d) {
+    compute_qt_diffusion_s_source(dims, p0_half, alpha0, alpha0_half, flux, qt, qv, T, tendency,
+                                  shim_lambda_constant, shim_latent_heat_variable, dx, d);
 }

@@ -59,6 +59,13 @@ PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_UNSUPPORTED, PB_ERR_WORKSPACE = 0, 1, 2, 
 PB_FP64, PB_FP32 = 0, 1
 PB_SURFACE_NONE, PB_SURFACE_SULLIVAN_PATTON, PB_SURFACE_BOMEX, PB_SURFACE_DYCOMS_RF01 = 0, 1, 2, 3
 PB_SURFACE_SCRATCH = 512
+PB_SGS_UNIFORM, PB_SGS_SMAGORINSKY = 1, 2
+PB_SGS_LENGTH_GRID, PB_SGS_LENGTH_WALL, PB_SGS_LENGTH_ILES = 0, 1, 2
+
+
+class PbSgs(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("length", ctypes.c_int), ("cs", ctypes.c_double),
+                ("prt", ctypes.c_double), ("viscosity", ctypes.c_double), ("diffusivity", ctypes.c_double)]
 
 
 def precision_of(namelist) -> int:
@@ -95,6 +102,9 @@ SIGNATURES = {
     "pb_pressure_solve_noalloc": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "pb_surface_update": (_I, [_DIMS, ctypes.POINTER(PbSurface), _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                _P, _P, ctypes.POINTER(PbSurfaceFields), _P]),
+    "pb_kinematics_sgs": (_I, [_DIMS, ctypes.POINTER(PbSgs), _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pb_scalar_diffusion": (_I, [_DIMS, _P, _P, _P, _P, _I, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
+    "pb_momentum_diffusion": (_I, [_DIMS] + [_P] * 15),
     "pb_get_error": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "pb_clear_error": (_I, [_P]),
     "pb_status_string": (ctypes.c_char_p, [_I]),

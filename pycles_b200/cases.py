@@ -35,7 +35,7 @@ def dry_cbl(Gr, RS, Th, seed=0, amplitude=0.1):
     RS.u0, RS.v0 = 1.0, 0.0
     RS.initialize(Gr, Th, device=getattr(Gr, "device", "cuda"))
     sh = Gr.shape
-    z = Gr.zl_half
+    z = Gr.z_half
     theta = np.where(z <= 800.0, 300.0, 300.0 + (z - 800.0) * 0.006)
     pert = _perturbation(Gr.npg, seed, amplitude).reshape(sh)
     p0 = RS.p0_half
@@ -56,7 +56,7 @@ def bomex(Gr, RS, Th, seed=0, theta_amp=0.1, qt_amp=2.5e-5):
     RS.Pg, RS.Tg, RS.qtg = 1.015e5, 300.4, 0.02245
     RS.initialize(Gr, Th, device=getattr(Gr, "device", "cuda"))
     sh = Gr.shape
-    z = Gr.zl_half
+    z = Gr.z_half
     thetal = np.empty_like(z)
     qt = np.empty_like(z)
     u = np.empty_like(z)
@@ -154,7 +154,7 @@ def dycoms(Gr, RS, Th, seed=0, amplitude=0.1):
     RS.Tg = 289.0 * (RS.Pg / th.p_tilde) ** (287.0 / 1015.0)
     RS.initialize(Gr, Th, device=getattr(Gr, "device", "cuda"))
     sh = Gr.shape
-    z = Gr.zl_half
+    z = Gr.z_half
     thetal = np.where(z <= 840.0, 289.0, 297.5 + np.cbrt(np.maximum(z - 840.0, 0.0)))
     qt = np.where(z <= 840.0, 9.0 / 1000.0, 1.5 / 1000.0)
     p0 = RS.p0_half

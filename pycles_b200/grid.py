@@ -50,8 +50,11 @@ class Grid:
         self.x, self.x_half = out["x"], out["x_half"]
         self.y, self.y_half = out["y"], out["y_half"]
         self.z, self.z_half = out["z"], out["z_half"]
+        # Grid.pyx:162-163: zl_half is extracted from zl, not from z_half, so on
+        # one rank it holds the face heights (z); the wall-adjusted and ILES
+        # Smagorinsky length scales read it
         self.zl = self.z.copy()
-        self.zl_half = self.z_half.copy()
+        self.zl_half = self.zl.copy()
 
     # convenience --------------------------------------------------------
     @property

@@ -18,6 +18,7 @@ from .advection import MomentumAdvection, ScalarAdvection
 from .grid import Grid
 from .pressure import PressureSolver
 from .reference_state import ReferenceState
+from .sgs import SGS, Kinematics, MomentumDiffusion, ScalarDiffusion
 from .surface import SurfaceFactory
 from .thermodynamics import ThermodynamicsDry, ThermodynamicsSA
 from .time_stepping import TimeStepping
@@ -64,6 +65,13 @@ class HotPathSimulation:
         self.TS = TimeStepping()
         self.RS = ReferenceState(Gr)
         self.Sur = SurfaceFactory(namelist)
+        # subgrid scale and diffusion when the namelist has an sgs section
+        # (the measured configurations have none)
+        self.SGS = SGS(namelist) if "sgs" in namelist else None
+        if self.SGS is not None:
+            self.Ke = Kinematics()
+            self.SD = ScalarDiffusion(namelist, None, self.DV)
+            self.MD = MomentumDiffusion(self.DV)
         PV = self.PV
         PV.add_variable("u", "m/s", "u", "u velocity component", "sym", "velocity")
         PV.set_velocity_direction("u", 0)
@@ -76,6 +84,9 @@ class HotPathSimulation:
         PV.initialize(Gr, device=self.device)
         self.DV.initialize(Gr, device=self.device)
         self.Sur.initialize(Gr, self.RS)
+        if self.SGS is not None:
+            self.Ke.initialize(Gr)
+            self.SGS.initialize(Gr, PV)
         self.SA.initialize(Gr, PV)
         self.MA.initialize(Gr, PV)
         self.TS.initialize(namelist, PV)
@@ -134,7 +145,7 @@ class HotPathSimulation:
         unless fuse_rk is off or a surface scheme adds tendencies between the
         advection and the stage."""
         return (self.fuse_rk and self.MA.precision == _capi.PB_FP32
-                and self.Sur.scheme == _capi.PB_SURFACE_NONE)
+                and self.Sur.scheme == _capi.PB_SURFACE_NONE and self.SGS is None)
 
     def _clear_w_tendency(self, stream=None):
         """Fused stepping: the w tendency is cleared once the fused pass has
@@ -186,8 +197,13 @@ class HotPathSimulation:
         TS.rk_step = rk_step
         if not self._fused():
             self.MA.update(Gr, RS, PV, stream=stream)
-            # Sur.update comes next in Simulation3d.pyx:167
+            # then Sur, SGS, SD and MD (Simulation3d.pyx:167-172); Ke.update
+            # (:160) is folded into SGS.update: no velocity changes between
             self.Sur.update(Gr, RS, PV, self.DV, stream=stream)
+            if self.SGS is not None:
+                self.SGS.update(Gr, self.DV, PV, self.Ke, self.Sur, stream=stream)
+                self.SD.update(Gr, RS, PV, self.DV, stream=stream)
+                self.MD.update(Gr, RS, PV, self.DV, self.Ke, stream=stream)
             m(3)
             TS.update(Gr, PV, stream=stream)
             return

@@ -9,7 +9,9 @@ reference kernels driven by the restated glue (oracle.glue, backend "ref"):
 thermodynamics, scalar advection, momentum advection, pressure, one full
 time step, and Simulation3d.run's prologue + one step.  The surface
 fixtures hold, per surface scheme, the scheme's update after the
-thermodynamics and one time step with the scheme in the stage.
+thermodynamics and one time step with the scheme in the stage; the sgs
+fixtures the strain-rate magnitude, viscosity and diffusivity, the scalar
+and momentum diffusion tendencies and one time step with them.
 """
 from __future__ import annotations
 
@@ -142,6 +144,79 @@ def make_surface(name, scheme, cfg):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=meta, **out)
 
 
+# subgrid scale and diffusion (SGS.pyx, Kinematics.pyx, ScalarDiffusion.pyx,
+# MomentumDiffusion.pyx): namelist sections as the reference reads them
+SGS_CASES = {
+    "sgs_smagorinsky_bomex": (dict(case="bomex", nx=12, ny=10, nz=16, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0),
+                              {"sgs": {"scheme": "Smagorinsky"}, "diffusion": {"qt_entropy_source": True}}),
+    "sgs_smagorinsky_iles_bomex": (dict(case="bomex", nx=10, ny=12, nz=14, dx=100.0, dy=100.0, dz=40.0, gw=3,
+                                        dt=1.0),
+                                   {"sgs": {"scheme": "Smagorinsky", "Smagorinsky": {"iles": True, "cs": 0.2}}}),
+    "sgs_smagorinsky_wall_dry": (dict(case="dry_cbl", nx=8, ny=8, nz=12, dx=50.0, dy=50.0, dz=50.0, gw=3, dt=0.5),
+                                 {"sgs": {"scheme": "Smagorinsky", "Smagorinsky": {"wall": True}},
+                                  "meta": {"casename": "SullivanPatton"}}),
+    "sgs_uniform_dycoms": (dict(case="dycoms", nx=8, ny=10, nz=16, dx=35.0, dy=35.0, dz=60.0, gw=4, dt=0.25,
+                                scalar_order=7, momentum_order=5),
+                           {"sgs": {"scheme": "UniformViscosity",
+                                    "UniformViscosity": {"viscosity": 75.0, "diffusivity": 75.0}}}),
+}
+
+
+def make_sgs(name, cfg, extra):
+    """Kinematics + SGS after the thermodynamics, the scalar and momentum
+    diffusion tendencies, and one time step with them (and the case's
+    surface scheme when the namelist names one), from the reference's C
+    driven by the restated glue."""
+    from helpers import host_case, oracle_dims, oracle_sim
+    from oracle import ref
+    from oracle.sgs import OracleSGS, scheme_from_namelist
+    from oracle.surface import OracleSurface
+    from pycles_b200.grid import Grid
+    assert ref.available(), "oracle/_ref missing: run oracle/build_ref.py"
+    nl, rs, f0 = host_case(**cfg)
+    nl = dict(nl, **extra)
+    f = stir(f0)
+    d = oracle_dims(nl)
+    zl_half = Grid(nl).zl_half
+    conf = scheme_from_namelist(nl)
+    casename = extra.get("meta", {}).get("casename")
+
+    def attach(s):
+        s.sgs = OracleSGS(conf, d, zl_half)
+        if casename:
+            s.surface = OracleSurface(casename, d, u0=rs["u0"], v0=rs["v0"])
+        return s
+
+    out = {"rs_" + k: np.asarray(v) for k, v in rs.items()}
+    for k, v in f.items():
+        out["in_" + k] = v
+    for k, v in f0.items():
+        out["in0_" + k] = v
+    s = attach(oracle_sim(nl, rs, f, backend="ref"))
+    s.update_all_bcs()
+    s.sgs.ke_update(s)
+    s.th_update()
+    s.sgs.sgs_update(s)
+    out["sgs_strain_rate_mag"] = s.sgs.strain_rate_mag.copy()
+    out["sgs_viscosity"] = s.sgs.viscosity.copy()
+    out["sgs_diffusivity"] = s.sgs.diffusivity.copy()
+    s.tendencies[:] = 0.0
+    s.sgs.sd_update(s)
+    for k in s.names:
+        out["sdtend_" + k] = s.tend(k).copy()
+    s.tendencies[:] = 0.0
+    s.sgs.md_update(s)
+    for k in s.names:
+        out["mdtend_" + k] = s.tend(k).copy()
+    s = attach(oracle_sim(nl, rs, f0, backend="ref"))
+    s.update_all_bcs()
+    s.step()
+    for k in s.names:
+        out["step_" + k] = s.var(k).copy()
+    meta = np.array([repr(cfg), repr(extra)])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=meta, **out)
+
+
 def main(names=None):
     for name, cfg in CASES.items():
         if not names or name in names:
@@ -150,6 +225,10 @@ def main(names=None):
     for name, (scheme, cfg) in SURFACE_CASES.items():
         if not names or name in names:
             make_surface(name, scheme, cfg)
+            print("wrote", name)
+    for name, (cfg, extra) in SGS_CASES.items():
+        if not names or name in names:
+            make_sgs(name, cfg, extra)
             print("wrote", name)
 
 
