@@ -352,6 +352,92 @@ def _time_surface(sim, cfg, peak, calls=50, warm=3):
             "frac": round(ach / peak, 4)}
 
 
+def _time_sgs(sim, peak, calls=10, warm=2):
+    """Smagorinsky subgrid scale and diffusion on the timed state: CUDA-event
+    time per launch of pb_kinematics_sgs (strain-rate magnitude + viscosity
+    and diffusivity), pb_scalar_diffusion (all scalars) and
+    pb_momentum_diffusion, with their algorithmic bytes per interior cell
+    (each field read once, each result written once, tendencies read and
+    written): 56, 8 + 24 per scalar, 112.  The tendencies are restored
+    afterwards."""
+    import ctypes
+
+    import torch
+
+    from pycles_b200 import _capi
+    Gr, PV, DV, RS = sim.Gr, sim.PV, sim.DV, sim.RS
+    L = _capi.load()
+    npg, dev = Gr.dims.npg, PV.values.device
+    smag, visc, diff = (torch.zeros(npg, dtype=torch.float64, device=dev) for _ in range(3))
+    sgs = _capi.PbSgs(_capi.PB_SGS_SMAGORINSKY, _capi.PB_SGS_LENGTH_GRID, 0.17, 1.0 / 3.0, 0.0, 0.0)
+    vel = [_capi.ptr(PV.values[int(PV.velocity_directions[d]) * npg:]) for d in range(3)]
+    tvel = [_capi.ptr(PV.tendencies[int(PV.velocity_directions[d]) * npg:]) for d in range(3)]
+    dvp = lambda n: _capi.ptr(DV.values[DV.get_varshift(Gr, n):])
+    scal = [i for i in range(PV.nv) if PV.var_type[i] == 1]
+    ns = len(scal)
+    vals = (ctypes.c_void_p * ns)(*[_capi.ptr(PV.values[i * npg:]) for i in scal])
+    tends = (ctypes.c_void_p * ns)(*[_capi.ptr(PV.tendencies[i * npg:]) for i in scal])
+    s_t = _capi.ptr(PV.tendencies[PV.get_varshift(Gr, "s"):])
+    st = _capi.stream_handle(None)
+    d = ctypes.byref(Gr.dims)
+    launches = {
+        "kinematics_sgs": (lambda: L.pb_kinematics_sgs(d, ctypes.byref(sgs), *vel, dvp("buoyancy_frequency"), None,
+                                                       _capi.ptr(smag), _capi.ptr(visc), _capi.ptr(diff), st), 56.0),
+        "scalar_diffusion": (lambda: L.pb_scalar_diffusion(d, _capi.ptr(RS.d_rho0), _capi.ptr(RS.d_rho0_half),
+                                                           _capi.ptr(RS.d_alpha0_half), _capi.ptr(diff), ns, vals,
+                                                           tends, None, -1, -1, None, None, None, st),
+                             8.0 + 24.0 * ns),
+        "momentum_diffusion": (lambda: L.pb_momentum_diffusion(
+            d, _capi.ptr(RS.d_rho0), _capi.ptr(RS.d_rho0_half), _capi.ptr(RS.d_alpha0), _capi.ptr(RS.d_alpha0_half),
+            *vel, _capi.ptr(visc), _capi.ptr(smag), dvp("temperature"), *tvel, s_t, st), 112.0),
+    }
+    tend = PV.tendencies.clone()
+    out = {}
+    stream = torch.cuda.current_stream()
+    for name, (fn, nbytes) in launches.items():
+        for _ in range(warm):
+            _capi.check(fn(), name)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(calls):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / calls
+        ach = nbytes * Gr.dims.npl / (ms / 1e3) / 1e9
+        out[name] = {"ms_per_launch": round(ms, 4), "algorithmic_bytes_per_cell": nbytes,
+                     "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
+    PV.tendencies.copy_(tend)
+    del smag, visc, diff, tend
+    out["scheme"] = "Smagorinsky (grid length scale), FP64; one launch of each kernel per RK stage"
+    return out
+
+
+def _time_stats(sim, peak, calls=10, warm=2):
+    """HorizontalMean of one prognostic field (the statistics' most common
+    reduction) on the timed state: CUDA-event time per call (two launches)
+    and the field's bytes over it."""
+    import torch
+
+    from pycles_b200.statistics import HorizontalStatistics
+    st = HorizontalStatistics(sim.Gr)
+    f = sim.PV.field("s", sim.Gr)
+    for _ in range(warm):
+        st.HorizontalMean(sim.Gr, f)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(calls):
+        st.HorizontalMean(sim.Gr, f)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / calls
+    nbytes = 8.0 * sim.Gr.dims.npg
+    ach = nbytes / (ms / 1e3) / 1e9
+    return {"reduction": "HorizontalMean of s", "ms_per_call": round(ms, 4), "bytes_per_call": nbytes,
+            "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -451,6 +537,8 @@ def run_ours(args, rank, world, local_rank):
     # ---- roofline per component; the headline is the largest one ----------
     peak, peak_kind = _peaks()
     surface = _time_surface(sim, cfg, peak) if not args.no_surface else None
+    sgs = _time_sgs(sim, peak) if not args.no_surface else None
+    stats = _time_stats(sim, peak) if not args.no_surface else None
     r = results[head]
     nv = PV.nv
     comps = {}
@@ -503,6 +591,8 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roofline,
             "e2e": e2e,
             "surface": surface,
+            "sgs": sgs,
+            "statistics": stats,
             "gpu_launches": r["gpu_launches"],
             "clocks": r["clocks"],
             "device_error_word": r["device_error_word"],
@@ -604,7 +694,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surface", action="store_true",
-                    help="skip the timing of the case's surface scheme (reported beside the step)")
+                    help="skip the timings of the case's surface scheme and of the Smagorinsky subgrid scale "
+                         "and diffusion (reported beside the step)")
     ap.add_argument("--cpu-cores", type=int, default=None)
     ap.add_argument("--seed-refresh-interval", type=int, default=0,
                     help="thermodynamics updates between refreshes of the learned seed (default: the "

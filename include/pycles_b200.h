@@ -527,6 +527,40 @@ int pb_momentum_diffusion(const pb_dims* dims, const double* rho0, const double*
                           const double* T, double* ut, double* vt, double* wt, double* s_tend, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Horizontal statistics
+ * --------------------------------------------------------------------- */
+
+/* The reductions of ParallelMPI (ParallelMPI.pyx:196-540), one rank. */
+enum pb_stat_kind {
+  PB_STAT_MEAN = 0,                      /* HorizontalMean :196-241                      */
+  PB_STAT_MEAN_SQUARES = 1,              /* HorizontalMeanofSquares :243-289 (v1 v2)     */
+  PB_STAT_MEAN_CUBES = 2,                /* HorizontalMeanofCubes :291-325 (v1 v2 v3)    */
+  PB_STAT_MAX = 3,                       /* HorizontalMaximum :327-357                   */
+  PB_STAT_MIN = 4,                       /* HorizontalMinimum :359-389                   */
+  PB_STAT_MEAN_SURFACE = 5,              /* HorizontalMeanSurface :391-428 (one plane)   */
+  PB_STAT_MEAN_CONDITIONAL = 6,          /* HorizontalMeanConditional :430-483           */
+  PB_STAT_MEAN_SQUARES_CONDITIONAL = 7   /* HorizontalMeanofSquaresConditional :485-540  */
+};
+
+/* Bytes of device scratch pb_horizontal_stat needs for this grid. */
+long long pb_stat_workspace_bytes(const pb_dims* dims);
+
+/*
+ * One horizontal statistic over the interior columns, per level: out[k],
+ * k = 0 .. nlg2-1 (device, nlg2 doubles), as the reference's loops and
+ * normalisation give it: the means times 1/(n0 n1); the conditional means
+ * divided by max(sum of the mask, 1); the maximum / minimum starting from
+ * -9e12 / 9e12.  PB_STAT_MEAN_SURFACE reduces one nlg0*nlg1 plane (indexed
+ * i*nlg1 + j) to out[0] and needs no workspace.  v2, v3, mask: NULL where
+ * the kind does not use them.  The sums use a fixed partition and order
+ * (deterministic; not the reference's sequential order, so sums agree to
+ * rounding).
+ */
+int pb_horizontal_stat(const pb_dims* dims, int kind, const double* v1, const double* v2, const double* v3,
+                       const double* mask, double* out, void* workspace, long long workspace_bytes,
+                       void* stream);
+
+/* ------------------------------------------------------------------------
  * Errors
  * --------------------------------------------------------------------- */
 

@@ -942,3 +942,52 @@ def compute_entropy_source(d: Dims, viscosity, strain_rate_mag, temperature, ent
     reg = _region(sh, d.gw, d.gw)
     S = strain_rate_mag.reshape(sh)[reg]
     entropy_tendency.reshape(sh)[reg] += S * S * viscosity.reshape(sh)[reg] / temperature.reshape(sh)[reg]
+
+
+# ---------------------------------------------------------------------------
+# horizontal statistics, ParallelMPI.pyx:196-540 (one rank; the loops'
+# sequential order: per level, i then j over the interior columns)
+# ---------------------------------------------------------------------------
+def _hsum(d: Dims, col, combine=None, init=0.0):
+    sh = d.shape
+    g_ = d.gw
+    acc = np.full(sh[2], init, dtype=np.float64)
+    for i in range(g_, sh[0] - g_):
+        for j in range(g_, sh[1] - g_):
+            v = col(i, j)
+            acc = acc + v if combine is None else combine(acc, v)
+    return acc
+
+
+def horizontal_stat(d: Dims, kind, v1, v2=None, v3=None, mask=None):
+    """HorizontalMean (:196-241), ...ofSquares (:243-289), ...ofCubes
+    (:291-325), HorizontalMaximum (:327-357), HorizontalMinimum (:359-389),
+    HorizontalMeanSurface (:391-428), HorizontalMeanConditional (:430-483),
+    HorizontalMeanofSquaresConditional (:485-540)."""
+    sh = d.shape
+    n_horizontal_i = 1.0 / float(d.n[1] * d.n[0])
+    A = v1.reshape(sh) if kind != "surface" else v1.reshape(sh[0], sh[1])
+    B = v2.reshape(sh) if v2 is not None else None
+    C = v3.reshape(sh) if v3 is not None else None
+    M = mask.reshape(sh) if mask is not None else None
+    if kind == "mean":
+        return _hsum(d, lambda i, j: A[i, j]) * n_horizontal_i
+    if kind == "squares":
+        return _hsum(d, lambda i, j: A[i, j] * B[i, j]) * n_horizontal_i
+    if kind == "cubes":
+        return _hsum(d, lambda i, j: A[i, j] * B[i, j] * C[i, j]) * n_horizontal_i
+    if kind == "max":
+        return _hsum(d, lambda i, j: A[i, j], np.fmax, -9e12)
+    if kind == "min":
+        return _hsum(d, lambda i, j: A[i, j], np.fmin, 9e12)
+    if kind == "surface":
+        g_ = d.gw
+        s = 0.0
+        for i in range(g_, sh[0] - g_):
+            for j in range(g_, sh[1] - g_):
+                s += A[i, j]
+        return s * n_horizontal_i
+    if kind in ("conditional", "squares_conditional"):
+        prod = (lambda i, j: A[i, j] * M[i, j]) if kind == "conditional" else (lambda i, j: A[i, j] * B[i, j] * M[i, j])
+        return _hsum(d, prod) / np.maximum(_hsum(d, lambda i, j: M[i, j]), 1.0)
+    raise ValueError(kind)

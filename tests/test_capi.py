@@ -82,6 +82,12 @@ def test_invalid_arguments_rejected_without_device():
     args = [p] * 14
     args[7] = None  # qt
     assert L.pb_surface_update(d, ctypes.byref(sc), *args, ctypes.byref(fields), None) == _capi.PB_ERR_ARG
+    assert L.pb_horizontal_stat(d, _capi.PB_STAT_MEAN, p, None, None, None, p, None, 0, None) == \
+        _capi.PB_ERR_WORKSPACE
+    assert L.pb_horizontal_stat(d, _capi.PB_STAT_MEAN_CUBES, p, p, None, None, p, p, 1 << 30, None) == \
+        _capi.PB_ERR_ARG
+    assert L.pb_horizontal_stat(d, 99, p, p, p, p, p, p, 1 << 30, None) == _capi.PB_ERR_ARG
+    assert L.pb_stat_workspace_bytes(d) == 2 * 296 * Gr.dims.nlg[2] * 8
     fields.scratch = None
     sc.scheme = _capi.PB_SURFACE_SULLIVAN_PATTON
     assert L.pb_surface_update(d, ctypes.byref(sc), *([p] * 14), ctypes.byref(fields), None) == _capi.PB_ERR_ARG

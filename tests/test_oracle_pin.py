@@ -338,3 +338,22 @@ def test_sgs_namelist_switches():
     assert c["variant"] == "wall"
     c = scheme_from_namelist({"sgs": {"scheme": "UniformViscosity"}})
     assert c["viscosity"] == 0.0 and c["diffusivity"] == 0.0 and not c["qt_entropy_source"]
+
+
+def test_horizontal_stat_restatement():
+    """The sequential restatement of ParallelMPI's reductions against numpy
+    reductions of the same interior columns (order aside, they agree), and
+    HorizontalMean against the one the pressure glue uses."""
+    nl, rs, f = host_case(**SMALL)
+    d = oracle_dims(nl)
+    rng = np.random.default_rng(2)
+    a, b = f["s"], rng.standard_normal(d.npg)
+    m = (rng.random(d.npg) < 0.5).astype(float)
+    g_ = d.gw
+    I = lambda x: x.reshape(d.shape)[g_:-g_, g_:-g_, :]
+    assert rel_l2(port.horizontal_stat(d, "mean", a), port.horizontal_mean(d, a)) < 1e-15
+    assert rel_l2(port.horizontal_stat(d, "squares", a, b), (I(a) * I(b)).mean(axis=(0, 1))) < 1e-13
+    assert np.array_equal(port.horizontal_stat(d, "max", b), I(b).max(axis=(0, 1)))
+    assert np.array_equal(port.horizontal_stat(d, "min", b), I(b).min(axis=(0, 1)))
+    cond = (I(b) * I(m)).sum(axis=(0, 1)) / np.maximum(I(m).sum(axis=(0, 1)), 1.0)
+    assert rel_l2(port.horizontal_stat(d, "conditional", b, mask=m), cond) < 1e-13
