@@ -251,11 +251,13 @@ __global__ void __launch_bounds__(kThreads) momentum_diffusion(MArgs a) {
   const int j = g.gw + blockIdx.y, i = g.gw + blockIdx.z;
   if (k >= g.n2 - g.gw) return;
   const long long ijk = (long long)i * g.is + (long long)j * g.js + k;
-#pragma unroll 1
+  // fully unrolled: the component indices fold into the stencil offsets
+  // and the loads shared by the nine fluxes are issued once
+#pragma unroll
   for (int i1 = 0; i1 < 3; ++i1) {
     double t = a.tend[i1][ijk];
     const double al = i1 != 2 ? a.alpha0_half[k] : a.alpha0[k];
-#pragma unroll 1
+#pragma unroll
     for (int i2 = 0; i2 < 3; ++i2) {
       const double fh = mflux(a, i1, i2, ijk, k);
       const double fl = mflux(a, i1, i2, ijk - stride_of(g, i2), i2 == 2 ? k - 1 : k);
