@@ -527,6 +527,51 @@ int pb_momentum_diffusion(const pb_dims* dims, const double* rho0, const double*
                           const double* T, double* ut, double* vt, double* wt, double* s_tend, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Case forcing
+ * --------------------------------------------------------------------- */
+
+/* Forcing schemes, as Forcing.__init__ (Forcing.pyx:29-67) picks them by case. */
+enum pb_forcing_scheme {
+  PB_FORCING_NONE = 0,
+  PB_FORCING_SULLIVAN_PATTON = 1,  /* ForcingSullivanPatton (Forcing.pyx:256-300): Coriolis */
+  PB_FORCING_BOMEX = 2,            /* ForcingBomex (:102-254): pressure gradient, sources, subsidence */
+  PB_FORCING_DYCOMS_RF01 = 3       /* ForcingDyCOMS_RF01 (:346-460): subsidence, Coriolis */
+};
+
+/*
+ * The scheme's per-level profiles (device, nlg2 doubles each, as the
+ * scheme's initialize sets them from Grid.zl_half and p0_half) and
+ * constants.  dtdt, dqtdt: Bomex's large-scale temperature and qt
+ * tendencies; subsidence: the large-scale vertical velocity (Bomex,
+ * DYCOMS_RF01); u0, v0: the Galilean shift.
+ */
+typedef struct pb_forcing {
+  int scheme;
+  double coriolis_param;
+  double u0, v0;
+  const double* ug;
+  const double* vg;
+  const double* dtdt;
+  const double* dqtdt;
+  const double* subsidence;
+} pb_forcing;
+
+/*
+ * Forcing.update for the scheme, in its order: Bomex -- large_scale_p_gradient
+ * (Forcing.pyx:1982-2011) with umean, vmean the horizontal means of u and v
+ * (pb_horizontal_stat), the entropy and qt sources (s_tendency_c,
+ * Csrc/entropies.h:17-21), then apply_subsidence (:2013-2039) of s, qt, u,
+ * v; DYCOMS_RF01 -- apply_subsidence of s, qt, u, v, then coriolis_force
+ * (:1954-1980); SullivanPatton -- coriolis_force.  As in the reference the
+ * subsidence also reaches the tendencies of the top ghost levels.
+ * PB_FORCING_NONE returns PB_OK without work.
+ */
+int pb_forcing_update(const pb_dims* dims, const pb_forcing* forcing, const double* p0_half,
+                      const double* umean, const double* vmean, const double* u, const double* v,
+                      const double* s, const double* qt, const double* ql, const double* T, double* ut,
+                      double* vt, double* s_tend, double* qt_tend, void* stream);
+
+/* ------------------------------------------------------------------------
  * Horizontal statistics
  * --------------------------------------------------------------------- */
 

@@ -4,8 +4,8 @@ TEST INFRASTRUCTURE ONLY.
 ``OracleSim`` reproduces one rank of ``Simulation3d.run`` (Simulation3d.pyx:
 140-189) restricted to the hot-path components, in the reference's order per
 RK stage: [Ke.update,] Th.update, SA.update, MA.update, [Sur.update,]
-[SGS.update, SD.update, MD.update,] TS.update, PV.Update_all_bcs,
-Pr.update.  The kernels come from one of two backends:
+[SGS.update, SD.update, MD.update,] [Fo.update,] TS.update,
+PV.Update_all_bcs, Pr.update.  The kernels come from one of two backends:
 
 * ``"ref"``  -- the reference's own C (oracle/ref.py), TDMA from the
                reference's cythonized SparseSolvers when it was built;
@@ -160,6 +160,7 @@ class OracleSim:
         self.secant_iters = None
         self.surface = None  # an oracle.surface.OracleSurface, updated after MA as Simulation3d.pyx:167
         self.sgs = None  # an oracle.sgs.OracleSGS: Ke at the stage start, SGS/SD/MD after Sur (:159-172)
+        self.forcing = None  # an oracle.forcing.OracleForcing, after SD/MD (:173)
         if moist:
             x, y = table_xy if table_xy is not None else cc_table()
             self.table_xy = (x, y)
@@ -326,6 +327,8 @@ class OracleSim:
             self.sgs.sgs_update(self)
             self.sgs.sd_update(self)
             self.sgs.md_update(self)
+        if self.forcing is not None:
+            self.forcing.update(self)
         self.ts_update(rk_step)
         self.update_all_bcs()
         self.pr_update()

@@ -991,3 +991,94 @@ def horizontal_stat(d: Dims, kind, v1, v2=None, v3=None, mask=None):
         prod = (lambda i, j: A[i, j] * M[i, j]) if kind == "conditional" else (lambda i, j: A[i, j] * B[i, j] * M[i, j])
         return _hsum(d, prod) / np.maximum(_hsum(d, lambda i, j: M[i, j]), 1.0)
     raise ValueError(kind)
+
+
+# ---------------------------------------------------------------------------
+# case forcing, Forcing.pyx (Cython, restated) + s_tendency_c (Csrc/entropies.h:17-21)
+# ---------------------------------------------------------------------------
+omega = 7.2921151467064e-5  # generate_parameters.py:38
+
+
+def s_tendency_c(p0, qt, qv, T, qt_tendency, T_tendency):
+    """Csrc/entropies.h:17-21."""
+    pv = pv_c(p0, qt, qv)
+    pd = pd_c(p0, qt, qv)
+    return cpm_c(qt) * T_tendency / T + (sv_c(pv, T) - sd_c(pd, T)) * qt_tendency
+
+
+def forcing_profiles(scheme, zl_half, p0_half):
+    """The profiles each forcing's initialize sets (Forcing.pyx: SullivanPatton
+    :260-268, Bomex :106-152, DyCOMS_RF01 :347-389), from Grid.zl_half."""
+    n = len(zl_half)
+    z = np.asarray(zl_half, dtype=np.float64)
+    P = {k: np.zeros(n) for k in ("ug", "vg", "dtdt", "dqtdt", "subsidence")}
+    if scheme == "SullivanPatton":
+        P["ug"][:] = 1.0
+        P["coriolis_param"] = 1.0e-4
+    elif scheme == "Bomex":
+        P["coriolis_param"] = 0.376e-4
+        for k in range(n):
+            P["ug"][k] = -10.0 + (1.8e-3) * z[k]
+            ex = float(exner_c(p0_half[k]))
+            if z[k] <= 1500.0:
+                P["dtdt"][k] = (-2.0 / (3600 * 24.0)) * ex
+            if z[k] > 1500.0:
+                P["dtdt"][k] = (-2.0 / (3600 * 24.0) + (z[k] - 1500.0) * (0.0 - -2.0 / (3600 * 24.0))
+                                / (3000.0 - 1500.0)) * ex
+            if z[k] <= 300.0:
+                P["dqtdt"][k] = -1.2e-8
+            if z[k] > 300.0 and z[k] <= 500.0:
+                P["dqtdt"][k] = -1.2e-8 + (z[k] - 300.0) * (0.0 - -1.2e-8) / (500.0 - 300.0)
+            if z[k] <= 1500.0:
+                P["subsidence"][k] = 0.0 + z[k] * (-0.65 / 100.0 - 0.0) / (1500.0 - 0.0)
+            if z[k] > 1500.0 and z[k] <= 2100.0:
+                P["subsidence"][k] = -0.65 / 100 + (z[k] - 1500.0) * (0.0 - -0.65 / 100.0) / (2100.0 - 1500.0)
+    elif scheme == "DYCOMS_RF01":
+        divergence = 3.75e-6
+        P["coriolis_param"] = 2.0 * omega * math.sin(31.5 * pi / 180.0)
+        for k in range(n):
+            P["subsidence"][k] = -z[k] * divergence
+        P["ug"][:] = 7.0
+        P["vg"][:] = -5.5
+    else:
+        raise ValueError(scheme)
+    return P
+
+
+def apply_subsidence(d: Dims, rho0, rho0_half, subsidence, values, tendencies):
+    """Forcing.pyx:2013-2039: over the interior columns, for k in [gw,
+    nlg2-gw-1) tend = (phi[k+1] - phi[k]) dzi sub[k] is subtracted; the
+    levels from nlg2-gw-1 up (the top interior level and the ghosts) get the
+    last tend subtracted again."""
+    sh = d.shape
+    g_ = d.gw
+    V = values.reshape(sh)[g_:sh[0] - g_, g_:sh[1] - g_, :]
+    T = tendencies.reshape(sh)[g_:sh[0] - g_, g_:sh[1] - g_, :]
+    kmax = sh[2] - g_ - 1
+    tend = (V[:, :, g_ + 1:kmax + 1] - V[:, :, g_:kmax]) * d.dxi[2] * subsidence[None, None, g_:kmax]
+    T[:, :, g_:kmax] -= tend
+    T[:, :, kmax:] -= tend[:, :, -1:]
+
+
+def coriolis_force(d: Dims, u, v, ut, vt, ug, vg, coriolis_param, u0, v0):
+    """Forcing.pyx:1954-1980."""
+    sh = d.shape
+    r = _region(sh, d.gw, d.gw)
+    U, V = u.reshape(sh), v.reshape(sh)
+    def at(A, di, dj):
+        return A[r[0].start + di:r[0].stop + di, r[1].start + dj:r[1].stop + dj, r[2]]
+    u_at_v = 0.25 * (U[r] + at(U, -1, 0) + at(U, -1, 1) + at(U, 0, 1)) + u0
+    v_at_u = 0.25 * (V[r] + at(V, 1, 0) + at(V, 1, -1) + at(V, 0, -1)) + v0
+    k = _kvec(np.asarray(vg), r)
+    ut.reshape(sh)[r] = ut.reshape(sh)[r] - coriolis_param * (k - v_at_u)
+    vt.reshape(sh)[r] = vt.reshape(sh)[r] + coriolis_param * (_kvec(np.asarray(ug), r) - u_at_v)
+
+
+def large_scale_p_gradient(d: Dims, umean, vmean, ut, vt, ug, vg, coriolis_param, u0, v0):
+    """Forcing.pyx:1982-2011."""
+    sh = d.shape
+    r = _region(sh, d.gw, d.gw)
+    u_at_v = _kvec(np.asarray(umean), r) + u0
+    v_at_u = _kvec(np.asarray(vmean), r) + v0
+    ut.reshape(sh)[r] = ut.reshape(sh)[r] - coriolis_param * (_kvec(np.asarray(vg), r) - v_at_u)
+    vt.reshape(sh)[r] = vt.reshape(sh)[r] + coriolis_param * (_kvec(np.asarray(ug), r) - u_at_v)

@@ -281,3 +281,12 @@ def compute_entropy_source(d: Dims, viscosity, strain_rate_mag, temperature, ent
     dc = d.c()
     _fn("compute_entropy_source", [ctypes.c_void_p] + [_dp] * 4)(
         ctypes.byref(dc), _p(viscosity), _p(strain_rate_mag), _p(temperature), _p(entropy_tendency))
+
+
+def s_tendency_c(p0, qt, qv, T, qt_tendency, T_tendency):
+    f = _fn("ref_s_tendency", [ctypes.c_double] * 6, ctypes.c_double)
+    b = np.broadcast_arrays(*[np.asarray(x, dtype=np.float64) for x in (p0, qt, qv, T, qt_tendency, T_tendency)])
+    out = np.empty(b[0].shape)
+    for idx in np.ndindex(out.shape):
+        out[idx] = f(*[float(x[idx]) for x in b])
+    return out

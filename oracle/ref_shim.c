@@ -121,3 +121,8 @@ void ref_compute_qt_diffusion_s_source(struct DimStruct* dims, double* p0_half, 
     compute_qt_diffusion_s_source(dims, p0_half, alpha0, alpha0_half, flux, qt, qv, T, tendency,
                                   shim_lambda_constant, shim_latent_heat_variable, dx, d);
 }
+
+/* Csrc/entropies.h:17-21 (the forcing's entropy source) */
+double ref_s_tendency(double p0, double qt, double qv, double T, double qt_tendency, double T_tendency) {
+    return s_tendency_c(p0, qt, qv, T, qt_tendency, T_tendency);
+}

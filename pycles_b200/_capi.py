@@ -60,6 +60,13 @@ PB_FP64, PB_FP32 = 0, 1
 PB_SURFACE_NONE, PB_SURFACE_SULLIVAN_PATTON, PB_SURFACE_BOMEX, PB_SURFACE_DYCOMS_RF01 = 0, 1, 2, 3
 PB_SURFACE_SCRATCH = 512
 PB_SGS_UNIFORM, PB_SGS_SMAGORINSKY = 1, 2
+PB_FORCING_NONE, PB_FORCING_SULLIVAN_PATTON, PB_FORCING_BOMEX, PB_FORCING_DYCOMS_RF01 = 0, 1, 2, 3
+
+
+class PbForcing(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("coriolis_param", ctypes.c_double), ("u0", ctypes.c_double),
+                ("v0", ctypes.c_double), ("ug", _vp), ("vg", _vp), ("dtdt", _vp), ("dqtdt", _vp),
+                ("subsidence", _vp)]
 (PB_STAT_MEAN, PB_STAT_MEAN_SQUARES, PB_STAT_MEAN_CUBES, PB_STAT_MAX, PB_STAT_MIN, PB_STAT_MEAN_SURFACE,
  PB_STAT_MEAN_CONDITIONAL, PB_STAT_MEAN_SQUARES_CONDITIONAL) = range(8)
 PB_SGS_LENGTH_GRID, PB_SGS_LENGTH_WALL, PB_SGS_LENGTH_ILES = 0, 1, 2
@@ -109,6 +116,7 @@ SIGNATURES = {
     "pb_momentum_diffusion": (_I, [_DIMS] + [_P] * 15),
     "pb_stat_workspace_bytes": (_LL, [_DIMS]),
     "pb_horizontal_stat": (_I, [_DIMS, _I, _P, _P, _P, _P, _P, _P, _LL, _P]),
+    "pb_forcing_update": (_I, [_DIMS, ctypes.POINTER(PbForcing)] + [_P] * 14),
     "pb_get_error": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "pb_clear_error": (_I, [_P]),
     "pb_status_string": (ctypes.c_char_p, [_I]),

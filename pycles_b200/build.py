@@ -48,13 +48,13 @@ def nvcc() -> str:
 
 
 # Translation units and their extra flags.  The thermodynamics, the FP64
-# plain-form advection, the surface fluxes, the subgrid scale and the
-# statistics are compiled without FMA contraction so that they
+# plain-form advection, the surface fluxes, the subgrid scale, the
+# statistics and the forcing are compiled without FMA contraction so that they
 # follow the reference's separately rounded arithmetic (see csrc/crmath.cuh
 # and csrc/advection_f64.cu).
 UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"]), ("advection_f64.cu", ["-fmad=false"]),
          ("thermo_fast.cu", []), ("surface.cu", ["-fmad=false"]), ("sgs.cu", ["-fmad=false"]),
-         ("stats.cu", ["-fmad=false"])]
+         ("stats.cu", ["-fmad=false"]), ("forcing.cu", ["-fmad=false"])]
 
 
 def _run(cmd):

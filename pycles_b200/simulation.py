@@ -18,6 +18,7 @@ from .advection import MomentumAdvection, ScalarAdvection
 from .grid import Grid
 from .pressure import PressureSolver
 from .reference_state import ReferenceState
+from .forcing import ForcingFactory
 from .sgs import SGS, Kinematics, MomentumDiffusion, ScalarDiffusion
 from .surface import SurfaceFactory
 from .thermodynamics import ThermodynamicsDry, ThermodynamicsSA
@@ -65,6 +66,7 @@ class HotPathSimulation:
         self.TS = TimeStepping()
         self.RS = ReferenceState(Gr)
         self.Sur = SurfaceFactory(namelist)
+        self.Fo = ForcingFactory(namelist)
         # subgrid scale and diffusion when the namelist has an sgs section
         # (the measured configurations have none)
         self.SGS = SGS(namelist) if "sgs" in namelist else None
@@ -84,6 +86,7 @@ class HotPathSimulation:
         PV.initialize(Gr, device=self.device)
         self.DV.initialize(Gr, device=self.device)
         self.Sur.initialize(Gr, self.RS)
+        self._fo_ready = False
         if self.SGS is not None:
             self.Ke.initialize(Gr)
             self.SGS.initialize(Gr, PV)
@@ -145,7 +148,8 @@ class HotPathSimulation:
         unless fuse_rk is off or a surface scheme adds tendencies between the
         advection and the stage."""
         return (self.fuse_rk and self.MA.precision == _capi.PB_FP32
-                and self.Sur.scheme == _capi.PB_SURFACE_NONE and self.SGS is None)
+                and self.Sur.scheme == _capi.PB_SURFACE_NONE and self.SGS is None
+                and self.Fo.scheme == _capi.PB_FORCING_NONE)
 
     def _clear_w_tendency(self, stream=None):
         """Fused stepping: the w tendency is cleared once the fused pass has
@@ -204,6 +208,11 @@ class HotPathSimulation:
                 self.SGS.update(Gr, self.DV, PV, self.Ke, self.Sur, stream=stream)
                 self.SD.update(Gr, RS, PV, self.DV, stream=stream)
                 self.MD.update(Gr, RS, PV, self.DV, self.Ke, stream=stream)
+            if self.Fo.scheme != _capi.PB_FORCING_NONE:  # Fo.update (:173)
+                if not self._fo_ready:  # the profiles need the installed reference state
+                    self.Fo.initialize(Gr, RS)
+                    self._fo_ready = True
+                self.Fo.update(Gr, RS, PV, self.DV, stream=stream)
             m(3)
             TS.update(Gr, PV, stream=stream)
             return

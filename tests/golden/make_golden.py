@@ -11,7 +11,9 @@ time step, and Simulation3d.run's prologue + one step.  The surface
 fixtures hold, per surface scheme, the scheme's update after the
 thermodynamics and one time step with the scheme in the stage; the sgs
 fixtures the strain-rate magnitude, viscosity and diffusivity, the scalar
-and momentum diffusion tendencies and one time step with them.
+and momentum diffusion tendencies and one time step with them; the case
+fixtures the case forcing's tendencies and one time step of the whole case
+(surface, forcing, subgrid scale).
 """
 from __future__ import annotations
 
@@ -217,6 +219,65 @@ def make_sgs(name, cfg, extra):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=meta, **out)
 
 
+# whole cases: the case's surface scheme and forcing (and, where given, the
+# subgrid scale), chosen by meta.casename as the reference does
+FORCING_CASES = {
+    "case_bomex": (dict(case="bomex", nx=12, ny=10, nz=16, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0),
+                   {"meta": {"casename": "Bomex"}}),
+    "case_dycoms_rf01": (dict(case="dycoms", nx=8, ny=10, nz=16, dx=35.0, dy=35.0, dz=60.0, gw=4, dt=0.25,
+                              scalar_order=7, momentum_order=5),
+                         {"meta": {"casename": "DYCOMS_RF01"}, "sgs": {"scheme": "Smagorinsky"}}),
+    "case_sullivan_patton": (dict(case="dry_cbl", nx=8, ny=8, nz=12, dx=50.0, dy=50.0, dz=50.0, gw=3, dt=0.5),
+                             {"meta": {"casename": "SullivanPatton"},
+                              "sgs": {"scheme": "Smagorinsky", "Smagorinsky": {"wall": True}}}),
+}
+
+
+def make_case(name, cfg, extra):
+    """The case forcing's tendencies after the thermodynamics, and one time
+    step with the case's surface, forcing and subgrid scale in the stage."""
+    from helpers import host_case, oracle_dims, oracle_sim
+    from oracle import ref
+    from oracle.forcing import OracleForcing
+    from oracle.sgs import OracleSGS, scheme_from_namelist
+    from oracle.surface import OracleSurface
+    from pycles_b200.grid import Grid
+    assert ref.available(), "oracle/_ref missing: run oracle/build_ref.py"
+    nl, rs, f0 = host_case(**cfg)
+    nl = dict(nl, **extra)
+    f = stir(f0)
+    d = oracle_dims(nl)
+    zl_half = Grid(nl).zl_half
+    casename = extra["meta"]["casename"]
+
+    def attach(s):
+        s.surface = OracleSurface(casename, d, u0=rs["u0"], v0=rs["v0"])
+        s.forcing = OracleForcing(casename, d, rs["p0_half"], zl_half, u0=rs["u0"], v0=rs["v0"])
+        if "sgs" in nl:
+            s.sgs = OracleSGS(scheme_from_namelist(nl), d, zl_half)
+        return s
+
+    out = {"rs_" + k: np.asarray(v) for k, v in rs.items()}
+    for k, v in f.items():
+        out["in_" + k] = v
+    for k, v in f0.items():
+        out["in0_" + k] = v
+    s = attach(oracle_sim(nl, rs, f, backend="ref"))
+    s.update_all_bcs()
+    s.th_update()
+    s.tendencies[:] = 0.0
+    s.forcing.update(s)
+    for k in s.names:
+        out["fotend_" + k] = s.tend(k).copy()
+    s = attach(oracle_sim(nl, rs, f0, backend="ref"))
+    s.update_all_bcs()
+    s.step()
+    for k in s.names:
+        out["step_" + k] = s.var(k).copy()
+    meta = np.array([repr(cfg), repr(extra)])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=meta, **out)
+
+
 def main(names=None):
     for name, cfg in CASES.items():
         if not names or name in names:
@@ -229,6 +290,10 @@ def main(names=None):
     for name, (cfg, extra) in SGS_CASES.items():
         if not names or name in names:
             make_sgs(name, cfg, extra)
+            print("wrote", name)
+    for name, (cfg, extra) in FORCING_CASES.items():
+        if not names or name in names:
+            make_case(name, cfg, extra)
             print("wrote", name)
 
 

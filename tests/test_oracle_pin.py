@@ -357,3 +357,64 @@ def test_horizontal_stat_restatement():
     assert np.array_equal(port.horizontal_stat(d, "min", b), I(b).min(axis=(0, 1)))
     cond = (I(b) * I(m)).sum(axis=(0, 1)) / np.maximum(I(m).sum(axis=(0, 1)), 1.0)
     assert rel_l2(port.horizontal_stat(d, "conditional", b, mask=m), cond) < 1e-13
+
+
+# ---- whole cases: surface + forcing (+ subgrid scale) ----------------------
+CASE_FIXTURES = ["case_bomex", "case_dycoms_rf01", "case_sullivan_patton"]
+
+
+@pytest.mark.parametrize("name", CASE_FIXTURES)
+def test_case_golden_port(name):
+    """The restated forcing (and surface, subgrid scale) on the numpy
+    restatement reproduces the reference-generated case fixtures: the
+    forcing tendencies bit for bit, one time step to 1e-13."""
+    from oracle.forcing import OracleForcing
+    from oracle.sgs import OracleSGS, scheme_from_namelist
+    from oracle.surface import OracleSurface
+    from pycles_b200.grid import Grid
+    z, nl, rs, f, f0 = _sgs_fixture(name)
+    d = oracle_dims(nl)
+    casename = nl["meta"]["casename"]
+    zl = Grid(nl).zl_half
+
+    def attach(s):
+        s.surface = OracleSurface(casename, d, u0=float(rs["u0"]), v0=float(rs["v0"]))
+        s.forcing = OracleForcing(casename, d, rs["p0_half"], zl, u0=float(rs["u0"]), v0=float(rs["v0"]))
+        if "sgs" in nl:
+            s.sgs = OracleSGS(scheme_from_namelist(nl), d, zl)
+        return s
+
+    s = attach(oracle_sim(nl, rs, f, "port"))
+    s.update_all_bcs()
+    s.th_update()
+    s.tendencies[:] = 0.0
+    s.forcing.update(s)
+    for k in s.names:
+        assert np.array_equal(s.tend(k), z["fotend_" + k]), k
+    s = attach(oracle_sim(nl, rs, f0, "port"))
+    s.update_all_bcs()
+    s.step()
+    for k in s.names:
+        assert rel_l2(s.var(k), z["step_" + k]) < 1e-13, k
+
+
+@pytest.mark.parametrize("casename", ["SullivanPatton", "Bomex", "DYCOMS_RF01"])
+def test_forcing_profiles_match_restatement(casename):
+    """The package's host-side forcing profiles (pycles_b200/forcing.py) equal
+    the oracle's restatement of the schemes' initialize, bit for bit."""
+    from pycles_b200.forcing import ForcingFactory
+    from pycles_b200.grid import Grid
+    nl, rs, f = host_case(**SMALL)
+    Gr = Grid(nl)
+    Gr.device = "cpu"
+    fo = ForcingFactory({"meta": {"casename": casename}})
+
+    class RS:
+        p0_half = rs["p0_half"]
+
+    P = {k: np.zeros(len(Gr.zl_half)) for k in ("ug", "vg", "dtdt", "dqtdt", "subsidence")}
+    fo._profiles(np.asarray(Gr.zl_half), np.asarray(RS.p0_half), P)
+    O = port.forcing_profiles(casename, Gr.zl_half, rs["p0_half"])
+    for k in P:
+        assert np.array_equal(P[k], O[k]), k
+    assert fo.coriolis_param == O["coriolis_param"]
