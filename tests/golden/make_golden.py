@@ -113,7 +113,8 @@ SURFACE_CASES = {
 def make_surface(name, scheme, cfg):
     """The surface scheme's update after the thermodynamics (fluxes and the
     tendencies of the first interior level), and one time step with the
-    scheme in the stage, from the reference's C driven by the restated glue."""
+    scheme and the case's forcing in the stage, from the reference's C driven
+    by the restated glue."""
     from helpers import host_case, oracle_dims, oracle_sim
     from oracle import ref
     from oracle.surface import OracleSurface
@@ -136,8 +137,12 @@ def make_surface(name, scheme, cfg):
         out["sur_" + n] = getattr(s.surface, n).copy()
     for k in s.names:
         out["surtend_" + k] = s.tend(k).copy()
+    # the case name selects the forcing too (Forcing.pyx:29-67)
+    from oracle.forcing import OracleForcing
+    from pycles_b200.grid import Grid
     s = oracle_sim(nl, rs, f0, backend="ref")
     s.surface = OracleSurface(scheme, d, u0=rs["u0"], v0=rs["v0"])
+    s.forcing = OracleForcing(scheme, d, rs["p0_half"], Grid(nl).zl_half, u0=rs["u0"], v0=rs["v0"])
     s.update_all_bcs()
     s.step()
     for k in s.names:
@@ -186,7 +191,9 @@ def make_sgs(name, cfg, extra):
     def attach(s):
         s.sgs = OracleSGS(conf, d, zl_half)
         if casename:
+            from oracle.forcing import OracleForcing
             s.surface = OracleSurface(casename, d, u0=rs["u0"], v0=rs["v0"])
+            s.forcing = OracleForcing(casename, d, rs["p0_half"], zl_half, u0=rs["u0"], v0=rs["v0"])
         return s
 
     out = {"rs_" + k: np.asarray(v) for k, v in rs.items()}

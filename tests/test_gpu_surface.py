@@ -62,8 +62,9 @@ def test_surface_update_vs_reference_golden(name, precision):
 
 @pytest.mark.parametrize("name", NAMES)
 def test_surface_step_vs_reference_golden(name):
-    """One time step with the scheme between the advection and the SSP-RK3
-    stage (Simulation3d.pyx:165-175)."""
+    """One time step with the scheme (and the case's forcing, which the case
+    name selects as well) between the advection and the SSP-RK3 stage
+    (Simulation3d.pyx:165-175)."""
     z, nl, rs, _, f0 = _load(name)
     for precision, tol in (("fp64", 1e-12), ("fp32", 1e-6)):
         g = gpu_sim(nl, rs, f0, precision=precision)

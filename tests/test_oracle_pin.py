@@ -243,8 +243,11 @@ def test_surface_golden_port(name):
         assert np.array_equal(getattr(s.surface, n), z["sur_" + n]), n
     for k in s.names:
         assert np.array_equal(s.tend(k), z["surtend_" + k]), k
+    from oracle.forcing import OracleForcing
+    from pycles_b200.grid import Grid
     s = oracle_sim(nl, rs, f0, "port")
     s.surface = OracleSurface(scheme, d, u0=float(rs["u0"]), v0=float(rs["v0"]))
+    s.forcing = OracleForcing(scheme, d, rs["p0_half"], Grid(nl).zl_half, u0=float(rs["u0"]), v0=float(rs["v0"]))
     s.update_all_bcs()
     s.step()
     for k in s.names:
@@ -301,7 +304,10 @@ def test_sgs_golden_port(name):
     def attach(s):
         s.sgs = OracleSGS(conf, d, Grid(nl).zl_half)
         if casename:
+            from oracle.forcing import OracleForcing
             s.surface = OracleSurface(casename, d, u0=float(rs["u0"]), v0=float(rs["v0"]))
+            s.forcing = OracleForcing(casename, d, rs["p0_half"], Grid(nl).zl_half, u0=float(rs["u0"]),
+                                      v0=float(rs["v0"]))
         return s
 
     s = attach(oracle_sim(nl, rs, f, "port"))
