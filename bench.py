@@ -438,6 +438,37 @@ def _time_stats(sim, peak, calls=10, warm=2):
             "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
 
 
+def _time_forcing(sim, cfg, peak, calls=10, warm=2):
+    """The case forcing of the configuration's case (DYCOMS_RF01 on the DYCOMS
+    workload) on the timed state: CUDA-event time per call, with its
+    algorithmic bytes per interior cell (read s, qt, u, v; read and write
+    their tendencies: 96 B; Bomex also reads ql and T: 112 B; SullivanPatton
+    u, v and their tendencies: 48 B).  The tendencies are restored."""
+    import torch
+
+    from pycles_b200.forcing import ForcingFactory
+    scheme = SURFACE_OF_CASE[cfg["case"]]
+    fo = ForcingFactory({"meta": {"casename": scheme}})
+    fo.initialize(sim.Gr, sim.RS)
+    args = (sim.Gr, sim.RS, sim.PV, sim.DV)
+    tend = sim.PV.tendencies.clone()
+    for _ in range(warm):
+        fo.update(*args)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(calls):
+        fo.update(*args)
+    b.record(stream)
+    torch.cuda.synchronize()
+    sim.PV.tendencies.copy_(tend)
+    ms = a.elapsed_time(b) / calls
+    nbytes = {"SullivanPatton": 48.0, "Bomex": 112.0, "DYCOMS_RF01": 96.0}[scheme]
+    ach = nbytes * sim.Gr.dims.npl / (ms / 1e3) / 1e9
+    return {"scheme": scheme, "ms_per_call": round(ms, 4), "algorithmic_bytes_per_cell": nbytes,
+            "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -539,6 +570,7 @@ def run_ours(args, rank, world, local_rank):
     surface = _time_surface(sim, cfg, peak) if not args.no_surface else None
     sgs = _time_sgs(sim, peak) if not args.no_surface else None
     stats = _time_stats(sim, peak) if not args.no_surface else None
+    forcing = _time_forcing(sim, cfg, peak) if not args.no_surface else None
     r = results[head]
     nv = PV.nv
     comps = {}
@@ -593,6 +625,7 @@ def run_ours(args, rank, world, local_rank):
             "surface": surface,
             "sgs": sgs,
             "statistics": stats,
+            "forcing": forcing,
             "gpu_launches": r["gpu_launches"],
             "clocks": r["clocks"],
             "device_error_word": r["device_error_word"],
@@ -694,8 +727,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surface", action="store_true",
-                    help="skip the timings of the case's surface scheme and of the Smagorinsky subgrid scale "
-                         "and diffusion (reported beside the step)")
+                    help="skip the timings of the case's surface scheme and forcing, of the Smagorinsky "
+                         "subgrid scale and diffusion and of a horizontal mean (reported beside the step)")
     ap.add_argument("--cpu-cores", type=int, default=None)
     ap.add_argument("--seed-refresh-interval", type=int, default=0,
                     help="thermodynamics updates between refreshes of the learned seed (default: the "
