@@ -87,11 +87,14 @@ __global__ void __launch_bounds__(kThreads) kinematics_sgs(KArgs a) {
   double m = 0.0;
   if (i >= 1 && i < g.n0 - 1 && j >= 1 && j < g.n1 - 1 && k >= 1 && k < g.n2 - 1) {
     const int c[3] = {i, j, k};
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double t = strain(g, a.V, d, d, ijk - stride_of(g, d));
       m += t * t;
     }
+#pragma unroll
     for (int v1 = 0; v1 < 2; ++v1) {
+#pragma unroll
       for (int d = v1; d < 3; ++d) {
         const long long s1 = stride_of(g, v1), sd = stride_of(g, d);
         const double p1 = strain(g, a.V, v1, d, ijk);
