@@ -572,6 +572,31 @@ int pb_forcing_update(const pb_dims* dims, const pb_forcing* forcing, const doub
                       double* vt, double* s_tend, double* qt_tend, void* stream);
 
 /* ------------------------------------------------------------------------
+ * DYCOMS radiation
+ * --------------------------------------------------------------------- */
+
+/* RadiationDyCOMS_RF01's constants (Radiation.pyx:231-240): f0 (namelist
+ * radiation.dycoms_f0, default 70), f1 = 22, kap = 85, alpha_z = 1,
+ * divergence = 3.75e-6. */
+typedef struct pb_dycoms_radiation_params {
+  double f0, f1, kap, alpha_z, divergence;
+} pb_dycoms_radiation_params;
+
+/*
+ * RadiationDyCOMS_RF01.update (Radiation.pyx:252-353) on one rank: per
+ * interior column the level of the 8 g/kg qt isoline zi, the flux F of
+ * Stevens et al. 2005 eq. 3 on the n2+1 faces, the heating rate
+ * -(F[k+1] - F[k]) dzi / rho0_half[k] (indexed without the ghost offset,
+ * as the reference does) into heating_rate (interior cells), then
+ * s_tend += heating / T and dTdt_rad = heating / cpm(qt).  z: Grid.z
+ * (nlg2 face heights).  A column with no level above 8 g/kg takes zi above
+ * the domain (the reference reuses the previous pencil's zi there).
+ */
+int pb_dycoms_radiation(const pb_dims* dims, const pb_dycoms_radiation_params* params,
+                        const double* rho0_half, const double* z, const double* ql, const double* qt,
+                        const double* T, double* s_tend, double* heating_rate, double* dTdt_rad, void* stream);
+
+/* ------------------------------------------------------------------------
  * Horizontal statistics
  * --------------------------------------------------------------------- */
 

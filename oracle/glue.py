@@ -4,7 +4,7 @@ TEST INFRASTRUCTURE ONLY.
 ``OracleSim`` reproduces one rank of ``Simulation3d.run`` (Simulation3d.pyx:
 140-189) restricted to the hot-path components, in the reference's order per
 RK stage: [Ke.update,] Th.update, SA.update, MA.update, [Sur.update,]
-[SGS.update, SD.update, MD.update,] [Fo.update,] TS.update,
+[SGS.update, SD.update, MD.update,] [Fo.update,] [Ra.update,] TS.update,
 PV.Update_all_bcs, Pr.update.  The kernels come from one of two backends:
 
 * ``"ref"``  -- the reference's own C (oracle/ref.py), TDMA from the
@@ -161,6 +161,7 @@ class OracleSim:
         self.surface = None  # an oracle.surface.OracleSurface, updated after MA as Simulation3d.pyx:167
         self.sgs = None  # an oracle.sgs.OracleSGS: Ke at the stage start, SGS/SD/MD after Sur (:159-172)
         self.forcing = None  # an oracle.forcing.OracleForcing, after SD/MD (:173)
+        self.radiation = None  # an oracle.radiation.OracleRadiation, after Fo (:174)
         if moist:
             x, y = table_xy if table_xy is not None else cc_table()
             self.table_xy = (x, y)
@@ -329,6 +330,8 @@ class OracleSim:
             self.sgs.md_update(self)
         if self.forcing is not None:
             self.forcing.update(self)
+        if self.radiation is not None:
+            self.radiation.update(self)
         self.ts_update(rk_step)
         self.update_all_bcs()
         self.pr_update()

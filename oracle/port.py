@@ -1082,3 +1082,52 @@ def large_scale_p_gradient(d: Dims, umean, vmean, ut, vt, ug, vg, coriolis_param
     v_at_u = _kvec(np.asarray(vmean), r) + v0
     ut.reshape(sh)[r] = ut.reshape(sh)[r] - coriolis_param * (_kvec(np.asarray(vg), r) - v_at_u)
     vt.reshape(sh)[r] = vt.reshape(sh)[r] + coriolis_param * (_kvec(np.asarray(ug), r) - u_at_v)
+
+
+# ---------------------------------------------------------------------------
+# DYCOMS radiation, Radiation.pyx:230-353 (Cython, restated)
+# ---------------------------------------------------------------------------
+def dycoms_radiation(d: Dims, rho0_half, z, ql, qt, T, s_tend, heating_rate, dTdt_rad, f0=70.0, f1=22.0,
+                     kap=85.0, alpha_z=1.0, divergence=3.75e-6):
+    """RadiationDyCOMS_RF01.update on one rank: per interior column (z
+    pencils in i, j order) zi/rhoi at the highest level with qt > 8e-3 (kept
+    from the previous column when none qualifies, as the reference's
+    variables are), the three flux terms of Stevens et al. 2005 eq. 3, the
+    heating rate -(F[k+1] - F[k]) dzi / rho0_half[k] (the reference indexes
+    rho0_half without the ghost offset here), then s_tend += heating / T and
+    dTdt_rad = heating / cpm(qt)."""
+    sh = d.shape
+    g_ = d.gw
+    n2 = d.n[2]
+    dz, dzi = d.dx[2], d.dxi[2]
+    QL, QT = ql.reshape(sh), qt.reshape(sh)
+    H = heating_rate.reshape(sh)
+    zi = rhoi = float("nan")
+    for i in range(g_, sh[0] - g_):
+        for j in range(g_, sh[1] - g_):
+            for k in range(n2):
+                if QT[i, j, g_ + k] > 8e-3:
+                    zi = z[g_ + k]
+                    rhoi = rho0_half[g_ + k]
+            f = [0.0] * (n2 + 1)
+            for k in range(n2):
+                if z[g_ + k] >= zi:
+                    c = math.cbrt(z[g_ + k] - zi)
+                    f[k + 1] = rhoi * cpd * divergence * alpha_z * (math.pow(c, 4) / 4.0 + zi * c)
+                else:
+                    f[k + 1] = 0.0
+            q1 = 0.0
+            f[0] += f1 * math.exp(-q1)
+            for k in range(1, n2 + 1):
+                q1 += kap * rho0_half[g_ + k - 1] * QL[i, j, g_ + k - 1] * dz
+                f[k] += f1 * math.exp(-q1)
+            q0 = 0.0
+            f[n2] += f0 * math.exp(-q0)
+            for k in range(n2 - 1, -1, -1):
+                q0 += kap * rho0_half[g_ + k] * QL[i, j, g_ + k] * dz
+                f[k] += f0 * math.exp(-q0)
+            for k in range(n2):
+                H[i, j, g_ + k] = -(f[k + 1] - f[k]) * dzi / rho0_half[k]
+    r = _region(sh, g_, g_)
+    s_tend.reshape(sh)[r] += H[r] / T.reshape(sh)[r]
+    dTdt_rad.reshape(sh)[r] = H[r] / cpm_c(QT[r])

@@ -63,6 +63,10 @@ PB_SGS_UNIFORM, PB_SGS_SMAGORINSKY = 1, 2
 PB_FORCING_NONE, PB_FORCING_SULLIVAN_PATTON, PB_FORCING_BOMEX, PB_FORCING_DYCOMS_RF01 = 0, 1, 2, 3
 
 
+class PbDycomsRadiation(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("f0", "f1", "kap", "alpha_z", "divergence")]
+
+
 class PbForcing(ctypes.Structure):
     _fields_ = [("scheme", ctypes.c_int), ("coriolis_param", ctypes.c_double), ("u0", ctypes.c_double),
                 ("v0", ctypes.c_double), ("ug", _vp), ("vg", _vp), ("dtdt", _vp), ("dqtdt", _vp),
@@ -117,6 +121,7 @@ SIGNATURES = {
     "pb_stat_workspace_bytes": (_LL, [_DIMS]),
     "pb_horizontal_stat": (_I, [_DIMS, _I, _P, _P, _P, _P, _P, _P, _LL, _P]),
     "pb_forcing_update": (_I, [_DIMS, ctypes.POINTER(PbForcing)] + [_P] * 14),
+    "pb_dycoms_radiation": (_I, [_DIMS, ctypes.POINTER(PbDycomsRadiation)] + [_P] * 9),
     "pb_get_error": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "pb_clear_error": (_I, [_P]),
     "pb_status_string": (ctypes.c_char_p, [_I]),

@@ -54,7 +54,8 @@ def nvcc() -> str:
 # and csrc/advection_f64.cu).
 UNITS = [("pb_all.cu", []), ("thermo.cu", ["-fmad=false"]), ("advection_f64.cu", ["-fmad=false"]),
          ("thermo_fast.cu", []), ("surface.cu", ["-fmad=false"]), ("sgs.cu", ["-fmad=false"]),
-         ("stats.cu", ["-fmad=false"]), ("forcing.cu", ["-fmad=false"])]
+         ("stats.cu", ["-fmad=false"]), ("forcing.cu", ["-fmad=false"]),
+         ("radiation.cu", ["-fmad=false"])]
 
 
 def _run(cmd):

@@ -19,6 +19,7 @@ from .grid import Grid
 from .pressure import PressureSolver
 from .reference_state import ReferenceState
 from .forcing import ForcingFactory
+from .radiation import RadiationFactory
 from .sgs import SGS, Kinematics, MomentumDiffusion, ScalarDiffusion
 from .surface import SurfaceFactory
 from .thermodynamics import ThermodynamicsDry, ThermodynamicsSA
@@ -67,6 +68,7 @@ class HotPathSimulation:
         self.RS = ReferenceState(Gr)
         self.Sur = SurfaceFactory(namelist)
         self.Fo = ForcingFactory(namelist)
+        self.Ra = RadiationFactory(namelist)
         # subgrid scale and diffusion when the namelist has an sgs section
         # (the measured configurations have none)
         self.SGS = SGS(namelist) if "sgs" in namelist else None
@@ -87,6 +89,7 @@ class HotPathSimulation:
         self.DV.initialize(Gr, device=self.device)
         self.Sur.initialize(Gr, self.RS)
         self._fo_ready = False
+        self.Ra.initialize(Gr)
         if self.SGS is not None:
             self.Ke.initialize(Gr)
             self.SGS.initialize(Gr, PV)
@@ -149,7 +152,7 @@ class HotPathSimulation:
         advection and the stage."""
         return (self.fuse_rk and self.MA.precision == _capi.PB_FP32
                 and self.Sur.scheme == _capi.PB_SURFACE_NONE and self.SGS is None
-                and self.Fo.scheme == _capi.PB_FORCING_NONE)
+                and self.Fo.scheme == _capi.PB_FORCING_NONE and not self.Ra.active)
 
     def _clear_w_tendency(self, stream=None):
         """Fused stepping: the w tendency is cleared once the fused pass has
@@ -213,6 +216,7 @@ class HotPathSimulation:
                     self.Fo.initialize(Gr, RS)
                     self._fo_ready = True
                 self.Fo.update(Gr, RS, PV, self.DV, stream=stream)
+            self.Ra.update(Gr, RS, PV, self.DV, self.Sur, self.TS, stream=stream)  # Ra.update (:174)
             m(3)
             TS.update(Gr, PV, stream=stream)
             return

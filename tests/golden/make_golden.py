@@ -143,6 +143,9 @@ def make_surface(name, scheme, cfg):
     s = oracle_sim(nl, rs, f0, backend="ref")
     s.surface = OracleSurface(scheme, d, u0=rs["u0"], v0=rs["v0"])
     s.forcing = OracleForcing(scheme, d, rs["p0_half"], Grid(nl).zl_half, u0=rs["u0"], v0=rs["v0"])
+    if scheme == "DYCOMS_RF01":  # RadiationFactory (Radiation.pyx:30-57)
+        from oracle.radiation import OracleRadiation
+        s.radiation = OracleRadiation(d, Grid(nl).z)
     s.update_all_bcs()
     s.step()
     for k in s.names:
@@ -262,6 +265,9 @@ def make_case(name, cfg, extra):
         s.forcing = OracleForcing(casename, d, rs["p0_half"], zl_half, u0=rs["u0"], v0=rs["v0"])
         if "sgs" in nl:
             s.sgs = OracleSGS(scheme_from_namelist(nl), d, zl_half)
+        if casename == "DYCOMS_RF01":  # RadiationFactory (Radiation.pyx:30-57)
+            from oracle.radiation import OracleRadiation
+            s.radiation = OracleRadiation(d, Grid(nl).z)
         return s
 
     out = {"rs_" + k: np.asarray(v) for k, v in rs.items()}
@@ -276,6 +282,12 @@ def make_case(name, cfg, extra):
     s.forcing.update(s)
     for k in s.names:
         out["fotend_" + k] = s.tend(k).copy()
+    if s.radiation is not None:
+        s.tendencies[:] = 0.0
+        s.radiation.update(s)
+        out["ratend_s"] = s.tend("s").copy()
+        out["ra_heating_rate"] = s.radiation.heating_rate.copy()
+        out["ra_dTdt_rad"] = s.radiation.dTdt_rad.copy()
     s = attach(oracle_sim(nl, rs, f0, backend="ref"))
     s.update_all_bcs()
     s.step()

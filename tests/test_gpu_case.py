@@ -1,9 +1,9 @@
 """Whole cases on the GPU against the fixtures generated from the
 reference's own C (tests/golden/make_golden.py): the case forcing
 (pb_forcing_update) after the thermodynamics, and one time step with the
-case's surface, forcing and subgrid scale in the stage (Bomex;
-DYCOMS_RF01 with Smagorinsky; SullivanPatton with the wall-adjusted
-Smagorinsky).  Tolerances (relative L2): forcing tendencies 1e-12 (plain
+case's surface, forcing, radiation and subgrid scale in the stage (Bomex;
+DYCOMS_RF01 with its radiation and Smagorinsky; SullivanPatton with the
+wall-adjusted Smagorinsky).  Tolerances (relative L2): forcing tendencies 1e-12 (plain
 form; the horizontal means of u and v are summed in another order) and 1e-9
 (precision form); one step 1e-12 (plain) and 1e-6 (precision)."""
 import os
@@ -70,3 +70,24 @@ def test_case_step_vs_reference_golden(name):
         print(name, precision, "step:", {k: f"{v:.1e}" for k, v in errs.items()})
         for k, v in errs.items():
             assert v < tol, (precision, k)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_dycoms_radiation_vs_reference_golden(precision):
+    """RadiationDyCOMS_RF01 (Radiation.pyx:230-353) after the thermodynamics:
+    heating rate, temperature tendency and entropy tendency (1e-12 plain,
+    1e-9 precision form)."""
+    z, nl, rs, f, _ = _load("case_dycoms_rf01")
+    g = gpu_sim(nl, rs, f, precision=precision)
+    assert g.Ra.active
+    g.PV.Update_all_bcs(g.Gr)
+    g.Th.update(g.Gr, g.RS, g.PV, g.DV)
+    g.PV.tendencies.zero_()
+    g.Ra.update(g.Gr, g.RS, g.PV, g.DV)
+    tol = 1e-12 if precision == "fp64" else 1e-9
+    errs = {"s_tend": rel_l2(gpu_tends(g)["s"], z["ratend_s"]),
+            "heating_rate": rel_l2(g.Ra.heating_rate.cpu().numpy(), z["ra_heating_rate"]),
+            "dTdt_rad": rel_l2(g.Ra.dTdt_rad.cpu().numpy(), z["ra_dTdt_rad"])}
+    print(precision, {k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        assert v < tol, k

@@ -248,6 +248,9 @@ def test_surface_golden_port(name):
     s = oracle_sim(nl, rs, f0, "port")
     s.surface = OracleSurface(scheme, d, u0=float(rs["u0"]), v0=float(rs["v0"]))
     s.forcing = OracleForcing(scheme, d, rs["p0_half"], Grid(nl).zl_half, u0=float(rs["u0"]), v0=float(rs["v0"]))
+    if scheme == "DYCOMS_RF01":
+        from oracle.radiation import OracleRadiation
+        s.radiation = OracleRadiation(d, Grid(nl).z)
     s.update_all_bcs()
     s.step()
     for k in s.names:
@@ -388,6 +391,9 @@ def test_case_golden_port(name):
         s.forcing = OracleForcing(casename, d, rs["p0_half"], zl, u0=float(rs["u0"]), v0=float(rs["v0"]))
         if "sgs" in nl:
             s.sgs = OracleSGS(scheme_from_namelist(nl), d, zl)
+        if casename == "DYCOMS_RF01":
+            from oracle.radiation import OracleRadiation
+            s.radiation = OracleRadiation(d, Grid(nl).z)
         return s
 
     s = attach(oracle_sim(nl, rs, f, "port"))
@@ -397,6 +403,11 @@ def test_case_golden_port(name):
     s.forcing.update(s)
     for k in s.names:
         assert np.array_equal(s.tend(k), z["fotend_" + k]), k
+    if s.radiation is not None:
+        s.tendencies[:] = 0.0
+        s.radiation.update(s)
+        assert np.array_equal(s.tend("s"), z["ratend_s"])
+        assert np.array_equal(s.radiation.heating_rate, z["ra_heating_rate"])
     s = attach(oracle_sim(nl, rs, f0, "port"))
     s.update_all_bcs()
     s.step()
