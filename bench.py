@@ -465,8 +465,28 @@ def _time_forcing(sim, cfg, peak, calls=10, warm=2):
     ms = a.elapsed_time(b) / calls
     nbytes = {"SullivanPatton": 48.0, "Bomex": 112.0, "DYCOMS_RF01": 96.0}[scheme]
     ach = nbytes * sim.Gr.dims.npl / (ms / 1e3) / 1e9
-    return {"scheme": scheme, "ms_per_call": round(ms, 4), "algorithmic_bytes_per_cell": nbytes,
-            "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
+    out = {"scheme": scheme, "ms_per_call": round(ms, 4), "algorithmic_bytes_per_cell": nbytes,
+           "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
+    if scheme == "DYCOMS_RF01":
+        # its radiation (Radiation.pyx:230-353): read ql, qt (twice), T; read
+        # and write the s tendency; write the heating rate and dT/dt: 64 B
+        from pycles_b200.radiation import RadiationFactory
+        ra = RadiationFactory({"meta": {"casename": scheme}})
+        ra.initialize(sim.Gr)
+        for _ in range(warm):
+            ra.update(*args)
+        a.record(stream)
+        for _ in range(calls):
+            ra.update(*args)
+        b.record(stream)
+        torch.cuda.synchronize()
+        sim.PV.tendencies.copy_(tend)
+        ms = a.elapsed_time(b) / calls
+        ach = 64.0 * sim.Gr.dims.npl / (ms / 1e3) / 1e9
+        out["radiation"] = {"ms_per_call": round(ms, 4), "algorithmic_bytes_per_cell": 64.0,
+                            "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
+        del ra
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
