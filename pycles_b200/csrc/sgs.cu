@@ -171,7 +171,7 @@ __device__ __forceinline__ double sflux(const SArgs& a, const double* phi, doubl
 // (scalar_flux_divergence, Csrc/flux_divergence.h:4-32) and, for qt, the
 // entropy source (compute_qt_diffusion_s_source,
 // Csrc/scalar_diffusion.h:70-113).
-__global__ void __launch_bounds__(kThreads) scalar_diffusion(SArgs a) {
+__global__ void __launch_bounds__(kThreads, 8) scalar_diffusion(SArgs a) {
   const G& g = a.g;
   const int k = g.gw + blockIdx.x * kThreads + threadIdx.x;
   const int j = g.gw + blockIdx.y, i = g.gw + blockIdx.z;

@@ -34,7 +34,7 @@ constexpr double vkb = 0.35;
 constexpr double beta_m = 4.7;
 constexpr double gamma_m = 15.0;
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;  // one column per thread at 512 x 512 (latency-bound plane work)
 constexpr int kMaxBlocks = PB_SURFACE_SCRATCH;
 
 __device__ __forceinline__ double interp_2(double a, double b) { return 0.5 * (a + b); }
