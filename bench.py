@@ -563,6 +563,12 @@ def run_ours(args, rank, world, local_rank):
         stream = torch.cuda.current_stream(dev)
         host = torch.empty(PV.values.numel(), dtype=torch.float64, pin_memory=True)
         host.copy_(PV.values)
+        # untimed warm-up through the same host-memory path (first touch of
+        # the pinned buffer, copy-stream set-up), as for the device timing
+        for _ in range(args.warmup):
+            sim.step_host(host, stream=stream)
+        for cs in sim.copy_streams():
+            stream.wait_stream(cs)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
