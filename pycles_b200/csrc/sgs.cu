@@ -166,6 +166,16 @@ __device__ __forceinline__ double sflux(const SArgs& a, const double* phi, doubl
          a.dxi_div[d];
 }
 
+// The same flux without the range tests, for a face inside [gw-1, nlg-gw)
+// and off the level gw-1.
+__device__ __forceinline__ double sflux_in(const SArgs& a, const double* phi, double factor, int d, long long p,
+                                           int pk) {
+  const long long s = stride_of(a.g, d);
+  const double rho = d == 2 ? a.rho0[pk] : a.rho0_half[pk];
+  return -factor * (0.5 * (__ldg(a.D + p) + __ldg(a.D + p + s))) * (__ldg(phi + p + s) - __ldg(phi + p)) * rho *
+         a.dxi_div[d];
+}
+
 // ScalarDiffusion.update (ScalarDiffusion.pyx:112-150) for one interior
 // cell: per scalar in order, per direction, the flux divergence
 // (scalar_flux_divergence, Csrc/flux_divergence.h:4-32) and, for qt, the
@@ -195,10 +205,10 @@ __global__ void __launch_bounds__(kThreads, 8) scalar_diffusion(SArgs a) {
     }
     for (int d = 0; d < 3; ++d) {
       const long long s = stride_of(g, d);
-      int lo[3] = {i, j, k};
-      lo[d] -= 1;
-      const double fh = sflux(a, phi, a.factor[n], d, ijk, i, j, k);
-      const double fl = sflux(a, phi, a.factor[n], d, ijk - s, lo[0], lo[1], lo[2]);
+      // an interior cell's own face and the face below it lie inside the
+      // flux range; only the face below the first level (k = gw) is 0
+      const double fh = sflux_in(a, phi, a.factor[n], d, ijk, k);
+      const double fl = (d == 2 && k == g.gw) ? 0.0 : sflux_in(a, phi, a.factor[n], d, ijk - s, d == 2 ? k - 1 : k);
       t -= a.alpha0_half[k] * (fh - fl) * g.dxi[d];
       if (src) {
         int hi[3] = {i, j, k};
