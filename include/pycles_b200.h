@@ -359,12 +359,15 @@ int pb_pressure_solve(const pb_dims* dims, const double* rho0, const double* rho
  *           library holds the 64 MiB until the process exits.
  *   Set-up: the first call on a device, and the first call after the grid
  *           changes, takes the array's device address (cudaGetSymbolAddress)
- *           and fills the grid constants synchronously -- make that first
- *           call before any stream capture.
+ *           and fills the grid constants synchronously; a grid change first
+ *           waits for the whole device, so solves of the previous grid still
+ *           queued on any stream finish with their own constants -- make
+ *           that first call before any stream capture.
  *   Races : all calls on a device share the array (it keeps the last call's
  *           contents; nothing needs clearing, every word read is written
  *           first in the same call), so calls that may overlap on the GPU
- *           must be ordered by the caller.
+ *           must be ordered by the caller.  Host threads are serialised by a
+ *           lock held from the set-up until the call's kernels are enqueued.
  */
 #define PB_PRESSURE_NOALLOC_MAX_BYTES (64ll << 20)
 int pb_pressure_solve_noalloc(const pb_dims* dims, const double* rho0, const double* rho0_half,

@@ -579,10 +579,18 @@ def update_third(values, tendencies, value_copy, rk_step, dt):
 # pressure, PressureSolver.pyx + PressureFFTParallel.pyx (one rank)
 # ---------------------------------------------------------------------------
 def horizontal_mean(d: Dims, values):
-    """ParallelMPI.HorizontalMean (ParallelMPI.pyx:196-241), one rank."""
+    """ParallelMPI.HorizontalMean (ParallelMPI.pyx:196-241), one rank: every
+    level's sum is accumulated in the reference's order, i outer, j inner,
+    one rounded addition per column (:219-226), then scaled by
+    1/(n0 n1) (:232-236).  The order matters: w's horizontal mean is a
+    cancelling sum, and the pressure solve subtracts it from every cell."""
     V = values.reshape(d.shape)
     g_ = d.gw
-    s = V[g_:d.shape[0] - g_, g_:d.shape[1] - g_, :].sum(axis=(0, 1))
+    s = np.zeros(d.shape[2])
+    for i in range(g_, d.shape[0] - g_):
+        Vi = V[i]
+        for j in range(g_, d.shape[1] - g_):
+            s += Vi[j]
     return s * (1.0 / float(d.n[1] * d.n[0]))
 
 

@@ -371,6 +371,65 @@ __global__ void hmean_final(Geo g, const double* __restrict__ partial, double* _
   if (threadIdx.x == 0) mean[k] = red[0] * n_horizontal_i;
 }
 
+// Plain form: HorizontalMean in the reference's order (ParallelMPI.pyx:219-
+// 226).  Each level's sum is one chain of rounded additions over the
+// interior columns, i outer and j inner, which no reordering may change:
+// w's horizontal mean cancels, and the solve subtracts it from every cell.
+// A block owns 32 levels, one lane each.  Warp 0 only adds: it walks a tile
+// of kSerialTile columns in shared memory, one dependent addition per column,
+// while the other 31 warps load the next tile (kSerialPer columns each, all
+// loads in flight at once) into the other half of a double buffer.
+constexpr int kSerialWarps = 32;
+constexpr int kSerialPer = 12;
+constexpr int kSerialTile = (kSerialWarps - 1) * kSerialPer;  // columns per tile
+constexpr int kSerialLd = 33;  // doubles per column in the tile (odd: no bank conflicts)
+__global__ void __launch_bounds__(kSerialWarps * 32, 1) hmean_serial(Geo g, const double* __restrict__ w,
+                                                                     double* __restrict__ mean,
+                                                                     double n_horizontal_i) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* tile = reinterpret_cast<double*>(smraw);  // [2][kSerialTile][kSerialLd]
+  const int nl1 = (int)(g.n1 - 2 * g.gw);
+  const int ncol = (int)(g.n0 - 2 * g.gw) * nl1;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long k = (long long)blockIdx.x * 32 + lane;
+  const bool kok = k < g.n2;
+  const int ntiles = (ncol + kSerialTile - 1) / kSerialTile;
+  auto produce = [&](int t) {
+    double v[kSerialPer];
+#pragma unroll
+    for (int q = 0; q < kSerialPer; ++q) {
+      const int col = t * kSerialTile + (wid - 1) * kSerialPer + q;
+      v[q] = 0.0;
+      if (col < ncol && kok) {
+        const int i = col / nl1, j = col - (col / nl1) * nl1;
+        v[q] = w[(g.gw + i) * g.is + (g.gw + j) * g.js + k];
+      }
+    }
+    double* dst = tile + (t & 1) * kSerialTile * kSerialLd + (wid - 1) * kSerialPer * kSerialLd + lane;
+#pragma unroll
+    for (int q = 0; q < kSerialPer; ++q) dst[q * kSerialLd] = v[q];
+  };
+  double s = 0.0;
+  if (wid > 0) produce(0);
+  __syncthreads();
+  for (int t = 0; t < ntiles; ++t) {
+    if (wid > 0) {
+      if (t + 1 < ntiles) produce(t + 1);
+    } else {
+      const double* cur = tile + (t & 1) * kSerialTile * kSerialLd + lane;
+      const int nc = min(kSerialTile, ncol - t * kSerialTile);
+      if (nc == kSerialTile) {
+#pragma unroll 12
+        for (int c = 0; c < kSerialTile; ++c) s = add_rn(s, cur[c * kSerialLd]);
+      } else {
+        for (int c = 0; c < nc; ++c) s = add_rn(s, cur[c * kSerialLd]);
+      }
+    }
+    __syncthreads();
+  }
+  if (wid == 0 && kok) mean[k] = mul_rn(s, n_horizontal_i);
+}
+
 __global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nghost; t += stride) {
@@ -979,11 +1038,18 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
   const long long Nx = dims->n[0], Ny = dims->n[1], nz = dims->n[2];
   const long long nghost = g.npg - Nx * Ny * nz;
 
-  const int kpad = (int)((g.n2 + 31) / 32 * 32);
-  hmean_partial<<<kPartials, kpad < 1024 ? kpad : 1024, 0, st>>>(g, w, a.partial);
-  pb_note_launch();
-  hmean_final<<<(unsigned)g.n2, 256, 0, st>>>(g, a.partial, a.mean, kPartials, 1.0 / (double)(Ny * Nx));
-  pb_note_launch();
+  if (precision == PB_FP64) {  // the reference's summation order
+    const size_t sm = 2 * (size_t)kSerialTile * kSerialLd * sizeof(double);
+    PB_CUDA_TRY(cudaFuncSetAttribute(hmean_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    hmean_serial<<<ceil_div(g.n2, 32), kSerialWarps * 32, sm, st>>>(g, w, a.mean, 1.0 / (double)(Ny * Nx));
+    pb_note_launch();
+  } else {  // precision form: a deterministic parallel sum
+    const int kpad = (int)((g.n2 + 31) / 32 * 32);
+    hmean_partial<<<kPartials, kpad < 1024 ? kpad : 1024, 0, st>>>(g, w, a.partial);
+    pb_note_launch();
+    hmean_final<<<(unsigned)g.n2, 256, 0, st>>>(g, a.partial, a.mean, kPartials, 1.0 / (double)(Ny * Nx));
+    pb_note_launch();
+  }
   if (nghost > 0) {
     zero_ghosts<<<stream_blocks(nghost), 256, 0, st>>>(g, divergence, nghost);
     pb_note_launch();

@@ -16,11 +16,17 @@
 //   call on each device (with that device current) takes the address with
 //   cudaGetSymbolAddress and fills the grid constants (wave numbers,
 //   twiddles).  That set-up is synchronous; it runs again when the grid
-//   changes.  Make the first call for a grid before any stream capture.
+//   changes, and then it first waits for the whole device
+//   (cudaDeviceSynchronize), so that a solve of the previous grid still
+//   queued on any stream finishes with the constants it was launched with.
+//   Make the first call for a grid before any stream capture.
 // * All calls on a device share the one array and it keeps the last call's
 //   contents.  Every scratch word the solve reads is written earlier in the
 //   same call, so nothing needs clearing; but calls that overlap on the GPU
 //   (different streams, no ordering between them) race on the array.
+// * Host threads are serialised: a call holds a lock from its set-up until
+//   its kernels are enqueued, so no other thread's re-initialisation can
+//   change the constants in between.
 #include <mutex>
 
 #include "pb_common.cuh"
@@ -62,23 +68,25 @@ extern "C" int pb_pressure_solve_noalloc(const pb_dims* dims, const double* rho0
   int dev = 0;
   PB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return PB_ERR_UNSUPPORTED;
-  void* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    NoallocSlot& slot = g_noalloc[dev];
-    if (slot.addr == nullptr) {
-      void* p = nullptr;
-      PB_CUDA_TRY(cudaGetSymbolAddress(&p, pb_pressure_scratch));
-      slot.addr = p;
-    }
-    if (!slot.have_dims || !same_dims(slot.dims, *dims)) {
-      rc = pb_pressure_init(dims, slot.addr, PB_PRESSURE_NOALLOC_MAX_BYTES);
-      if (rc) return rc;
-      slot.dims = *dims;
-      slot.have_dims = true;
-    }
-    base = slot.addr;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  NoallocSlot& slot = g_noalloc[dev];
+  if (slot.addr == nullptr) {
+    void* p = nullptr;
+    PB_CUDA_TRY(cudaGetSymbolAddress(&p, pb_pressure_scratch));
+    slot.addr = p;
+  }
+  if (!slot.have_dims || !same_dims(slot.dims, *dims)) {
+    // the constants are rewritten by synchronous copies on the legacy
+    // stream, which do not wait for non-blocking streams: drain the device
+    // first so that no queued solve of the previous grid reads new values
+    slot.have_dims = false;
+    PB_CUDA_TRY(cudaDeviceSynchronize());
+    rc = pb_pressure_init(dims, slot.addr, PB_PRESSURE_NOALLOC_MAX_BYTES);
+    if (rc) return rc;
+    PB_CUDA_TRY(cudaDeviceSynchronize());
+    slot.dims = *dims;
+    slot.have_dims = true;
   }
   return pressure_solve_impl(dims, rho0, rho0_half, alpha0, alpha0_half, u, v, w, divergence, dynamic_pressure,
-                             static_cast<char*>(base), PB_FP64, 0, as_stream(stream));
+                             static_cast<char*>(slot.addr), PB_FP64, 0, as_stream(stream));
 }

@@ -172,3 +172,48 @@ def sample_inputs(states, n, rng_seed=0, jitter=(200.0, 3.0, 5e-4), device="cuda
         v = a[idx] + j * (2.0 * torch.rand(n, device=device, generator=g, dtype=torch.float64) - 1.0)
         out.append(v.clamp(lo, hi))
     return out
+
+
+def cell_inputs(sim):
+    """(p0 per cell, s, qt) of a simulation's current state: the network's
+    inputs for every ghosted cell (CUDA float64 tensors, views where they can
+    be)."""
+    Gr = sim.Gr
+    n2 = int(Gr.dims.nlg[2])
+    p0 = sim.RS.d_p0_half.repeat(int(Gr.npg) // n2)
+    return p0, sim.PV.field("s", Gr), sim.PV.field("qt", Gr)
+
+
+def train_seed(thermo, states, n_samples=6_000_000, held_out_states=None, n_held_out=1_000_000, epochs=12,
+               batch=16384, seed=0, device="cuda"):
+    """Trains a SeedMLP on (p0, s, qt) -> T pairs from the plain FP64 secant
+    (pb_eos_sa) drawn, with a small seeded jitter, from simulation states
+    (a list of (p0, s, qt) flat tensors, e.g. ``cell_inputs`` of runs saved
+    along the way); only the saturated samples become pairs.  Evaluated on
+    pairs drawn from ``held_out_states`` (default: the training states with
+    another seed).  Returns (mlp, info) or (None, info) when the states hold
+    too few saturated cells."""
+    P, S, Q = sample_inputs(states, n_samples, rng_seed=1 + seed, device=device)
+    P, S, Q, T, T1, _ = training_pairs(thermo, P, S, Q)
+    info = {"training_pairs": int(P.numel()), "epochs": epochs}
+    if P.numel() < 1000:
+        return None, info
+    r = T - T1
+    mlp = SeedMLP(device=device, seed=seed, out_mean=float(r.mean()), out_scale=2.0 * float(r.std()))
+    torch.cuda.synchronize()
+    import time
+    t0 = time.time()
+    hist = mlp.train(P, S, Q, T, T1, epochs=epochs, batch=batch, seed=seed)
+    torch.cuda.synchronize()
+    info["train_seconds"] = round(time.time() - t0, 2)
+    info["final_batch_loss"] = hist[-1]
+    Ph, Sh, Qh = sample_inputs(held_out_states or states, n_held_out, rng_seed=1000 + seed, device=device)
+    Ph, Sh, Qh, Th, _, its_h = training_pairs(thermo, Ph, Sh, Qh)
+    if Ph.numel():
+        guess = mlp.forward(Ph, Sh, Qh)
+        _, it_seed = secant_iterations(thermo, Ph, Sh, Qh, seed=guess)
+        info.update({"held_out_pairs": int(Ph.numel()),
+                     "seed_mean_abs_error_K": float((guess - Th).abs().mean()),
+                     "pointwise_mean_iterations_plain": float(its_h.double().mean()),
+                     "pointwise_mean_iterations_seeded": float(it_seed.double().mean())})
+    return mlp, info

@@ -72,6 +72,44 @@ def test_noalloc_matches_workspace_entry_point_twice():
             assert rel_l2(out[n], ref[n]) <= 1e-12, (call, n)
 
 
+def test_noalloc_alternating_grids_on_a_non_blocking_stream():
+    """Two grids in turn on one non-blocking stream with no host sync between
+    the calls: each grid change rewrites the shared constants, which must not
+    reach a solve of the other grid still queued on the stream."""
+    import torch
+
+    from pycles_b200 import _capi
+    L = _capi.load()
+    fn = L.pb_pressure_solve_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p] * 11
+    grids = [_inputs(32, 24, 20, seed=7), _inputs(64, 32, 16, seed=8)]
+    refs = []
+    for Gr, RS, vel in grids:
+        rc, ref = _solve(Gr, RS, vel, noalloc=False)
+        _capi.check(rc, "pb_pressure_solve")
+        refs.append(ref)
+    st = torch.cuda.Stream()
+    assert st.cuda_stream != 0
+    outs = []
+    with torch.cuda.stream(st):
+        for rnd in range(3):
+            for Gr, RS, vel in grids:
+                u, v, w = (x.clone() for x in vel)
+                div = torch.zeros(Gr.npg, dtype=torch.float64, device="cuda")
+                p = torch.zeros(Gr.npg, dtype=torch.float64, device="cuda")
+                rc = fn(ctypes.byref(Gr.dims), RS.d_rho0.data_ptr(), RS.d_rho0_half.data_ptr(),
+                        RS.d_alpha0.data_ptr(), RS.d_alpha0_half.data_ptr(), u.data_ptr(), v.data_ptr(),
+                        w.data_ptr(), div.data_ptr(), p.data_ptr(), st.cuda_stream)
+                _capi.check(rc, "pb_pressure_solve_noalloc")
+                outs.append((u, v, w, div, p))
+    st.synchronize()
+    for idx, tensors in enumerate(outs):
+        ref = refs[idx % 2]
+        for n, t in zip(("u", "v", "w", "div", "p"), tensors):
+            assert rel_l2(t.cpu().numpy(), ref[n]) <= 1e-12, (idx, n)
+
+
 def test_noalloc_rejects_grids_beyond_its_array():
     from pycles_b200 import _capi
     from pycles_b200.grid import Grid
