@@ -1,9 +1,39 @@
 // Advection entry points and the FP32 precision-form instantiations of the
 // kernels in advection_kernels.cuh (the FP64 plain form is instantiated in
 // advection_f64.cu, compiled without FMA contraction).
+#include <cudaTypedefs.h>
+
 #include "advection_kernels.cuh"
+#include "momentum_tma.cuh"
+
+int pb_make_plane_map(CUtensorMap* map, const double* field, const Geo& g, int box_k, int box_j) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return 1;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)g.n2, (cuuint64_t)g.n1, (cuuint64_t)g.n0};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.n2 * 8, (cuuint64_t)(g.n1 * g.n2) * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box_j, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(field), dims, strides, box,
+                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : 1;
+}
 
 namespace pbadv {
+
+// The precision form's momentum pass: the TMA plane ring where the fields
+// allow it (even nlg2, 16-byte aligned arrays), else the register-prefetch
+// plane kernel.
+static bool use_tma(const Geo& g, const MomArgs& a) {
+  return pb_tma_plane_ok(g, a.vel[0]) && pb_tma_plane_ok(g, a.vel[1]) && pb_tma_plane_ok(g, a.vel[2]);
+}
 
 cudaError_t scalar_fp32(int order, int ns, const Geo& g, ScalarArgs base, double* const* flux_dir[3],
                         const double* const vel[3], cudaStream_t st) {
@@ -12,10 +42,14 @@ cudaError_t scalar_fp32(int order, int ns, const Geo& g, ScalarArgs base, double
 }
 
 cudaError_t momentum_fp32(int order, const Geo& g, const MomArgs& a, cudaStream_t st) {
+  if (use_tma(g, a))
+    return order == 5 ? launch_momentum_tma<5, false>(g, a, st) : launch_momentum_tma<7, false>(g, a, st);
   return order == 5 ? launch_momentum<5, true>(g, a, st) : launch_momentum<7, true>(g, a, st);
 }
 
 cudaError_t momentum_rk3_fp32(int order, const Geo& g, const MomArgs& a, cudaStream_t st) {
+  if (use_tma(g, a))
+    return order == 5 ? launch_momentum_tma<5, true>(g, a, st) : launch_momentum_tma<7, true>(g, a, st);
   return order == 5 ? launch_momentum_rk3<5>(g, a, st) : launch_momentum_rk3<7>(g, a, st);
 }
 
@@ -142,6 +176,7 @@ extern "C" int pb_momentum_advection(const pb_dims* dims, const double* rho0, co
   a.rho0_half = rho0_half;
   a.alpha0 = alpha0;
   a.alpha0_half = alpha0_half;
+  a.err = pb_error_word_ptr();
   cudaStream_t st = as_stream(stream);
   cudaError_t e;
   e = precision == PB_FP64 ? pbadv::momentum_fp64(order, g, a, st) : pbadv::momentum_fp32(order, g, a, st);
@@ -178,6 +213,7 @@ extern "C" int pb_momentum_advection_rk3(const pb_dims* dims, const double* rho0
   a.copy[0] = u_copy;
   a.copy[1] = v_copy;
   a.copy[2] = w_copy;
+  a.err = pb_error_word_ptr();
   a.dt = dt;
   a.stage = rk_step;
   const cudaError_t e = pbadv::momentum_rk3_fp32(order, g, a, as_stream(stream));

@@ -58,6 +58,7 @@ struct MomArgs {
   double* copy[3];
   double dt;
   int stage;
+  unsigned int* err;           // device error word (bounded waits of the TMA plane ring)
 };
 
 template <int ORDER>

@@ -32,9 +32,12 @@ def _stir(f, seed=1, amp=0.3):
 # tiles of the one-pass kernels cut mid-domain: 33 rows (15 + 15 + 3), 40
 # levels (31 + 9), an odd x extent
 MOIST_TILES = dict(MOIST, nx=19, ny=33, nz=40)
+# an odd number of ghosted levels (39 + 8): the fields' rows are not 16-byte
+# multiples, so the momentum pass takes the kernel without TMA plane copies
+MOIST_ODD_LEVELS = dict(MOIST, nx=19, ny=33, nz=39)
 
 
-@pytest.mark.parametrize("cfg", [MOIST, MOIST_TILES], ids=["small", "tiles"])
+@pytest.mark.parametrize("cfg", [MOIST, MOIST_TILES, MOIST_ODD_LEVELS], ids=["small", "tiles", "odd_levels"])
 def test_fp32_advection_tendencies(cfg):
     nl, rs, f = host_case(**cfg)
     f = _stir(f)
