@@ -180,7 +180,20 @@ def _cpu_worker(args):
         t0 = time.perf_counter()
         sim.step()
         times.append(time.perf_counter() - t0)
-    return nx * ny * nz, times
+    # what this process actually ran: the compiled reference library mapped
+    # into it, and the reference's cythonized TDMA for the pressure columns
+    mapped = []
+    try:
+        with open("/proc/self/maps") as fh:
+            mapped = sorted({ln.split()[-1] for ln in fh if "oracle/_ref/" in ln and ln.rstrip().endswith(".so")})
+    except OSError:
+        pass
+    tdma = None
+    if backend == "ref":
+        from oracle import ref as oref
+        tdma = oref.tdma_module() is not None
+    return nx * ny * nz, times, {"backend": backend, "ref_libraries_mapped": [os.path.basename(m) for m in mapped],
+                                 "reference_tdma": tdma}
 
 
 def cpu_reference_run(cfg, nsteps, nwarm, backend="ref", cores=None):
@@ -197,17 +210,24 @@ def cpu_reference_run(cfg, nsteps, nwarm, backend="ref", cores=None):
         with ctx.Pool(cores) as pool:
             res = pool.map(_cpu_worker, [(cfg, nsteps + nwarm, backend, barrier)] * cores)
     cells = res[0][0]
+    ran = [r[2] for r in res]
     per_step = []
     for s in range(nwarm, nwarm + nsteps):
         wall = max(r[1][s] for r in res)
         per_step.append(cores * cells * 3 / wall)
     nx, ny, nz = _cpu_sample_shape(cfg)
-    kind = "reference" if backend == "ref" else "port"
+    # the label follows what every worker reports it ran, not this process's check
+    all_ref = all(r["backend"] == "ref" and "libpycles_ref.so" in r["ref_libraries_mapped"] for r in ran)
+    kind = "reference" if all_ref else "port"
     sample = (f"{cores} concurrent processes, each one time step of a {nx}x{ny}x{nz} sub-domain "
               f"(gw={cfg['gw']}, WENO{cfg.get('scalar_order', 5)}/{cfg.get('momentum_order', 5)}) of the same case; "
               f"{'reference C kernels compiled from source + restated glue' if kind == 'reference' else 'numpy port'}"
               "; no halo exchange or pencil transposes between processes (MPI-free upper bound)")
-    return per_step, {"kind": kind, "cores": cores, "sample": sample}
+    workers = {"backend": sorted({r["backend"] for r in ran}),
+               "ref_libraries_mapped": sorted({m for r in ran for m in r["ref_libraries_mapped"]}),
+               "workers_with_reference_library": sum("libpycles_ref.so" in r["ref_libraries_mapped"] for r in ran),
+               "workers_with_reference_tdma": sum(bool(r["reference_tdma"]) for r in ran)}
+    return per_step, {"kind": kind, "cores": cores, "sample": sample, "workers": workers}
 
 
 # ---------------------------------------------------------------------------
@@ -275,41 +295,94 @@ def _time_steps(sim, steps, local_rank, world):
     return elapsed_ms, comp_ms, launches, clock_info, secant
 
 
+# Training distribution of the learned seed: states of the moist BOMEX-like
+# configurations (64x64x75 and 256x256x128, FP64 plain form, saved at the
+# listed steps), each sampled cell jittered uniformly by these half-widths in
+# (p0 [Pa], s [J/kg/K], qt [kg/kg]).  Those states hold no saturated cell
+# (no surface fluxes build a cloud layer), so the spread is what reaches the
+# saturated part of the network's input box; it also covers the
+# stratocumulus (DYCOMS-like) states the network is then used on.
+SEED_TRAIN_STATES = (("c2_bomex", (0, 20, 40)), ("c3_bomex", (0, 5)))
+SEED_JITTER = (1500.0, 45.0, 5.0e-3)
+SEED_PAIRS = 10_000_000
+
+
 def _train_seed(sim, fields, log):
-    """Learned seed for the secant: pairs from the plain FP64 secant on the
-    saturated (p0, s, qt) of this state with a seeded jitter, trained with
-    the library's own tensor-core kernels (outside the timed region), and
-    evaluated on a held-out sample."""
+    """Learned seed for the secant (outside the timed region): 10^7 pairs
+    from the plain FP64 secant on inputs drawn around states of the moist
+    64x64x75 and 256x256x128 configurations, trained with the library's own
+    tensor-core kernels, and evaluated on held-out pairs from the benchmark's
+    own state (never trained on)."""
     import torch
 
     from pycles_b200 import learned
+    from pycles_b200.simulation import CONFIGS, HotPathSimulation, namelist_for
+    states = []
+    for name, steps in SEED_TRAIN_STATES:
+        src = HotPathSimulation(namelist_for(**CONFIGS[name], precision="fp64"), device=sim.device)
+        src.initialize(seed=1)
+        src.run(0)
+        done = 0
+        for s in steps:
+            for _ in range(s - done):
+                src.step()
+            done = s
+            states.append(tuple(t.clone() for t in learned.cell_inputs(src)))
+        del src
+    torch.cuda.empty_cache()
     Gr = sim.Gr
     n2 = Gr.dims.nlg[2]
-    s = torch.as_tensor(fields["s"], device=sim.device)
-    qt = torch.as_tensor(fields["qt"], device=sim.device)
-    p0 = sim.RS.d_p0_half.repeat(Gr.npg // n2)
-    P, S, Q = learned.sample_inputs([(p0, s, qt)], 6_000_000, rng_seed=1, device=sim.device)
-    P, S, Q, T, T1, its = learned.training_pairs(sim.Th, P, S, Q)
-    if P.numel() < 1000:
-        return None
-    r = T - T1
-    mlp = learned.SeedMLP(device=sim.device, seed=0, out_mean=float(r.mean()), out_scale=2.0 * float(r.std()))
-    torch.cuda.synchronize()
-    t0 = time.time()
-    hist = mlp.train(P, S, Q, T, T1, epochs=12, batch=16384)
-    torch.cuda.synchronize()
-    train_s = time.time() - t0
-    Ph, Sh, Qh = learned.sample_inputs([(p0, s, qt)], 1_000_000, rng_seed=2, device=sim.device)
-    Ph, Sh, Qh, Th, _, its_h = learned.training_pairs(sim.Th, Ph, Sh, Qh)
-    seed = mlp.forward(Ph, Sh, Qh)
-    _, it_seed = learned.secant_iterations(sim.Th, Ph, Sh, Qh, seed=seed)
-    info = {"training_pairs": int(P.numel()), "epochs": 12, "train_seconds": round(train_s, 2),
-            "final_batch_loss": hist[-1], "held_out_pairs": int(Ph.numel()),
-            "seed_mean_abs_error_K": float((seed - Th).abs().mean()),
-            "pointwise_mean_iterations_plain": float(its_h.double().mean()),
-            "pointwise_mean_iterations_seeded": float(it_seed.double().mean())}
+    held = [(sim.RS.d_p0_half.repeat(Gr.npg // n2), torch.as_tensor(fields["s"], device=sim.device),
+             torch.as_tensor(fields["qt"], device=sim.device))]
+    mlp, info = learned.train_seed(sim.Th, states, n_pairs=SEED_PAIRS, jitter=SEED_JITTER, held_out_states=held,
+                                   n_held_out=1_000_000, device=sim.device)
+    info["trained_on"] = (f"inputs drawn around {len(states)} FP64 states of "
+                          + ", ".join(f"{n} (steps {list(st)})" for n, st in SEED_TRAIN_STATES)
+                          + f", uniform jitter +-{SEED_JITTER} in (p0, s, qt)")
+    info["held_out_on"] = "the benchmark's own initial state (cells as they are, no jitter)"
+    del states
+    torch.cuda.empty_cache()
     log(f"learned seed: {info}")
+    if mlp is None:
+        return None
     return mlp, info
+
+
+def _learned_at_c4(trained, dev, args, log):
+    """The learned seed at 256x256x128 (cloud-topped state, the c4_dycoms
+    configuration): precision form with and without the seed (the network
+    trained for the headline, never on this state), device time per step and
+    mean secant iterations per saturated cell over the timed steps."""
+    import torch
+
+    from pycles_b200.simulation import CONFIGS, HotPathSimulation, namelist_for
+    cfg = CONFIGS["c4_dycoms"]
+    out = {"workload": (f"c4_dycoms: {cfg['nx']}x{cfg['ny']}x{cfg['nz']} cells, dx={cfg['dx']} m, dz={cfg['dz']} m, "
+                        f"WENO5, dt={cfg['dt']}, seeded DYCOMS-RF01-like state")}
+    fields = rs = None
+    for form, seeded in (("fp32", False), ("fp32+learned", True)):
+        sim = HotPathSimulation(namelist_for(**cfg, precision="fp32"), device=dev)
+        if fields is None:
+            fields = sim.initialize(seed=0)
+            rs = sim.RS.profiles()
+        else:
+            sim.set_reference_state(rs)
+            sim.load_fields(fields)
+        if seeded:
+            sim.Th.mlp = trained[0]
+        sim.run(0)
+        for _ in range(args.warmup):
+            sim.step()
+        torch.cuda.synchronize()
+        elapsed_ms, comp_ms, _, _, secant = _time_steps(sim, max(args.steps, 12), 0, 1)
+        n = max(args.steps, 12)
+        out[form] = {"ms_per_step": round(elapsed_ms / n, 4), "thermo_ms_per_step": round(comp_ms["thermo"] / n, 4),
+                     "mean_secant_iterations_per_saturated_cell": secant["mean_iterations_per_saturated_cell"],
+                     "saturated_cells_per_stage": secant["saturated_cells_per_stage"]}
+        log(f"c4 {form}: {out[form]}")
+        del sim
+        torch.cuda.empty_cache()
+    return out
 
 
 # surface scheme of each configuration's case (Surface.pyx:39-74)
@@ -546,11 +619,30 @@ def run_ours(args, rank, world, local_rank):
             "pressure_refine_sweeps": sim.Pr.refine_sweeps if precision == "fp32" else None,
         }
         log(f"form {form}: {results[form]['ms_per_step']:.2f} ms/step")
+        if precision == "fp32" and sim._fused() and not args.no_unfused:
+            # the same form with every call launched as called (no advection
+            # deferred into the time step): what a caller that switches the
+            # fusion off, or adds tendency terms, gets
+            sim.fuse_rk = False
+            sim.step()
+            torch.cuda.synchronize()
+            un_ms, un_comp, _, _, _ = _time_steps(sim, args.steps, local_rank, world)
+            sim.fuse_rk = True
+            sim.step()
+            torch.cuda.synchronize()
+            results[form]["unfused_ms_per_step"] = un_ms / args.steps
+            results[form]["unfused_component_ms_per_step"] = {c: round(v / args.steps, 4) for c, v in un_comp.items()}
+            results[form]["stage_calls"] = ("the reference's call order per stage (Th, SA, MA, TS, bcs, Pr); "
+                                            "SA and MA deferred into TS.update, which runs the fused passes")
+            log(f"form {form} unfused: {results[form]['unfused_ms_per_step']:.2f} ms/step")
         if form == forms[-1][0]:
             headline_sim = sim
         else:
             del sim
             torch.cuda.empty_cache()
+    c4 = None
+    if trained is not None and args.config == "c5_dycoms" and not args.no_c4:
+        c4 = _learned_at_c4(trained, dev, args, log)
     head = forms[-1][0]
     sim = headline_sim
     PV, Gr = sim.PV, sim.Gr
@@ -648,6 +740,7 @@ def run_ours(args, rank, world, local_rank):
             "component_ms_per_step": r["component_ms_per_step"],
             "roofline": roofline,
             "e2e": e2e,
+            "learned_seed_c4": c4,
             "surface": surface,
             "sgs": sgs,
             "statistics": stats,
@@ -709,16 +802,15 @@ def run_accuracy(args, cfg):
         err[form] = {}
         for step in (1, n):
             a, b = snaps[form][step], snaps["fp64"][step]
-            e = {}
-            for name in b:
-                scale = np.linalg.norm(b[name])
-                if name in ("u", "v", "w"):  # components at rest: the velocity field's norm
-                    scale = np.sqrt(sum(np.linalg.norm(b[m]) ** 2 for m in ("u", "v", "w")))
-                e[name] = float(np.linalg.norm(a[name] - b[name]) / scale)
+            e = {name: float(np.linalg.norm(a[name] - b[name]) / np.linalg.norm(b[name])) for name in b}
+            vel = np.sqrt(sum(np.linalg.norm(b[m]) ** 2 for m in ("u", "v", "w")))
+            e["velocity_pooled"] = float(np.sqrt(sum(np.linalg.norm(a[m] - b[m]) ** 2 for m in ("u", "v", "w")))
+                                         / vel)
             err[form][f"after_{step}_steps"] = e
     return {"accuracy": err, "reference_form": "fp64 plain", "steps": n,
             "config": {"workload": f"{args.config}: {cfg['nx']}x{cfg['ny']}x{cfg['nz']} cells", **cfg},
-            "norm": "relative L2 per field; u, v, w relative to the norm of the whole velocity field"}
+            "norm": ("relative L2 per field, each field against its own norm; velocity_pooled: the difference "
+                     "of (u, v, w) against the norm of the whole velocity field")}
 
 
 def _read_traffic(config, form, component):
@@ -749,6 +841,10 @@ def main():
                     help="fp64: plain form; fp32: precision form without and with the learned seed; "
                          "all: every form, headline the last (fp32+learned)")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-unfused", action="store_true",
+                    help="skip timing the precision forms with every call launched as called")
+    ap.add_argument("--no-c4", action="store_true",
+                    help="skip the learned seed's measurement at 256x256x128 (c4_dycoms)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -34,6 +34,15 @@ class ScalarAdvection:
                                     device=PV.values.device)
 
     def update(self, Gr, Rs, PV, DV=None, Pa=None, stream=None):
+        """ScalarAdvection.update (ScalarAdvection.pyx:69-123).  Precision
+        form with fused stages: recorded on PV and run by TimeStepping.update
+        together with the SSP-RK3 stage (or when PV.tendencies is read)."""
+        if self.precision == _capi.PB_FP32 and self.flux is None and PV.fused_stepping_ok():
+            PV.defer_advection("scalar", self, Gr, Rs, DV, stream)
+            return
+        self.update_now(Gr, Rs, PV, DV, stream=stream)
+
+    def update_now(self, Gr, Rs, PV, DV=None, stream=None):
         scal = [PV.index_name[i] for i in range(PV.nv) if PV.var_type[i] == 1]
         if not scal:
             return
@@ -63,6 +72,15 @@ class MomentumAdvection:
         return
 
     def update(self, Gr, Rs, PV, Pa=None, stream=None):
+        """MomentumAdvection.update (MomentumAdvection.pyx:41-69).  Precision
+        form with fused stages: recorded on PV and run by TimeStepping.update
+        together with the SSP-RK3 stage (or when PV.tendencies is read)."""
+        if self.precision == _capi.PB_FP32 and PV.fused_stepping_ok():
+            PV.defer_advection("momentum", self, Gr, Rs, None, stream)
+            return
+        self.update_now(Gr, Rs, PV, stream=stream)
+
+    def update_now(self, Gr, Rs, PV, DV=None, stream=None):
         npg = Gr.dims.npg
         vs = [int(PV.velocity_directions[d]) * npg for d in range(3)]
         rc = _capi.load().pb_momentum_advection(

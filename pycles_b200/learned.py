@@ -143,7 +143,9 @@ def training_pairs(thermo, p0, s, qt, max_iter=100):
     _capi.check(_capi.load().pb_eos_sa(ctypes.byref(table), p0.data_ptr(), s.data_ptr(), qt.data_ptr(), None,
                                        T.data_ptr(), None, None, T1.data_ptr(), its.data_ptr(), p0.numel(),
                                        max_iter, _capi.stream_handle(None)), "pb_eos_sa")
-    keep = its > 0
+    # saturated points whose secant converged to a finite temperature within
+    # the cap (a draw can leave the saturation table's range)
+    keep = (its > 0) & (its < max_iter) & torch.isfinite(T) & torch.isfinite(T1)
     return p0[keep], s[keep], qt[keep], T[keep], T1[keep], its[keep]
 
 
@@ -184,30 +186,44 @@ def cell_inputs(sim):
     return p0, sim.PV.field("s", Gr), sim.PV.field("qt", Gr)
 
 
-def train_seed(thermo, states, n_samples=6_000_000, held_out_states=None, n_held_out=1_000_000, epochs=12,
-               batch=16384, seed=0, device="cuda"):
+def train_seed(thermo, states, n_pairs=10_000_000, jitter=(200.0, 3.0, 5e-4), held_out_states=None,
+               n_held_out=1_000_000, epochs=12, batch=16384, seed=0, draw=10_000_000, max_draws=8, device="cuda"):
     """Trains a SeedMLP on (p0, s, qt) -> T pairs from the plain FP64 secant
-    (pb_eos_sa) drawn, with a small seeded jitter, from simulation states
-    (a list of (p0, s, qt) flat tensors, e.g. ``cell_inputs`` of runs saved
-    along the way); only the saturated samples become pairs.  Evaluated on
-    pairs drawn from ``held_out_states`` (default: the training states with
-    another seed).  Returns (mlp, info) or (None, info) when the states hold
-    too few saturated cells."""
-    P, S, Q = sample_inputs(states, n_samples, rng_seed=1 + seed, device=device)
-    P, S, Q, T, T1, _ = training_pairs(thermo, P, S, Q)
-    info = {"training_pairs": int(P.numel()), "epochs": epochs}
+    (pb_eos_sa).  Inputs are drawn from simulation states (a list of (p0, s,
+    qt) flat tensors, e.g. ``cell_inputs`` of runs saved along the way) with
+    a seeded uniform jitter of the given half-widths, in batches of ``draw``,
+    until ``n_pairs`` saturated samples are collected (only saturated points
+    are pairs: elsewhere the secant does not run).  Evaluated on pairs drawn
+    the same way from ``held_out_states`` (default: the training states,
+    another seed).  Returns (mlp, info); mlp is None when the draws hold too
+    few saturated points."""
+    import time
+    parts = [[] for _ in range(5)]
+    got, draws = 0, 0
+    while got < n_pairs and draws < max_draws:
+        P, S, Q = sample_inputs(states, draw, rng_seed=1 + seed + 7919 * draws, jitter=jitter, device=device)
+        P, S, Q, T, T1, _ = training_pairs(thermo, P, S, Q)
+        for lst, t in zip(parts, (P, S, Q, T, T1)):
+            lst.append(t)
+        got += P.numel()
+        draws += 1
+    P, S, Q, T, T1 = (torch.cat(lst)[:n_pairs] for lst in parts)
+    info = {"training_pairs": int(P.numel()), "samples_drawn": draws * draw, "epochs": epochs,
+            "jitter_half_widths": list(jitter)}
     if P.numel() < 1000:
         return None, info
     r = T - T1
     mlp = SeedMLP(device=device, seed=seed, out_mean=float(r.mean()), out_scale=2.0 * float(r.std()))
     torch.cuda.synchronize()
-    import time
     t0 = time.time()
     hist = mlp.train(P, S, Q, T, T1, epochs=epochs, batch=batch, seed=seed)
     torch.cuda.synchronize()
     info["train_seconds"] = round(time.time() - t0, 2)
     info["final_batch_loss"] = hist[-1]
-    Ph, Sh, Qh = sample_inputs(held_out_states or states, n_held_out, rng_seed=1000 + seed, device=device)
+    del P, S, Q, T, T1, r
+    held = held_out_states or states
+    hj = jitter if held_out_states is None else (0.0, 0.0, 0.0)
+    Ph, Sh, Qh = sample_inputs(held, n_held_out, rng_seed=1000 + seed, jitter=hj, device=device)
     Ph, Sh, Qh, Th, _, its_h = training_pairs(thermo, Ph, Sh, Qh)
     if Ph.numel():
         guess = mlp.forward(Ph, Sh, Qh)

@@ -45,6 +45,11 @@ CONFIGS = {
     "c1_dry_cbl": dict(case="dry_cbl", nx=32, ny=32, nz=32, dx=50.0, dy=50.0, dz=50.0, gw=3, dt=0.5),
     "c2_bomex": dict(case="bomex", nx=64, ny=64, nz=75, dx=100.0, dy=100.0, dz=40.0, gw=3, dt=1.0),
     "c3_bomex": dict(case="bomex", nx=256, ny=256, nz=128, dx=50.0, dy=50.0, dz=20.0, gw=3, dt=1.0),
+    # the learned seed's measurement grid (256 x 256 x 128, WENO5 as above)
+    # with a cloud-topped state: the BOMEX-like state above holds no
+    # saturated cell, so its secant never runs; dz 10 m puts the 840 m
+    # inversion and the cloud layer inside the 1280 m column
+    "c4_dycoms": dict(case="dycoms", nx=256, ny=256, nz=128, dx=50.0, dy=50.0, dz=10.0, gw=3, dt=0.5),
     "c5_dycoms": dict(case="dycoms", nx=512, ny=512, nz=256, dx=35.0, dy=35.0, dz=5.0, gw=4, dt=0.25,
                       scalar_order=7, momentum_order=5),
 }
@@ -118,24 +123,45 @@ class HotPathSimulation:
 
     # time stepping ---------------------------------------------------------
     def stage(self, rk_step: int, stream=None, mark=None):
-        """One RK stage in the order of Simulation3d.pyx:159-178.  mark(i),
-        if given, is called at the component boundaries (i = 0 before the
-        thermodynamics, 1 after it, 2 after the scalar advection, 3 after the
-        momentum advection -- with the u, v, w stage when fused, with the
-        surface fluxes when a surface scheme is set --, 4 after
-        the remaining RK3 stage and the ghost fill, 5 after the pressure
-        solve and its ghost fill)."""
-        Gr, PV, DV, RS = self.Gr, self.PV, self.DV, self.RS
+        """One RK stage with the reference's calls in the reference's order
+        (Simulation3d.pyx:159-178).  In the precision form without surface,
+        subgrid-scale, forcing or radiation terms, SA.update and MA.update
+        are deferred and TS.update runs them fused with the SSP-RK3 stage
+        (see PrognosticVariables); otherwise every call launches as called.
+        mark(i), if given, is called at the component boundaries (i = 0
+        before the thermodynamics, 1 after it, 2 after the scalar advection,
+        3 after the momentum advection -- with the u, v, w stage when fused,
+        with the surface, subgrid-scale, forcing and radiation terms when
+        they are on --, 4 after the remaining RK3 stage and the ghost fill,
+        5 after the pressure solve and its ghost fill)."""
+        Gr, PV, DV, RS, TS = self.Gr, self.PV, self.DV, self.RS, self.TS
         m = mark if mark is not None else (lambda i: None)
+        fused = self._fused()
+        PV.fuse_stages = fused
+        TS.rk_step = rk_step
         m(0)
         self.Th.update(Gr, RS, PV, DV, stream=stream)
         m(1)
-        if self._fused():
-            self._scalars_and_step(rk_step, stream)
-        else:
-            self.SA.update(Gr, RS, PV, DV, stream=stream)
-        m(2)
-        self._momentum_and_step(rk_step, stream, m)
+        self.SA.update(Gr, RS, PV, DV, stream=stream)
+        if not fused:
+            m(2)
+        self.MA.update(Gr, RS, PV, stream=stream)
+        # then Sur, SGS, SD and MD (Simulation3d.pyx:167-172); Ke.update
+        # (:160) is folded into SGS.update: no velocity changes between
+        self.Sur.update(Gr, RS, PV, DV, stream=stream)
+        if self.SGS is not None:
+            self.SGS.update(Gr, DV, PV, self.Ke, self.Sur, stream=stream)
+            self.SD.update(Gr, RS, PV, DV, stream=stream)
+            self.MD.update(Gr, RS, PV, DV, self.Ke, stream=stream)
+        if self.Fo.scheme != _capi.PB_FORCING_NONE:  # Fo.update (:173)
+            if not self._fo_ready:  # the profiles need the installed reference state
+                self.Fo.initialize(Gr, RS)
+                self._fo_ready = True
+            self.Fo.update(Gr, RS, PV, DV, stream=stream)
+        self.Ra.update(Gr, RS, PV, DV, self.Sur, TS, stream=stream)  # Ra.update (:174)
+        if not fused:
+            m(3)
+        TS.update(Gr, PV, stream=stream, mark=m if fused else None)
         PV.Update_all_bcs(Gr, stream=stream)
         m(4)
         # PressureSolver.update: the solve, then its ghost fill -- of the
@@ -147,98 +173,12 @@ class HotPathSimulation:
 
     def _fused(self) -> bool:
         """The precision form steps with the SSP-RK3 stage fused into the
-        momentum pass (velocities u, v, w first, as this driver adds them)
-        unless fuse_rk is off or a surface scheme adds tendencies between the
-        advection and the stage."""
+        advection passes (velocities u, v, w first, as this driver adds them)
+        unless fuse_rk is off or a surface, subgrid-scale, forcing or
+        radiation term adds tendencies between the advection and the stage."""
         return (self.fuse_rk and self.MA.precision == _capi.PB_FP32
                 and self.Sur.scheme == _capi.PB_SURFACE_NONE and self.SGS is None
                 and self.Fo.scheme == _capi.PB_FORCING_NONE and not self.Ra.active)
-
-    def _clear_w_tendency(self, stream=None):
-        """Fused stepping: the w tendency is cleared once the fused pass has
-        consumed it, as TimeStepping.update clears every tendency after the
-        stage (the other tendencies: the scalars' by their out-of-place
-        stage, u's and v's are never stored)."""
-        npg = self.Gr.dims.npg
-        w = int(self.PV.velocity_directions[2])
-        st = stream if stream is not None else torch.cuda.current_stream(self.PV.values.device)
-        with torch.cuda.stream(st):
-            self.PV.tendencies[w * npg:(w + 1) * npg].zero_()
-
-    def _next_values(self):
-        """The second value buffer of fused stepping."""
-        PV = self.PV
-        nxt = getattr(self, "_values_next", None)
-        if nxt is None or nxt.shape != PV.values.shape or nxt.device != PV.values.device:
-            nxt = self._values_next = torch.zeros_like(PV.values)
-        return nxt
-
-    def _scalars_and_step(self, rk_step: int, stream=None):
-        """Fused stepping: scalar advection with the scalars' SSP-RK3 stage,
-        new values into the second buffer."""
-        Gr, PV, RS, TS = self.Gr, self.PV, self.RS, self.TS
-        scal = [i for i in range(PV.nv) if PV.var_type[i] == 1]
-        if not scal:
-            return
-        npg = Gr.dims.npg
-        nxt = self._next_values()
-        cp = TS.value_copies.view(-1)
-        n = len(scal)
-        arr = lambda t: (ctypes.c_void_p * n)(*[_capi.ptr(t[i * npg:]) for i in scal])
-        vel = [PV.values[int(PV.velocity_directions[d]) * npg:] for d in range(3)]
-        rc = _capi.load().pb_scalar_advection_rk3(
-            ctypes.byref(Gr.dims), _capi.ptr(RS.d_rho0), _capi.ptr(RS.d_rho0_half), _capi.ptr(RS.d_alpha0),
-            _capi.ptr(RS.d_alpha0_half), _capi.ptr(vel[0]), _capi.ptr(vel[1]), _capi.ptr(vel[2]), n,
-            arr(PV.values), arr(PV.tendencies), arr(nxt), arr(cp), TS.dt, rk_step, self.SA.order,
-            _capi.stream_handle(stream))
-        _capi.check(rc, "pb_scalar_advection_rk3")
-
-    def _momentum_and_step(self, rk_step: int, stream=None, mark=None):
-        """Momentum advection and the SSP-RK3 stage of all prognostic
-        variables (mark(3) between the two).  Fused stepping: the momentum
-        pass applies the stage to u, v, w and writes them to the second
-        buffer (the scalar pass has written the scalars there), and the two
-        buffers swap roles."""
-        Gr, PV, RS, TS = self.Gr, self.PV, self.RS, self.TS
-        m = mark if mark is not None else (lambda i: None)
-        TS.rk_step = rk_step
-        if not self._fused():
-            self.MA.update(Gr, RS, PV, stream=stream)
-            # then Sur, SGS, SD and MD (Simulation3d.pyx:167-172); Ke.update
-            # (:160) is folded into SGS.update: no velocity changes between
-            self.Sur.update(Gr, RS, PV, self.DV, stream=stream)
-            if self.SGS is not None:
-                self.SGS.update(Gr, self.DV, PV, self.Ke, self.Sur, stream=stream)
-                self.SD.update(Gr, RS, PV, self.DV, stream=stream)
-                self.MD.update(Gr, RS, PV, self.DV, self.Ke, stream=stream)
-            if self.Fo.scheme != _capi.PB_FORCING_NONE:  # Fo.update (:173)
-                if not self._fo_ready:  # the profiles need the installed reference state
-                    self.Fo.initialize(Gr, RS)
-                    self._fo_ready = True
-                self.Fo.update(Gr, RS, PV, self.DV, stream=stream)
-            self.Ra.update(Gr, RS, PV, self.DV, self.Sur, self.TS, stream=stream)  # Ra.update (:174)
-            m(3)
-            TS.update(Gr, PV, stream=stream)
-            return
-        if [int(i) for i in PV.velocity_directions] != [0, 1, 2]:
-            raise ValueError("fused stepping expects u, v, w as the first prognostic variables")
-        npg = Gr.dims.npg
-        nxt = self._next_values()
-        cp = TS.value_copies.view(-1)
-        L = _capi.load()
-        sh = _capi.stream_handle(stream)
-        rc = L.pb_momentum_advection_rk3(
-            ctypes.byref(Gr.dims), _capi.ptr(RS.d_rho0), _capi.ptr(RS.d_rho0_half), _capi.ptr(RS.d_alpha0),
-            _capi.ptr(RS.d_alpha0_half), _capi.ptr(PV.values[0:]), _capi.ptr(PV.values[npg:]),
-            _capi.ptr(PV.values[2 * npg:]), _capi.ptr(PV.tendencies[2 * npg:]), _capi.ptr(nxt[0:]),
-            _capi.ptr(nxt[npg:]), _capi.ptr(nxt[2 * npg:]), _capi.ptr(cp[0:]), _capi.ptr(cp[npg:]),
-            _capi.ptr(cp[2 * npg:]), TS.dt, rk_step, self.MA.order, sh)
-        _capi.check(rc, "pb_momentum_advection_rk3")
-        self._clear_w_tendency(stream)
-        m(3)
-        PV.values, self._values_next = nxt, PV.values
-        if rk_step == 2:
-            TS.t += TS.dt
 
     def _fill_velocity_ghosts(self, stream=None):
         """Ghost fill of the velocities alone when they are the first

@@ -211,12 +211,15 @@ class ThermodynamicsSA:
         self._seed_y = None      # device float32[npg]: the network's output per cell
         self._seed_for = None    # the network seed_y belongs to
         self._seed_calls = 0
-        # updates between re-evaluations of the network (6: every second
+        # updates between re-evaluations of the network (12: every fourth
         # SSP-RK3 time step; 1: every update).  The network's output for a
         # cell moves ~1e-4 K over a few steps against its own ~1e-2 K error,
-        # and the secant decides every result; measured at 512x512x256 the
-        # mean secant iterations stay at 1.8-1.9 for intervals 3, 6 and 12.
-        self.seed_refresh_interval = max(1, int(namelist.get("gpu", {}).get("seed_refresh_interval", 6)))
+        # and the secant decides every result.  Measured at 512x512x256
+        # (thermodynamics ms per time step, seeded against unseeded 10.76):
+        # interval 6: 10.89 (1.94 secant iterations per saturated cell),
+        # 12: 10.67 (2.02), 24: 10.86 (2.23: more cells saturate between
+        # refreshes and start from the reference's point).
+        self.seed_refresh_interval = max(1, int(namelist.get("gpu", {}).get("seed_refresh_interval", 12)))
 
     def initialize(self, Gr, PV, DV, NS=None, Pa=None):
         PV.add_variable("s", "J kg^-1 K^-1", "s", "specific entropy", "sym", "scalar", Pa)

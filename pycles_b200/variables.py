@@ -30,7 +30,64 @@ class PrognosticVariables:
         self.velocity_directions = np.zeros((Gr.dims.dims,), dtype=np.int64)
         self.velocity_names_directional = ["" for _ in range(Gr.dims.dims)]
         self.values = None
-        self.tendencies = None
+        self._tendencies = None
+        # Deferred advection of the precision form.  ScalarAdvection.update
+        # and MomentumAdvection.update record their work here instead of
+        # launching when fused stepping is possible (fuse_stages, velocities
+        # first); TimeStepping.update then runs the advection kernels that
+        # apply the SSP-RK3 stage in the same pass.  Reading `tendencies`
+        # (as the surface, subgrid-scale, forcing and radiation updates do
+        # between the advection and the time step) first launches the
+        # recorded work as plain advection, so every caller sees the
+        # reference's tendencies.
+        self.fuse_stages = True
+        self.stable_values = False  # fused stages copy the new values back instead of swapping buffers
+        self.values_next = None     # second value buffer of fused stages
+        self._pending = {}
+        self._scalar_tendencies_stale = False
+
+    @property
+    def tendencies(self):
+        if self._pending:
+            self.flush_advection()
+        if self._scalar_tendencies_stale:
+            self._clear_stale_scalar_tendencies()
+        return self._tendencies
+
+    def _clear_stale_scalar_tendencies(self):
+        """A fused stage leaves its scalar advection tendency behind (the
+        scalar passes hand it from one direction to the next); the
+        reference's time step leaves zeros.  Cleared before the first read."""
+        self._scalar_tendencies_stale = False
+        npg = self._tendencies.numel() // max(self.nv, 1)
+        for i in range(self.nv):
+            if self.var_type[i] == 1:
+                self._tendencies[i * npg:(i + 1) * npg].zero_()
+
+    @tendencies.setter
+    def tendencies(self, t):
+        self._tendencies = t
+
+    def fused_stepping_ok(self):
+        """Whether advection may be deferred into the time step: fused stages
+        on and u, v, w the first three variables."""
+        return self.fuse_stages and [int(i) for i in self.velocity_directions] == [0, 1, 2]
+
+    def defer_advection(self, kind, component, Gr, Rs, DV=None, stream=None):
+        self._pending[kind] = (component, Gr, Rs, DV, stream)
+
+    def take_pending_advection(self):
+        pend, self._pending = self._pending, {}
+        return pend
+
+    def flush_advection(self):
+        """Launch deferred advection as plain (unfused) updates, scalars first
+        as the reference calls them."""
+        pend = self.take_pending_advection()
+        for kind in ("scalar", "momentum"):
+            if kind in pend:
+                comp, Gr, Rs, DV, stream = pend[kind]
+                comp.update_now(Gr, Rs, self, DV, stream=stream)
 
     def add_variable(self, name, units, nice_name, desc, bc_type, var_type, Pa=None):
         """PrognosticVariables.add_variable (PrognosticVariables.pyx:34-64)."""
@@ -76,9 +133,7 @@ class PrognosticVariables:
         return self.values[i * npg:(i + 1) * npg].view(*Gr.shape)
 
     def get_tendency_array(self, name, Gr):
-        i = self.name_index[name]
-        npg = Gr.dims.npg
-        return self.tendencies[i * npg:(i + 1) * npg].view(*Gr.shape)
+        return self.tendency(name, Gr).view(*Gr.shape)
 
     def field(self, name, Gr):
         i = self.name_index[name]
@@ -86,7 +141,11 @@ class PrognosticVariables:
 
     def tendency(self, name, Gr):
         i = self.name_index[name]
-        return self.tendencies[i * Gr.dims.npg:(i + 1) * Gr.dims.npg]
+        if self._pending:
+            self.flush_advection()
+        if self.var_type[i] == 1 and self._scalar_tendencies_stale:
+            self._clear_stale_scalar_tendencies()
+        return self._tendencies[i * Gr.dims.npg:(i + 1) * Gr.dims.npg]
 
     def Update_all_bcs(self, Gr, Pa=None, stream=None):
         """PrognosticVariables.update_all_bcs (PrognosticVariables.pyx:183-233)."""

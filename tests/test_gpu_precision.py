@@ -180,3 +180,69 @@ def test_fused_rk_step_equals_separate_passes():
     for n in ("temperature", "ql", "dynamic_pressure"):
         assert np.array_equal(da[n], db[n]), n
 
+
+
+@pytest.mark.parametrize("stable", [False, True], ids=["swap", "stable_address"])
+def test_reference_call_order_runs_fused_stages(stable):
+    """A caller that keeps Simulation3d.run's calls per stage (Th.update,
+    SA.update, MA.update, TS.update, PV.Update_all_bcs, Pr.update;
+    Simulation3d.pyx:159-178) gets the fused stages: the advection is
+    deferred into TS.update, which runs the passes that apply the SSP-RK3
+    stage.  The state equals the driver's fused step bit for bit, every
+    tendency is left at zero as the reference leaves it, and with
+    PV.stable_values the device address of PV.values never changes."""
+    import torch
+    nl, rs, f = host_case(**MOIST_TILES)
+    a = gpu_sim(nl, rs, f, precision="fp32")
+    a.run(2)
+    b = gpu_sim(nl, rs, f, precision="fp32")
+    Gr, RS, PV, DV, TS = b.Gr, b.RS, b.PV, b.DV, b.TS
+    PV.stable_values = stable
+    PV.Update_all_bcs(Gr)
+    b.Th.update(Gr, RS, PV, DV)
+    addr = PV.values.data_ptr()
+    for _ in range(2):
+        for rk in range(3):
+            TS.rk_step = rk
+            b.Th.update(Gr, RS, PV, DV)
+            b.SA.update(Gr, RS, PV, DV)
+            b.MA.update(Gr, RS, PV)
+            TS.update(Gr, PV)
+            PV.Update_all_bcs(Gr)
+            b.Pr.update(Gr, RS, DV, PV)
+    assert TS.fused_stages == 6
+    if stable:
+        assert PV.values.data_ptr() == addr
+    fa, fb = gpu_fields(a), gpu_fields(b)
+    for n in fa:
+        assert np.isfinite(fa[n]).all(), n
+        assert np.array_equal(fa[n], fb[n]), n
+    torch.cuda.synchronize()
+    assert float(PV.tendencies.abs().max()) == 0.0
+
+
+def test_deferred_advection_flushes_for_other_tendency_terms():
+    """Deferred advection is launched as plain advection as soon as anything
+    reads the tendencies before the time step (here a caller adding its own
+    term), so the caller sees the reference's tendencies and the stage runs
+    unfused."""
+    import torch
+    nl, rs, f = host_case(**MOIST_TILES)
+    f = _stir(f)
+    a = gpu_sim(nl, rs, f, precision="fp32")
+    a.fuse_rk = False
+    b = gpu_sim(nl, rs, f, precision="fp32")
+    for g in (a, b):
+        g.PV.Update_all_bcs(g.Gr)
+    a.SA.update(a.Gr, a.RS, a.PV, a.DV)
+    a.MA.update(a.Gr, a.RS, a.PV)
+    b.PV.fuse_stages = True
+    b.SA.update(b.Gr, b.RS, b.PV, b.DV)
+    b.MA.update(b.Gr, b.RS, b.PV)
+    assert b.PV._pending
+    tb = b.PV.tendencies  # flushes
+    assert not b.PV._pending
+    torch.cuda.synchronize()
+    assert torch.equal(a.PV.tendencies, tb)
+    b.TS.update(b.Gr, b.PV)
+    assert b.TS.fused_stages == 0
