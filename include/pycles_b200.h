@@ -345,6 +345,78 @@ int pb_pressure_solve(const pb_dims* dims, const double* rho0, const double* rho
                       double* w, double* divergence, double* dynamic_pressure, void* workspace,
                       long long workspace_bytes, int precision, int refine_sweeps, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Pressure solve of a domain split across GPUs (x-slabs: full y and z)
+ *
+ * The reference decomposes the domain over MPI ranks and transposes the
+ * spectral data between pencils with MPI_Alltoallv (ParallelMPI.pyx:542-1068,
+ * PressureFFTParallel.pyx:150-219) around the same mathematics as the
+ * single-rank solve.  Here the solve is cut into phases; between them the
+ * caller exchanges data between GPUs (all-to-all, halo exchange):
+ *   divergence (x-slab) -> [x-slab to z-slab] -> fft_forward (z-slab: every
+ *   column, a range of levels) -> [z-slab to row slab] -> fft_columns (every
+ *   level, a range of rows j) -> [back] -> fft_inverse -> [back to x-slab]
+ *   -> ghost fill + x-halo exchange of the pressure -> correct.
+ * Dense arrays are the interior cells [i][j][k] (k fastest) of the slab.
+ * The spectral arithmetic is the single-GPU solve's (the same kernels).
+ * ------------------------------------------------------------------------ */
+
+/* Byte offset of the spectral array W[k][j][m] (n2 levels of n1 rows of
+ * n0/2 + 1 complex values) in a workspace of pb_pressure_workspace_bytes(dims),
+ * for a caller that moves it between GPUs; -1 for invalid dims. */
+long long pb_pressure_spectral_offset(const pb_dims* dims);
+
+/* Per-level sums of `field` over this grid's interior columns, i outer and j
+ * inner as HorizontalMean adds them (ParallelMPI.pyx:219-226), unscaled:
+ * sums[nlg2].  A sharded mean adds the GPUs' sums, then scales by
+ * 1/(n0 n1) of the whole domain (ParallelMPI.pyx:229-236). */
+int pb_horizontal_sums(const pb_dims* dims, const double* field, double* sums, void* stream);
+
+/* PressureSolver.update's divergence (PressureSolver.pyx:113-175) on the
+ * cells of this slab: w - mean[k] (remove_mean_u3; mean has nlg2 values),
+ * then second_order_divergence, written to `divergence` (ghosts zero) and,
+ * when div_dense is not NULL, to a dense interior array.  The x-ghost planes
+ * of u must hold the neighbouring slab's values. */
+int pb_pressure_divergence(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                           const double* alpha0, const double* alpha0_half, const double* u,
+                           const double* v, const double* w, const double* mean, double* divergence,
+                           double* div_dense, int precision, void* stream);
+
+/* The precision form's refinement residual div - A p on the cells of this
+ * slab into a dense interior array (the pressure's ghosts filled, x-ghost
+ * planes from the neighbours).  No counterpart in the reference. */
+int pb_pressure_residual(const pb_dims* dims, const double* rho0, const double* rho0_half,
+                         const double* pressure, const double* divergence, double* resid_dense,
+                         void* stream);
+
+/* Forward x- and y-FFT (PressureFFTParallel.pyx:168-180) of the levels of a
+ * z-slab (dims: the whole horizontal plane, the slab's levels; indx_lo of x
+ * and y zero) from a dense right-hand side into the spectral array of a
+ * workspace that pb_pressure_init made for these dims: W[k][j][m], m =
+ * 0 .. n0/2 (the Hermitian half), complex FP64 (PB_FP64) or FP32. */
+int pb_pressure_fft_forward(const pb_dims* slab, void* workspace, long long workspace_bytes,
+                            const double* src_dense, int precision, void* stream);
+
+/* The Thomas solves (SparseSolvers.pyx:24-44, PressureFFTParallel.pyx:
+ * 181-205) of the (kx, ky) columns of a slab of rows j0 .. j0 + rows->n[1]
+ * - 1 over every level: spec W[k][j - j0][m] (complex, the precision's
+ * type) and scratch (doubles, the same count) of the caller; wave numbers
+ * from the z-slab's workspace (slab, slab_workspace); rho0, rho0_half over
+ * the whole column. */
+int pb_pressure_fft_columns(const pb_dims* rows, const double* rho0, const double* rho0_half,
+                            const pb_dims* slab, const void* slab_workspace, void* spec, double* scratch,
+                            int j0, int precision, void* stream);
+
+/* Inverse y- and x-FFT (PressureFFTParallel.pyx:206-219) of a z-slab's
+ * spectral array into a dense pressure. */
+int pb_pressure_fft_inverse(const pb_dims* slab, void* workspace, long long workspace_bytes,
+                            double* dst_dense, int precision, void* stream);
+
+/* second_order_pressure_correction with remove_mean_u3 on every cell
+ * (PressureSolver.pyx:83-136) of this slab; the pressure's ghosts filled. */
+int pb_pressure_correct(const pb_dims* dims, const double* pressure, double* u, double* v, double* w,
+                        const double* mean, void* stream);
+
 /*
  * pb_pressure_solve for callers that cannot allocate device memory.  No
  * counterpart in the reference.  Same inputs, outputs and results as

@@ -113,6 +113,14 @@ SIGNATURES = {
     "pb_pressure_init": (_I, [_DIMS, _P, _LL]),
     "pb_pressure_solve": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _I, _P]),
     "pb_pressure_solve_noalloc": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pb_pressure_spectral_offset": (_LL, [_DIMS]),
+    "pb_horizontal_sums": (_I, [_DIMS, _P, _P, _P]),
+    "pb_pressure_divergence": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "pb_pressure_residual": (_I, [_DIMS, _P, _P, _P, _P, _P, _P]),
+    "pb_pressure_fft_forward": (_I, [_DIMS, _P, _LL, _P, _I, _P]),
+    "pb_pressure_fft_columns": (_I, [_DIMS, _P, _P, _DIMS, _P, _P, _P, _I, _I, _P]),
+    "pb_pressure_fft_inverse": (_I, [_DIMS, _P, _LL, _P, _I, _P]),
+    "pb_pressure_correct": (_I, [_DIMS, _P, _P, _P, _P, _P, _P]),
     "pb_surface_update": (_I, [_DIMS, ctypes.POINTER(PbSurface), _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                _P, _P, ctypes.POINTER(PbSurfaceFields), _P]),
     "pb_kinematics_sgs": (_I, [_DIMS, ctypes.POINTER(PbSgs), _P, _P, _P, _P, _P, _P, _P, _P, _P]),

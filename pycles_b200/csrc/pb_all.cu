@@ -4,5 +4,6 @@
 #include "timestep.cu"
 #include "advection.cu"
 #include "pressure.cu"
+#include "pressure_shard.cu"
 #include "pressure_noalloc.cu"
 #include "mlp.cu"

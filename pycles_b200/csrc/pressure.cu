@@ -300,6 +300,12 @@ struct PArgs {
   const double* ky2;
   void* spec;     // double2 (plain form) or float2 (precision form) W[k][j][i]
   double* scr;
+  // sharded solves (pressure_shard): the x-FFT reads the right-hand side from
+  // a dense [i][j][k] interior array, the inverse x-FFT writes the result to
+  // one, and the Thomas solve of a slab of j rows starts at global row j0
+  const double* src_dense;
+  double* dst_dense;
+  int j0;
 };
 
 template <class C> __device__ __forceinline__ const C* twx_of(const PArgs& a);
@@ -439,21 +445,66 @@ __global__ void zero_ghosts(Geo g, double* __restrict__ f, long long nghost) {
   }
 }
 
+// Right-hand side of the forward x-FFT (fft_x_fwd's SRC) and destination of
+// the inverse (fft_x_inv's DST).
+constexpr int kSrcDivergence = 0, kSrcResidual = 1, kSrcDense = 2;
+constexpr int kDstWrite = 0, kDstAccumulate = 1, kDstDense = 2;
+
+// second_order_divergence (PressureSolver.pyx:138-175, d = 0, 1, 2 in order)
+// of the cell ijk at level k, w taken after remove_mean_u3 (w - mean[k]).
+// Plain form: the reference's divisions by alpha0 in its order, separately
+// rounded; precision form: multiplications by rho0 = 1/alpha0.
+template <bool PLAIN>
+__device__ __forceinline__ double divergence_at(const Geo& g, const PArgs& a, long long ijk, long long k) {
+  const double* __restrict__ U = a.u;
+  const double* __restrict__ V = a.v;
+  const double* __restrict__ Wv = a.w;
+  const double wc = sub_rn(Wv[ijk], a.mean[k]);
+  const double wm = sub_rn(Wv[ijk - 1], a.mean[k - 1]);
+  if constexpr (PLAIN) {
+    const double ah = a.alpha0_half[k];
+    double d = 0.0;
+    d = add_rn(d, mul_rn(sub_rn(U[ijk] / ah, U[ijk - g.is] / ah), g.dxi0));
+    d = add_rn(d, mul_rn(sub_rn(V[ijk] / ah, V[ijk - g.js] / ah), g.dxi1));
+    d = add_rn(d, mul_rn(sub_rn(wc / a.alpha0[k], wm / a.alpha0[k - 1]), g.dxi2));
+    return d;
+  } else {
+    const double rh = a.rho0_half[k];
+    return (U[ijk] - U[ijk - g.is]) * rh * g.dxi0 + (V[ijk] - V[ijk - g.js]) * rh * g.dxi1 +
+           (wc * a.rho0[k] - wm * a.rho0[k - 1]) * g.dxi2;
+  }
+}
+
+// The refinement residual div - A p of the cell ijk (level k, kk = k - gw),
+// A the operator the spectral solve inverts: second differences in x and y,
+// the rows of compute_off_diagonals / compute_diagonal in z.
+__device__ __forceinline__ double residual_at(const Geo& g, const PArgs& a, long long ijk, long long k, long long kk,
+                                              long long nz) {
+  const double* __restrict__ p = a.p;
+  const double pc = p[ijk];
+  const double lap_h = a.rho0_half[k] * ((p[ijk + g.is] - 2.0 * pc + p[ijk - g.is]) * (g.dxi0 * g.dxi0) +
+                                         (p[ijk + g.js] - 2.0 * pc + p[ijk - g.js]) * (g.dxi1 * g.dxi1));
+  double vert = 0.0;
+  if (kk < nz - 1) vert += a.rho0[k] * (p[ijk + 1] - pc);
+  if (kk > 0) vert -= a.rho0[k - 1] * (pc - p[ijk - 1]);
+  return a.div[ijk] - (lap_h + vert * (g.dxi2 * g.dxi2));
+}
+
 // ---- divergence (or refinement residual) + forward x-FFT --------------------
 // block = (interior j, chunk of KC = 2 LC interior levels); smem LC complex
 // lines of n0, line p holding levels 2p (real part) and 2p + 1 (imaginary).
-// RESID = false: the right-hand side is second_order_divergence
-//   (PressureSolver.pyx:138-175, d = 0, 1, 2 in order), written to `div`.
-// RESID = true: the right-hand side is the residual div - A p of the current
-//   pressure, A being the operator the spectral solve inverts (second
-//   differences in x and y, the rows of compute_off_diagonals /
-//   compute_diagonal in z); used by the iterative refinement of the
+// SRC = kSrcDivergence: the right-hand side is second_order_divergence
+//   (divergence_at), written to `div`.
+// SRC = kSrcResidual: the right-hand side is the residual div - A p of the
+//   current pressure (residual_at); used by the iterative refinement of the
 //   precision form.
+// SRC = kSrcDense: the right-hand side is read from a dense interior array
+//   (a slab of levels of a sharded solve).
 //
 // LGN > 0 instantiates the kernel for N = 2^LGN (KC = 2 ct_lines(LGN)), so
 // that the index arithmetic and the FFT passes are compile-time; LGN = 0
 // takes N and KC at run time.
-template <class C, bool RESID, int LGN>
+template <class C, int SRC, int LGN>
 __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KCrt) {
   using R = decltype(C().x);
   constexpr bool CT = LGN > 0;
@@ -470,14 +521,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KCr
   const int lc = (kc + 1) >> 1;
   const long long j = g.gw + jl;
   const int ld = line_ld(N);
-  const double dxi0 = g.dxi0, dxi1 = g.dxi1, dxi2 = g.dxi2;
-  // distinct arrays: lets the unrolled loop issue its loads ahead of the
-  // divergence stores of earlier iterations
-  const double* __restrict__ U = a.u;
-  const double* __restrict__ V = a.v;
-  const double* __restrict__ Wv = a.w;
-  const double* __restrict__ P = a.p;
-  const double* __restrict__ mean = a.mean;
+  const long long ny = g.n1 - 2 * g.gw;
   double* __restrict__ div = a.div;
 #pragma unroll 4
   for (int e = threadIdx.x; e < N * KC; e += kFftThreads) {
@@ -491,32 +535,13 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_fwd(Geo g, PArgs a, int KCr
     const long long k = g.gw + k0 + kl;
     const long long ijk = (g.gw + il) * g.is + j * g.js + k;
     double d;
-    if (!RESID) {
-      // w after remove_mean_u3 (PressureSolver.pyx:113-136), w - mean[k]
-      const double wc = sub_rn(Wv[ijk], mean[k]);
-      const double wm = sub_rn(Wv[ijk - 1], mean[k - 1]);
-      if constexpr (sizeof(C) == sizeof(double2)) {  // plain form: the reference's divisions and order
-        const double ah = a.alpha0_half[k];
-        d = 0.0;
-        d = add_rn(d, mul_rn(sub_rn(U[ijk] / ah, U[ijk - g.is] / ah), dxi0));
-        d = add_rn(d, mul_rn(sub_rn(V[ijk] / ah, V[ijk - g.js] / ah), dxi1));
-        d = add_rn(d, mul_rn(sub_rn(wc / a.alpha0[k], wm / a.alpha0[k - 1]), dxi2));
-      } else {  // precision form: times rho0 = 1/alpha0 instead of six FP64 divisions
-        const double rh = a.rho0_half[k];
-        d = (U[ijk] - U[ijk - g.is]) * rh * dxi0 + (V[ijk] - V[ijk - g.js]) * rh * dxi1 +
-            (wc * a.rho0[k] - wm * a.rho0[k - 1]) * dxi2;
-      }
+    if constexpr (SRC == kSrcDivergence) {
+      d = divergence_at<sizeof(C) == sizeof(double2)>(g, a, ijk, k);
       div[ijk] = d;
-    } else {
-      const double* __restrict__ p = P;
-      const double pc = p[ijk];
-      const double lap_h = a.rho0_half[k] * ((p[ijk + g.is] - 2.0 * pc + p[ijk - g.is]) * (dxi0 * dxi0) +
-                                             (p[ijk + g.js] - 2.0 * pc + p[ijk - g.js]) * (dxi1 * dxi1));
-      const long long kk = k - g.gw;
-      double vert = 0.0;
-      if (kk < nz - 1) vert += a.rho0[k] * (p[ijk + 1] - pc);
-      if (kk > 0) vert -= a.rho0[k - 1] * (pc - p[ijk - 1]);
-      d = div[ijk] - (lap_h + vert * (dxi2 * dxi2));
+    } else if constexpr (SRC == kSrcResidual) {
+      d = residual_at(g, a, ijk, k, k - g.gw, nz);
+    } else {  // a dense interior array (il, jl, k0 + kl)
+      d = a.src_dense[((long long)il * ny + jl) * nz + k0 + kl];
     }
     inr[slot] = (R)d;
   }
@@ -605,7 +630,7 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 4 : 2) tdma_kernel(Geo g
   const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
   const int i = (int)(col % Nx);
-  const int j = (int)(col / Nx);
+  const int j = (int)(col / Nx) + a.j0;  // global row (a slab of rows in a sharded solve)
   C* x = reinterpret_cast<C*>(a.spec) + col;
   double* scr = a.scr + col;
   if (i == 0 && j == 0) {  // mode (0,0) is set to zero (:197-200)
@@ -711,14 +736,18 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 4 : 2) tdma_kernel(Geo g
   }
 }
 
-// ---- inverse x-FFT -> pressure (ACC: add to the current pressure) ----------
+// ---- inverse x-FFT -> pressure ----------------------------------------------
+// DST = kDstWrite: write the pressure; kDstAccumulate: add to the current
+// pressure (refinement); kDstDense: write a dense interior array (a slab of
+// levels of a sharded solve).
 // block = (interior j, chunk of KC = 2 LC levels).  Line p gets
 // Z = A + i B over all m, A and B the stored half-spectra of levels 2p and
 // 2p + 1 extended by A[N-m] = conj A[m]; the inverse transform returns the
 // two real rows as Re z and Im z.
 // (LGN as for fft_x_fwd.)
-template <class C, bool ACC, int LGN>
+template <class C, int DST, int LGN>
 __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KCrt) {
+  constexpr bool ACC = DST == kDstAccumulate;
   constexpr bool CT = LGN > 0;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* in = reinterpret_cast<C*>(smraw);
@@ -757,6 +786,17 @@ __global__ void __launch_bounds__(kFftThreads) fft_x_inv(Geo g, PArgs a, int KCr
   const double sc = 1.0 / (double)N;
   const long long j = g.gw + jl;
   double* __restrict__ p = a.p;
+  if constexpr (DST == kDstDense) {
+    const long long ny = g.n1 - 2 * g.gw;
+    for (int e = threadIdx.x; e < N * KC; e += kFftThreads) {
+      int kl = 0, il = 0;
+      split_idx(e, KC, il, kl);
+      if (kl >= kc) continue;
+      const C z = res[(kl >> 1) * ld + swz(il)];
+      a.dst_dense[((long long)il * ny + jl) * nz + k0 + kl] = (double)((kl & 1) ? z.y : z.x) * sc;
+    }
+    return;
+  }
   // batches of kBatch elements: the pressure loads of a batch (ACC) are all
   // issued before its stores
   constexpr int kBatch = 8;
@@ -915,38 +955,38 @@ int ct_lg(long long n) {
   return lg;
 }
 
-template <class C, int LG>
-static int launch_x_fwd(const Geo& g, PArgs& a, bool resid, dim3 grid, size_t sm, int KC, cudaStream_t st) {
-  if (sm > 48 * 1024) {
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, false, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    if constexpr (sizeof(C) == 8)
-      PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, true, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  }
-  if constexpr (sizeof(C) == 8) {  // the refinement residual exists in the precision form only
-    if (resid) {
-      fft_x_fwd<C, true, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
-      return PB_OK;
-    }
-  }
-  fft_x_fwd<C, false, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
+template <class C, int SRC, int LG>
+static int launch_x_fwd_src(const Geo& g, PArgs& a, dim3 grid, size_t sm, int KC, cudaStream_t st) {
+  if (sm > 48 * 1024)
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_fwd<C, SRC, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  fft_x_fwd<C, SRC, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
   return PB_OK;
 }
 
 template <class C, int LG>
-static int launch_x_inv(const Geo& g, PArgs& a, bool acc, dim3 grid, size_t sm, int KC, cudaStream_t st) {
-  if (sm > 48 * 1024) {
-    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, false, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    if constexpr (sizeof(C) == 8)
-      PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, true, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+static int launch_x_fwd(const Geo& g, PArgs& a, int src, dim3 grid, size_t sm, int KC, cudaStream_t st) {
+  if (src == kSrcDense) return launch_x_fwd_src<C, kSrcDense, LG>(g, a, grid, sm, KC, st);
+  if constexpr (sizeof(C) == 8) {  // the refinement residual exists in the precision form only
+    if (src == kSrcResidual) return launch_x_fwd_src<C, kSrcResidual, LG>(g, a, grid, sm, KC, st);
   }
-  if constexpr (sizeof(C) == 8) {
-    if (acc) {
-      fft_x_inv<C, true, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
-      return PB_OK;
-    }
-  }
-  fft_x_inv<C, false, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
+  return launch_x_fwd_src<C, kSrcDivergence, LG>(g, a, grid, sm, KC, st);
+}
+
+template <class C, int DST, int LG>
+static int launch_x_inv_dst(const Geo& g, PArgs& a, dim3 grid, size_t sm, int KC, cudaStream_t st) {
+  if (sm > 48 * 1024)
+    PB_CUDA_TRY(cudaFuncSetAttribute(fft_x_inv<C, DST, LG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  fft_x_inv<C, DST, LG><<<grid, kFftThreads, sm, st>>>(g, a, KC);
   return PB_OK;
+}
+
+template <class C, int LG>
+static int launch_x_inv(const Geo& g, PArgs& a, int dst, dim3 grid, size_t sm, int KC, cudaStream_t st) {
+  if (dst == kDstDense) return launch_x_inv_dst<C, kDstDense, LG>(g, a, grid, sm, KC, st);
+  if constexpr (sizeof(C) == 8) {
+    if (dst == kDstAccumulate) return launch_x_inv_dst<C, kDstAccumulate, LG>(g, a, grid, sm, KC, st);
+  }
+  return launch_x_inv_dst<C, kDstWrite, LG>(g, a, grid, sm, KC, st);
 }
 
 template <class C, int LG>
@@ -972,40 +1012,83 @@ static int launch_y(const Geo& g, PArgs& a, bool inverse, dim3 grid, size_t sm, 
     default: { constexpr int L_ = 0; call; } break;  \
   }
 
+// The spectral solve in phases, so that a sharded solve can exchange data
+// between them: (1) forward x-FFT (from src) and forward y-FFT of every level
+// of the grid; (2) the Thomas solve of every (kx, ky) column; (3) inverse
+// y-FFT and inverse x-FFT (to dst).
+struct FftShape {
+  long long Nx, Ny, nz, Nh;
+  int LC, KC, IC, lgx, lgy;
+  size_t smx, smy;
+  dim3 gx, gy;
+};
+
 template <class C>
-static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t st) {
-  const long long Nx = g.n0 - 2 * g.gw, Ny = g.n1 - 2 * g.gw, nz = g.n2 - 2 * g.gw;
-  const long long Nh = Nx / 2 + 1;  // stored x-modes
-  const int LC = lines_for(Nx, sizeof(C));  // complex lines per x-FFT block
-  const int KC = 2 * LC;                    // levels per x-FFT block (two per line)
-  const size_t smx = fft_smem(Nx, LC, sizeof(C));
-  const int IC = lines_for(Ny, sizeof(C));
-  const size_t smy = fft_smem(Ny, IC, sizeof(C));
-  const int lgx = ct_lg(Nx), lgy = ct_lg(Ny);
-  if ((lgx && LC != ct_lines(lgx)) || (lgy && IC != ct_lines(lgy))) return PB_ERR_UNSUPPORTED;
-  const dim3 gx((unsigned)Ny, ceil_div(nz, KC));
-  const dim3 gy(ceil_div(Nh, IC), (unsigned)nz);
-  int rc = PB_OK;
-  PB_FFT_DISPATCH(lgx, rc = (launch_x_fwd<C, L_>(g, a, resid, gx, smx, KC, st)));
+static int fft_shape(const Geo& g, FftShape& f) {
+  f.Nx = g.n0 - 2 * g.gw;
+  f.Ny = g.n1 - 2 * g.gw;
+  f.nz = g.n2 - 2 * g.gw;
+  f.Nh = f.Nx / 2 + 1;  // stored x-modes
+  f.LC = lines_for(f.Nx, sizeof(C));  // complex lines per x-FFT block
+  f.KC = 2 * f.LC;                    // levels per x-FFT block (two per line)
+  f.smx = fft_smem(f.Nx, f.LC, sizeof(C));
+  f.IC = lines_for(f.Ny, sizeof(C));
+  f.smy = fft_smem(f.Ny, f.IC, sizeof(C));
+  f.lgx = ct_lg(f.Nx);
+  f.lgy = ct_lg(f.Ny);
+  if ((f.lgx && f.LC != ct_lines(f.lgx)) || (f.lgy && f.IC != ct_lines(f.lgy))) return PB_ERR_UNSUPPORTED;
+  f.gx = dim3((unsigned)f.Ny, ceil_div(f.nz, f.KC));
+  f.gy = dim3(ceil_div(f.Nh, f.IC), (unsigned)f.nz);
+  return PB_OK;
+}
+
+template <class C>
+static int fft_forward(const Geo& g, PArgs& a, int src, cudaStream_t st) {
+  FftShape f;
+  int rc = fft_shape<C>(g, f);
+  if (rc) return rc;
+  PB_FFT_DISPATCH(f.lgx, rc = (launch_x_fwd<C, L_>(g, a, src, f.gx, f.smx, f.KC, st)));
   if (rc) return rc;
   pb_note_launch();
   PB_LAUNCH_CHECK();
-  PB_FFT_DISPATCH(lgy, rc = (launch_y<C, L_>(g, a, false, gy, smy, IC, st)));
-  if (rc) return rc;
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
-  tdma_kernel<C><<<ceil_div(Nh * Ny, 256), 256, 0, st>>>(g, a);
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
-  PB_FFT_DISPATCH(lgy, rc = (launch_y<C, L_>(g, a, true, gy, smy, IC, st)));
-  if (rc) return rc;
-  pb_note_launch();
-  PB_LAUNCH_CHECK();
-  PB_FFT_DISPATCH(lgx, rc = (launch_x_inv<C, L_>(g, a, acc, gx, smx, KC, st)));
+  PB_FFT_DISPATCH(f.lgy, rc = (launch_y<C, L_>(g, a, false, f.gy, f.smy, f.IC, st)));
   if (rc) return rc;
   pb_note_launch();
   PB_LAUNCH_CHECK();
   return PB_OK;
+}
+
+template <class C>
+static int fft_columns(const Geo& g, PArgs& a, cudaStream_t st) {
+  const long long Nh = (g.n0 - 2 * g.gw) / 2 + 1, Ny = g.n1 - 2 * g.gw;
+  tdma_kernel<C><<<ceil_div(Nh * Ny, 256), 256, 0, st>>>(g, a);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  return PB_OK;
+}
+
+template <class C>
+static int fft_inverse(const Geo& g, PArgs& a, int dst, cudaStream_t st) {
+  FftShape f;
+  int rc = fft_shape<C>(g, f);
+  if (rc) return rc;
+  PB_FFT_DISPATCH(f.lgy, rc = (launch_y<C, L_>(g, a, true, f.gy, f.smy, f.IC, st)));
+  if (rc) return rc;
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  PB_FFT_DISPATCH(f.lgx, rc = (launch_x_inv<C, L_>(g, a, dst, f.gx, f.smx, f.KC, st)));
+  if (rc) return rc;
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  return PB_OK;
+}
+
+template <class C>
+static int fft_solve(const Geo& g, PArgs& a, bool resid, bool acc, cudaStream_t st) {
+  int rc;
+  if ((rc = fft_forward<C>(g, a, resid ? kSrcResidual : kSrcDivergence, st))) return rc;
+  if ((rc = fft_columns<C>(g, a, st))) return rc;
+  return fft_inverse<C>(g, a, acc ? kDstAccumulate : kDstWrite, st);
 }
 #undef PB_FFT_DISPATCH
 
@@ -1015,7 +1098,7 @@ static int pressure_solve_impl(const pb_dims* dims, const double* rho0, const do
                                int refine_sweeps, cudaStream_t st) {
   const Geo g = make_geo(dims);
   const PLayout L = playout(dims);
-  PArgs a;
+  PArgs a{};
   a.rho0 = rho0;
   a.rho0_half = rho0_half;
   a.alpha0 = alpha0;
