@@ -752,6 +752,59 @@ def run_ours(args, rank, world, local_rank):
     return out, sim
 
 
+def run_slabs(args, cfg, rank, world, local_rank):
+    """The precision form over x-slabs of the configuration's domain (one
+    slab per GPU; pycles_b200.parallel): device time of K steps after W
+    warm-up steps, the slowest rank's, for the whole domain."""
+    import torch
+
+    from pycles_b200 import _capi, cases, parallel
+    from pycles_b200.grid import Grid
+    from pycles_b200.reference_state import ReferenceState
+    from pycles_b200.simulation import namelist_for
+    from pycles_b200.thermodynamics import ThermodynamicsDry, ThermodynamicsSA
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    nl = namelist_for(**cfg, precision="fp32")
+    # the whole domain's seeded state, built the same way on every rank (host)
+    Gr = Grid(nl)
+    Gr.device = "cpu"
+    RS = ReferenceState(Gr)
+    Th = ThermodynamicsSA(nl) if cfg["case"] != "dry_cbl" else ThermodynamicsDry(nl)
+    fields = cases.CASES[cfg["case"]](Gr, RS, Th, seed=0)
+    comm = parallel.DistComm() if world > 1 else parallel.LocalComm(1)
+    sh = parallel.ShardedSimulation(nl, comm, [dev])
+    sh.load_global(RS.profiles(), fields)
+    del fields
+    sh.run(0)
+    _capi.clear_error()
+    for _ in range(args.warmup):
+        sh.step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    stream = torch.cuda.current_stream(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    L = _capi.load()
+    n0 = L.pb_launch_count()
+    a.record(stream)
+    for _ in range(args.steps):
+        sh.step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    launches = L.pb_launch_count() - n0
+    ms = max_over_ranks(a.elapsed_time(b), dev, world)
+    npl = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    return {"metric": METRIC, "value": npl * 3 * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32 fluxes/FFT, f64 accumulation, TDMA, secant",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"{args.config}: {cfg['nx']}x{cfg['ny']}x{cfg['nz']} cells in {world} x-slabs",
+                       "form": "fp32", "cells": npl, "l2": "inputs larger than L2 (no flush needed)",
+                       "parallelism": f"x-slabs x{world}"},
+            "e2e": None, "gpu_launches": launches, "device_error_word": _capi.get_error()}
+
+
 def run_accuracy(args, cfg):
     """Error of the precision forms against the FP64 plain form: the three
     forms start from the same seeded state and run N steps; per field the
@@ -846,6 +899,10 @@ def main():
     ap.add_argument("--no-c4", action="store_true",
                     help="skip the learned seed's measurement at 256x256x128 (c4_dycoms)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--decomposition", default="replicas", choices=["replicas", "slabs"],
+                    help="replicas: every GPU steps its own copy of the configuration (weak scaling); "
+                         "slabs: the configuration's domain split in x-slabs across the GPUs, halo "
+                         "exchanges and the pressure's transposes over NCCL (strong scaling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surface", action="store_true",
@@ -913,7 +970,10 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    out, _ = run_ours(args, rank, world, local_rank)
+    if args.decomposition == "slabs":
+        out = run_slabs(args, cfg, rank, world, local_rank)
+    else:
+        out, _ = run_ours(args, rank, world, local_rank)
     if rank == 0:
         out["cpu_baseline"] = cpu
         print(json.dumps(out))

@@ -135,17 +135,25 @@ __device__ __forceinline__ float weno5_c0(float a2, float a1, float b1, float b2
   // (beta0, beta2) = 13/12 (X2 - 2 X1)^2 + 1/4 (X2 - 4 X1)^2
   const float2 Sa = fma2(X1, f2(-2.0f, -2.0f), X2);
   const float2 Sb = fma2(X1, f2(-4.0f, -4.0f), X2);
-  const float2 E02 = fma2(mul2(Sa, f2(13.0f / 12.0f, 13.0f / 12.0f)), Sa,
-                          fma2(mul2(Sb, f2(0.25f, 0.25f)), Sb, f2(1e-10f, 1e-10f)));
+  // e_k = beta_k + 1e-10, all three scaled by kE (the weights d_k / e_k^2
+  // over their sum do not change when every e_k is scaled alike)
+  constexpr float kE = 1.0e4f;
+  const float2 E02 = fma2(mul2(Sa, f2(kE * 13.0f / 12.0f, kE * 13.0f / 12.0f)), Sa,
+                          fma2(mul2(Sb, f2(kE * 0.25f, kE * 0.25f)), Sb, f2(kE * 1e-10f, kE * 1e-10f)));
   const float s1a = a1 + b1, s1b = a1 - b1;
-  const float e1 = (13.0f / 12.0f) * s1a * s1a + 0.25f * s1b * s1b + 1e-10f;
+  const float e1 = (kE * 13.0f / 12.0f) * s1a * s1a + (kE * 0.25f) * s1b * s1b + kE * 1e-10f;
+  // the weights with numerators and denominator multiplied by
+  // e0^2 e1^2 e2^2: one reciprocal instead of four.  With the scaling the
+  // products stay normal numbers: >= 1e-24 where every stencil is flat
+  // (unscaled they reach 1e-40, which the packed multiplies flush to zero),
+  // <= 3e38 for first differences up to ~600
   const float2 Q02 = mul2(E02, E02);
-  const float al0 = __fdividef(0.1f, Q02.x);
-  const float al2 = __fdividef(0.3f, Q02.y);
-  const float al1 = __fdividef(0.6f, e1 * e1);
-  const float inv = __fdividef(1.0f, al0 + al1 + al2);
-  const float2 acc = mul2(f2(al0, al2), P02);
-  return (acc.x + acc.y + al1 * p1) * inv;
+  const float q1 = e1 * e1;
+  const float2 A02 = mul2(mul2(f2(0.1f, 0.3f), f2(Q02.y, Q02.x)), f2(q1, q1));  // (0.1 q1 q2, 0.3 q0 q1)
+  const float a1w = 0.6f * Q02.x * Q02.y;
+  const float2 acc = mul2(A02, P02);
+  const float inv = __fdividef(1.0f, A02.x + A02.y + a1w);
+  return (acc.x + acc.y + a1w * p1) * inv;
 }
 
 __device__ __forceinline__ float weno7_c0(float a3, float a2, float a1, float b1, float b2, float b3) {
