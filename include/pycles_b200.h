@@ -257,6 +257,16 @@ int pb_mlp_forward(const pb_mlp* mlp, const double* p0, const double* s, const d
                    double* T_seed, long long n, void* stream);
 
 /*
+ * The learned seed's refresh on the 5th-generation tensor cores (tcgen05,
+ * FP32 accumulators in tensor memory): net->seed_y[cell] = the network's
+ * output y for every cell with ql > 0, NaN elsewhere -- what pb_thermo_sa
+ * runs before its kernel when net->seed_refresh is set.  p0_half per level;
+ * s, qt, ql ghosted fields.  No counterpart in the reference.
+ */
+int pb_mlp_refresh_seed(const pb_mlp* net, const pb_dims* dims, const double* p0_half, const double* s,
+                        const double* qt, const double* ql, void* stream);
+
+/*
  * Adds the gradient of sum_i 0.5 (MLP(x_i) - target_i)^2 to grad[PB_MLP_NPARAM]
  * and the loss sum to *loss (both FP32, device, accumulated).  x: n x 3
  * inputs already normalised to [-1, 1]; target: n normalised outputs.

@@ -102,6 +102,7 @@ SIGNATURES = {
                           _P, _I, ctypes.POINTER(PbMlp), _P, _I, _I, _P]),
     "pb_eos_sa": (_I, [ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
     "pb_mlp_forward": (_I, [ctypes.POINTER(PbMlp), _P, _P, _P, _P, _LL, _P]),
+    "pb_mlp_refresh_seed": (_I, [ctypes.POINTER(PbMlp), _DIMS, _P, _P, _P, _P, _P]),
     "pb_mlp_grad": (_I, [ctypes.POINTER(PbMlp), _P, _P, _LL, _P, _P, _P]),
     "pb_mlp_adam": (_I, [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                          ctypes.c_float, _P, _P, _P, _P, _P, _P, _P]),

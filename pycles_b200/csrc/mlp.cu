@@ -3,6 +3,7 @@
 // fragment layouts.)
 #include "pb_common.cuh"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 #include "thermo_funcs.cuh"
 
 static_assert(mlpk::NPARAM == PB_MLP_NPARAM, "packed parameter count must match the public header");
@@ -61,109 +62,14 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(FwdArgs a) {
   }
 }
 
-// Refresh of the learned seed's per-cell network output y for the cells
-// that were saturated at the previous thermodynamics update (ql > 0 there).
-// Runs as its own kernel ahead of the thermodynamics kernel, which then
-// reads y: the network's code and shared memory stay out of the FP64 secant
-// kernel (whose instruction cache it overflowed).  Each warp scans its
-// chunks of 32 consecutive cells kBatch chunks at a time (kBatch flag loads
-// in flight), appends the flagged cells to a queue in shared memory and
-// evaluates the network whenever the queue holds a full 16-row tile, so the
-// tiles are full except the warp's last one.  Cells not flagged get NaN: a
-// cell that saturates between refreshes starts its secant from the
-// reference's second point, not from a stale output.
-struct RefreshArgs {
-  const __nv_bfloat16* w1;
-  const float* b1;
-  const __nv_bfloat16* w2;
-  const float* b2;
-  const __nv_bfloat16* w3;
-  const float* b3;
-  float lo[3], hi[3];
-  const double* p0;  // per level (n2)
-  const double* s;
-  const double* qt;
-  const double* ql;  // the previous update's condensate: the flag
-  float* y;
-  long long npg;
-  int n2;
-};
-
-constexpr int kRefreshWarps = 4;
-constexpr int kRefreshBatch = 8;                   // chunks scanned per round
-constexpr int kQueue = 32 * kRefreshBatch + 16;    // queue capacity per warp
-
-// One full tile from the head of the warp's queue q (cell indices).
-__device__ __forceinline__ void refresh_tile(const Smem& sm, const RefreshArgs& a, const int* q, int n) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane >> 2;
-  float x0[3] = {0.f, 0.f, 0.f}, x1[3] = {0.f, 0.f, 0.f};
-  long long i0 = -1, i1 = -1;
-  if (g < n) {
-    i0 = q[g];
-    x0[0] = norm_in(a.p0[(int)i0 % a.n2], a.lo[0], a.hi[0]);
-    x0[1] = norm_in(a.s[i0], a.lo[1], a.hi[1]);
-    x0[2] = norm_in(a.qt[i0], a.lo[2], a.hi[2]);
-  }
-  if (g + 8 < n) {
-    i1 = q[g + 8];
-    x1[0] = norm_in(a.p0[(int)i1 % a.n2], a.lo[0], a.hi[0]);
-    x1[1] = norm_in(a.s[i1], a.lo[1], a.hi[1]);
-    x1[2] = norm_in(a.qt[i1], a.lo[2], a.hi[2]);
-  }
-  float y0, y1;
-  forward_tile(sm, x0, x1, y0, y1, nullptr);
-  if ((lane & 3) == 0) {
-    if (i0 >= 0) a.y[i0] = y0;
-    if (i1 >= 0) a.y[i1] = y1;
-  }
-}
-
-__global__ void __launch_bounds__(32 * kRefreshWarps) mlp_seed_refresh_kernel(RefreshArgs a) {
-  __shared__ Smem sm;
-  __shared__ int queue[kRefreshWarps][kQueue];
-  stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3, threadIdx.x, blockDim.x);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int* q = queue[wid];
-  int nq = 0;  // warp-uniform queue length
-  const long long nchunk = (a.npg + 31) / 32;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  const long long first = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  for (long long cb = first; cb < nchunk; cb += (long long)kRefreshBatch * nwarps) {
-    unsigned masks[kRefreshBatch];
-#pragma unroll
-    for (int m = 0; m < kRefreshBatch; ++m) {
-      const long long idx = (cb + m * nwarps) * 32 + lane;
-      masks[m] = __ballot_sync(0xffffffffu, idx < a.npg && __ldg(a.ql + idx) > 0.0);
-    }
-#pragma unroll
-    for (int m = 0; m < kRefreshBatch; ++m) {
-      const long long idx = (cb + m * nwarps) * 32 + lane;
-      if ((masks[m] >> lane) & 1u) {
-        q[nq + __popc(masks[m] & ((1u << lane) - 1u))] = (int)idx;
-      } else if (idx < a.npg) {
-        a.y[idx] = __int_as_float(0x7fc00000);  // not evaluated: NaN, the secant takes its own start
-      }
-      nq += __popc(masks[m]);
-    }
-    __syncwarp();
-    int head = 0;
-    while (nq - head >= 16) {
-      refresh_tile(sm, a, q + head, 16);
-      head += 16;
-    }
-    // keep the remainder (< 16) at the front of the queue
-    __syncwarp();
-    const int rest = nq - head;
-    const int moved = lane < rest ? q[head + lane] : 0;
-    __syncwarp();
-    if (lane < rest) q[lane] = moved;
-    nq = rest;
-    __syncwarp();
-  }
-  if (nq > 0) refresh_tile(sm, a, q, nq);
-}
+// The refresh of the learned seed's per-cell network output y for the cells
+// that were saturated at the previous thermodynamics update (ql > 0 there)
+// runs on the tcgen05 tensor cores (mlp_tc.cuh), as its own kernel ahead of
+// the thermodynamics kernel, which then reads y: the network's code and
+// shared memory stay out of the FP64 secant kernel (whose instruction cache
+// it overflowed).  Cells not flagged get NaN: a cell that saturates between
+// refreshes starts its secant from the reference's second point, not from a
+// stale output.
 
 // Gradient of sum_r 0.5 (y_r - target_r)^2 over n normalised samples,
 // accumulated into grad[NPARAM] (packed, FP32), loss sum into *loss.
@@ -370,12 +276,11 @@ __global__ void mlp_adam_kernel(AdamArgs a) {
 
 static int mlp_blocks(long long work_tiles, int warps_per_block);
 
-// y[cell] = MLP(p0, s, qt) for every cell with ql > 0 (called by
-// pb_thermo_sa before its kernel; mlp validated there).
-cudaError_t pb_mlp_seed_refresh(const pb_mlp* mlp, const Geo& g, const double* p0, const double* s,
-                                const double* qt, const double* ql, cudaStream_t st) {
-  if (g.npg >= (1LL << 31)) return cudaErrorInvalidValue;  // the queue holds 32-bit cell indices
-  mlpk::RefreshArgs a;
+// The refresh on the tcgen05 tensor cores (mlp_tc.cuh): one persistent
+// block of 128 threads per resident slot, 6 per SM.
+static cudaError_t refresh_tc(const pb_mlp* mlp, const Geo& g, const double* p0, const double* s,
+                              const double* qt, const double* ql, cudaStream_t st) {
+  mlptc::RefreshTcArgs a;
   a.w1 = static_cast<const __nv_bfloat16*>(mlp->w1);
   a.b1 = mlp->b1;
   a.w2 = static_cast<const __nv_bfloat16*>(mlp->w2);
@@ -393,10 +298,25 @@ cudaError_t pb_mlp_seed_refresh(const pb_mlp* mlp, const Geo& g, const double* p
   a.y = mlp->seed_y;
   a.npg = g.npg;
   a.n2 = (int)g.n2;
-  mlpk::mlp_seed_refresh_kernel<<<mlp_blocks((g.npg + 31) / 32, mlpk::kRefreshWarps), 32 * mlpk::kRefreshWarps, 0,
-                                  st>>>(a);
+  a.err = pb_error_word_ptr();
+  cudaError_t e = cudaFuncSetAttribute(mlptc::mlp_seed_refresh_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)mlptc::kSmemRequest);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long tiles = (g.npg + mlptc::kThreads * mlptc::kScanBatch - 1) / (mlptc::kThreads * mlptc::kScanBatch);
+  const int blocks = (int)(tiles < 6LL * sms ? tiles : 6LL * sms);
+  mlptc::mlp_seed_refresh_tc<<<blocks < 1 ? 1 : blocks, mlptc::kThreads, mlptc::kSmemRequest, st>>>(a);
   pb_note_launch();
   return cudaGetLastError();
+}
+
+// y[cell] = MLP(p0, s, qt) for every cell with ql > 0 (called by
+// pb_thermo_sa before its kernel; mlp validated there).
+cudaError_t pb_mlp_seed_refresh(const pb_mlp* mlp, const Geo& g, const double* p0, const double* s,
+                                const double* qt, const double* ql, cudaStream_t st) {
+  if (g.npg >= (1LL << 31)) return cudaErrorInvalidValue;  // the queues hold 32-bit cell indices
+  return refresh_tc(mlp, g, p0, s, qt, ql, st);
 }
 
 static int mlp_blocks(long long work_tiles, int warps_per_block) {
@@ -405,6 +325,17 @@ static int mlp_blocks(long long work_tiles, int warps_per_block) {
   long long b = (work_tiles + warps_per_block - 1) / warps_per_block;
   if (b > (long long)sms * 8) b = (long long)sms * 8;
   return (int)(b < 1 ? 1 : b);
+}
+
+extern "C" int pb_mlp_refresh_seed(const pb_mlp* mlp, const pb_dims* dims, const double* p0_half, const double* s,
+                                   const double* qt, const double* ql, void* stream) {
+  int rc = pb_check_dims(dims);
+  if (rc) return rc;
+  if (!mlp || !mlp->w1 || !mlp->b1 || !mlp->w2 || !mlp->b2 || !mlp->w3 || !mlp->b3 || !mlp->seed_y || !p0_half ||
+      !s || !qt || !ql)
+    return PB_ERR_ARG;
+  const Geo g = make_geo(dims);
+  return pb_mlp_seed_refresh(mlp, g, p0_half, s, qt, ql, as_stream(stream)) == cudaSuccess ? PB_OK : PB_ERR_CUDA;
 }
 
 extern "C" int pb_mlp_forward(const pb_mlp* mlp, const double* p0, const double* s, const double* qt,

@@ -1,5 +1,9 @@
 // Learned saturation-adjustment seed: a 3 -> 64 -> 64 -> 1 SiLU MLP.
 //
+// Warp-level tiles for point lists (pb_mlp_forward) and training
+// (pb_mlp_grad); the refresh of a whole field's seeds runs on the tcgen05
+// tensor cores with the same arithmetic (mlp_tc.cuh).
+//
 // One warp evaluates a tile of 16 samples.  The three layers run on the
 // tensor cores with mma.sync m16n8k16 (BF16 operands, FP32 accumulation;
 // layer 1's inputs split into BF16 high and low parts, layer 3 as an N = 8
