@@ -81,11 +81,13 @@ COMPONENT_KERNELS = {
     "thermo": "thermo_sa_kernel (saturation adjustment, buoyancy, bvf, thetali; one launch per stage)",
     "scalar_adv": "scalar_march x, y + scalar_z (WENO fluxes + divergence; 3 launches per stage and scalar "
                   "in the precision form, the scalars' SSP-RK3 stage in scalar_z; 3 per stage in the plain form)",
-    "momentum_adv": "momentum_tile with the u, v, w SSP-RK3 stage in the precision form (1 launch per stage); "
+    "momentum_adv": "momentum_tma (y-z planes of u, v, w staged by TMA; momentum_tile on odd-level grids) with "
+                    "the u, v, w SSP-RK3 stage in the precision form (1 launch per stage); "
                     "momentum_march x, y + momentum_z in the plain form (3 launches)",
     "rk3+bcs": "rk3_kernel + ghost_fill_kernel (the precision form: the ghost fill alone, its stage is "
                "inside the advection passes)",
-    "pressure": "hmean, fft_x_fwd, fft_y, tdma, fft_x_inv (+ refinement), ghost_sym, correction",
+    "pressure": "hmean_partial + hmean_final (hmean_serial, the reference's summation order, in the plain "
+                "form), fft_x_fwd, fft_y, tdma, fft_x_inv (+ refinement), ghost_sym, correction",
 }
 
 

@@ -270,9 +270,15 @@ int pb_mlp_refresh_seed(const pb_mlp* net, const pb_dims* dims, const double* p0
  * Adds the gradient of sum_i 0.5 (MLP(x_i) - target_i)^2 to grad[PB_MLP_NPARAM]
  * and the loss sum to *loss (both FP32, device, accumulated).  x: n x 3
  * inputs already normalised to [-1, 1]; target: n normalised outputs.
+ * workspace: device scratch of at least pb_mlp_grad_workspace_bytes(n)
+ * bytes, 16-byte aligned (PB_ERR_WORKSPACE otherwise), for the per-block
+ * partial sums.  The result is deterministic: the partials are added in a
+ * fixed order (no floating-point atomics), so the same inputs give the same
+ * gradient bit for bit.  No counterpart in the reference.
  */
+long long pb_mlp_grad_workspace_bytes(long long n);
 int pb_mlp_grad(const pb_mlp* mlp, const float* x, const float* target, long long n, float* grad,
-                float* loss, void* stream);
+                float* loss, void* workspace, long long workspace_bytes, void* stream);
 
 /*
  * One Adam step on the FP32 master parameters (grad scaled by grad_scale),
@@ -432,9 +438,9 @@ int pb_pressure_correct(const pb_dims* dims, const double* pressure, double* u, 
  * counterpart in the reference.  Same inputs, outputs and results as
  * pb_pressure_solve (FP64), but its scratch lives in a fixed file-scope
  * device array inside the library instead of a caller workspace, for code
- * that may not call cudaMalloc (a graph capture that must not allocate, an
- * allocator policy that forbids late device allocations, a host binding
- * without a device allocator).
+ * that may not call cudaMalloc (a loop that cannot afford the device-wide
+ * synchronisation an allocation may bring, an allocator policy that forbids
+ * late device allocations, a host binding without a device allocator).
  *   Limit : pb_pressure_workspace_bytes(dims) must not exceed
  *           PB_PRESSURE_NOALLOC_MAX_BYTES (64 MiB, e.g. 128 x 128 x 160);
  *           larger grids return PB_ERR_WORKSPACE.  Every GPU that loads the

@@ -103,7 +103,8 @@ SIGNATURES = {
     "pb_eos_sa": (_I, [ctypes.POINTER(PbTable), _P, _P, _P, _P, _P, _P, _P, _P, _P, _LL, _I, _P]),
     "pb_mlp_forward": (_I, [ctypes.POINTER(PbMlp), _P, _P, _P, _P, _LL, _P]),
     "pb_mlp_refresh_seed": (_I, [ctypes.POINTER(PbMlp), _DIMS, _P, _P, _P, _P, _P]),
-    "pb_mlp_grad": (_I, [ctypes.POINTER(PbMlp), _P, _P, _LL, _P, _P, _P]),
+    "pb_mlp_grad_workspace_bytes": (_LL, [_LL]),
+    "pb_mlp_grad": (_I, [ctypes.POINTER(PbMlp), _P, _P, _LL, _P, _P, _P, _LL, _P]),
     "pb_mlp_adam": (_I, [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                          ctypes.c_float, _P, _P, _P, _P, _P, _P, _P]),
     "pb_thermo_dry": (_I, [_DIMS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),

@@ -73,6 +73,14 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(FwdArgs a) {
 
 // Gradient of sum_r 0.5 (y_r - target_r)^2 over n normalised samples,
 // accumulated into grad[NPARAM] (packed, FP32), loss sum into *loss.
+//
+// Deterministic: no floating-point atomics.  Each warp accumulates its
+// tiles (a fixed set: tile = warp + round * warps) into its own
+// shared-memory copy of the gradient, in program order; each block writes
+// the sum of its warps' copies (warp 0 + warp 1) as one row of a partials
+// array, and grad_reduce_kernel adds the rows in block order.  The block
+// count depends only on n (kGradMaxBlocks caps it), so the same inputs give
+// the same gradient bit for bit on every run and every device.
 struct GradArgs {
   const __nv_bfloat16* w1;
   const float* b1;
@@ -82,26 +90,36 @@ struct GradArgs {
   const float* b3;
   const float* x;       // n x 3
   const float* target;  // n
-  float* grad;
-  float* loss;
+  float* part;  // [gridDim.x][kPartStride]: a block's gradient, then its loss
   long long n;
 };
 
 constexpr int kGradWarps = 2;
-// dynamic shared memory of mlp_grad_kernel: the FP32 gradient accumulator
-constexpr size_t kGradSmem = NPARAM * sizeof(float);
+constexpr int kGradMaxBlocks = 1184;
+constexpr int kPartStride = NPARAM + 1;
+// dynamic shared memory of mlp_grad_kernel: one FP32 gradient accumulator
+// per warp
+constexpr size_t kGradSmem = (size_t)kGradWarps * NPARAM * sizeof(float);
+
+inline int grad_blocks(long long n) {
+  const long long tiles = (n + 15) / 16;
+  long long b = (tiles + kGradWarps - 1) / kGradWarps;
+  if (b > kGradMaxBlocks) b = kGradMaxBlocks;
+  return (int)(b < 1 ? 1 : b);
+}
 
 __global__ void __launch_bounds__(64) mlp_grad_kernel(GradArgs a) {
   __shared__ Smem sm;
-  extern __shared__ float acc[];  // [NPARAM]
+  extern __shared__ float acc_all[];  // [kGradWarps][NPARAM]
   __shared__ float dz2_s[kGradWarps][16][H];
   __shared__ float h1_s[kGradWarps][16][H];
-  __shared__ float loss_s;
+  __shared__ float loss_s[kGradWarps];
   stage_weights(sm, a.w1, a.b1, a.w2, a.b2, a.w3, a.b3, threadIdx.x, blockDim.x);
-  for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) acc[i] = 0.0f;
-  if (threadIdx.x == 0) loss_s = 0.0f;
+  for (int i = threadIdx.x; i < kGradWarps * NPARAM; i += blockDim.x) acc_all[i] = 0.0f;
   __syncthreads();
   const int wid = threadIdx.x >> 5;
+  // this warp's accumulator: every entry is written by one lane at a time
+  float* acc = acc_all + wid * NPARAM;
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -146,8 +164,8 @@ __global__ void __launch_bounds__(64) mlp_grad_kernel(GradArgs a) {
         }
         if (g == 0) {
           const int col = nt * 8 + 2 * t + p;
-          atomicAdd(&acc[OFF_W3 + col], gw3);
-          atomicAdd(&acc[OFF_B2 + col], gb2);
+          acc[OFF_W3 + col] += gw3;
+          acc[OFF_B2 + col] += gb2;
         }
       }
     }
@@ -155,7 +173,7 @@ __global__ void __launch_bounds__(64) mlp_grad_kernel(GradArgs a) {
     gb3 += __shfl_xor_sync(0xffffffffu, gb3, 4);
     gb3 += __shfl_xor_sync(0xffffffffu, gb3, 8);
     gb3 += __shfl_xor_sync(0xffffffffu, gb3, 16);
-    if (lane == 0) atomicAdd(&acc[OFF_B3], gb3);
+    if (lane == 0) acc[OFF_B3] += gb3;
     // stage dz2 and the BF16 h1 of this tile for the layer-2 weight gradient
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt)
@@ -216,8 +234,8 @@ __global__ void __launch_bounds__(64) mlp_grad_kernel(GradArgs a) {
         }
         if (g == 0) {
           const int k = nt2 * 8 + 2 * t + p;
-          atomicAdd(&acc[OFF_B1 + k], gb1);
-          for (int i = 0; i < 3; ++i) atomicAdd(&acc[OFF_W1 + k * 3 + i], gw[i]);
+          acc[OFF_B1 + k] += gb1;
+          for (int i = 0; i < 3; ++i) acc[OFF_W1 + k * 3 + i] += gw[i];
         }
       }
     }
@@ -228,15 +246,31 @@ __global__ void __launch_bounds__(64) mlp_grad_kernel(GradArgs a) {
       float sacc = 0.0f;
 #pragma unroll
       for (int r = 0; r < 16; ++r) sacc += dz2_s[wid][r][n] * h1_s[wid][r][k];
-      atomicAdd(&acc[OFF_W2 + e], sacc);
+      acc[OFF_W2 + e] += sacc;
     }
     __syncwarp();
   }
   for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
-  if (lane == 0) atomicAdd(&loss_s, lsum);
+  if (lane == 0) loss_s[wid] = lsum;
   __syncthreads();
-  for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) atomicAdd(&a.grad[i], acc[i]);
-  if (threadIdx.x == 0) atomicAdd(a.loss, loss_s);
+  static_assert(kGradWarps == 2, "the block's sum below adds two warps' copies");
+  float* row = a.part + (long long)blockIdx.x * kPartStride;
+  for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) row[i] = acc_all[i] + acc_all[NPARAM + i];
+  if (threadIdx.x == 0) row[NPARAM] = loss_s[0] + loss_s[1];
+}
+
+// grad[i] += sum over blocks b (in order) of part[b][i]; *loss likewise from
+// the rows' last entry.  One thread per entry; a row is read coalesced.
+__global__ void __launch_bounds__(256) grad_reduce_kernel(const float* __restrict__ part, int blocks,
+                                                          float* __restrict__ grad, float* __restrict__ loss) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kPartStride) return;
+  float s = 0.0f;
+  for (int b = 0; b < blocks; ++b) s += part[(long long)b * kPartStride + i];
+  if (i < NPARAM)
+    grad[i] += s;
+  else
+    *loss += s;
 }
 
 // Adam on the FP32 master parameters, then BF16 / FP32 copies for the kernels.
@@ -367,11 +401,19 @@ extern "C" int pb_mlp_forward(const pb_mlp* mlp, const double* p0, const double*
   return PB_OK;
 }
 
+extern "C" long long pb_mlp_grad_workspace_bytes(long long n) {
+  if (n < 0) return -1;
+  return (long long)mlpk::grad_blocks(n) * mlpk::kPartStride * (long long)sizeof(float);
+}
+
 extern "C" int pb_mlp_grad(const pb_mlp* mlp, const float* x, const float* target, long long n, float* grad,
-                           float* loss, void* stream) {
+                           float* loss, void* workspace, long long workspace_bytes, void* stream) {
   if (!mlp || !mlp->w1 || !mlp->b1 || !mlp->w2 || !mlp->b2 || !mlp->w3 || !mlp->b3) return PB_ERR_ARG;
   if (!x || !target || !grad || !loss || n < 0) return PB_ERR_ARG;
   if (n == 0) return PB_OK;
+  if (!workspace || workspace_bytes < pb_mlp_grad_workspace_bytes(n) ||
+      (reinterpret_cast<uintptr_t>(workspace) & 15))
+    return PB_ERR_WORKSPACE;
   mlpk::GradArgs a;
   a.w1 = static_cast<const __nv_bfloat16*>(mlp->w1);
   a.b1 = mlp->b1;
@@ -381,8 +423,7 @@ extern "C" int pb_mlp_grad(const pb_mlp* mlp, const float* x, const float* targe
   a.b3 = mlp->b3;
   a.x = x;
   a.target = target;
-  a.grad = grad;
-  a.loss = loss;
+  a.part = static_cast<float*>(workspace);
   a.n = n;
   // the shared-memory opt-in is set on each device's copy of the kernel
   static bool attr_set[64] = {};
@@ -393,8 +434,12 @@ extern "C" int pb_mlp_grad(const pb_mlp* mlp, const float* x, const float* targe
                                      (int)mlpk::kGradSmem));
     if (dev >= 0 && dev < 64) attr_set[dev] = true;
   }
-  mlpk::mlp_grad_kernel<<<mlp_blocks((n + 15) / 16, mlpk::kGradWarps), 32 * mlpk::kGradWarps, mlpk::kGradSmem,
-                          as_stream(stream)>>>(a);
+  const int blocks = mlpk::grad_blocks(n);
+  cudaStream_t st = as_stream(stream);
+  mlpk::mlp_grad_kernel<<<blocks, 32 * mlpk::kGradWarps, mlpk::kGradSmem, st>>>(a);
+  pb_note_launch();
+  PB_LAUNCH_CHECK();
+  mlpk::grad_reduce_kernel<<<ceil_div(mlpk::kPartStride, 256), 256, 0, st>>>(a.part, blocks, grad, loss);
   pb_note_launch();
   PB_LAUNCH_CHECK();
   return PB_OK;

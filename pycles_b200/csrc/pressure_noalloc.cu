@@ -2,9 +2,10 @@
 //
 // pb_pressure_solve needs a caller-provided workspace.  Some callers cannot
 // make one: code running where cudaMalloc is not allowed or not wanted --
-// inside a CUDA-graph capture that must not allocate, under an allocator
-// policy that forbids new device allocations after start-up, or from a host
-// language binding with no device allocator of its own.  This variant keeps
+// in a loop that cannot afford the device-wide synchronisation a cudaMalloc
+// or cudaFree may bring, under an allocator policy that forbids new device
+// allocations after start-up, or from a host language binding with no device
+// allocator of its own.  This variant keeps
 // its scratch in a fixed, file-scope device array instead, so the caller
 // passes only the inputs and outputs.
 //

@@ -47,6 +47,7 @@ class SeedMLP:
         self.v = torch.zeros_like(self.params)
         self.grad = torch.zeros_like(self.params)
         self.loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        self._grad_ws = None  # pb_mlp_grad's per-block partial sums
         self.step_count = 0
         self.out_mean = float(out_mean)
         self.out_scale = float(out_scale)
@@ -91,13 +92,18 @@ class SeedMLP:
         return out
 
     def grad_batch(self, x, target, stream=None):
-        """Zeroes and fills self.grad / self.loss for one batch (pb_mlp_grad)."""
+        """Zeroes and fills self.grad / self.loss for one batch (pb_mlp_grad,
+        deterministic: the same batch gives the same gradient bit for bit)."""
+        L = _capi.load()
+        need = int(L.pb_mlp_grad_workspace_bytes(x.shape[0]))
+        if self._grad_ws is None or self._grad_ws.numel() < need:
+            self._grad_ws = torch.empty(max(need, 16), dtype=torch.uint8, device=self.device)
         self.grad.zero_()
         self.loss.zero_()
         st = self.struct()
-        _capi.check(_capi.load().pb_mlp_grad(ctypes.byref(st), x.data_ptr(), target.data_ptr(), x.shape[0],
-                                             self.grad.data_ptr(), self.loss.data_ptr(),
-                                             _capi.stream_handle(stream)), "pb_mlp_grad")
+        _capi.check(L.pb_mlp_grad(ctypes.byref(st), x.data_ptr(), target.data_ptr(), x.shape[0],
+                                  self.grad.data_ptr(), self.loss.data_ptr(), self._grad_ws.data_ptr(),
+                                  self._grad_ws.numel(), _capi.stream_handle(stream)), "pb_mlp_grad")
 
     def adam(self, lr, n, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
         self.step_count += 1
@@ -198,6 +204,9 @@ def train_seed(thermo, states, n_pairs=10_000_000, jitter=(200.0, 3.0, 5e-4), he
     another seed).  Returns (mlp, info); mlp is None when the draws hold too
     few saturated points."""
     import time
+    # the jittered draws reach outside the saturation table (those pairs are
+    # dropped), which flags the device error word; leave it as it was found
+    word0 = _capi.get_error()
     parts = [[] for _ in range(5)]
     got, draws = 0, 0
     while got < n_pairs and draws < max_draws:
@@ -208,6 +217,8 @@ def train_seed(thermo, states, n_pairs=10_000_000, jitter=(200.0, 3.0, 5e-4), he
         got += P.numel()
         draws += 1
     P, S, Q, T, T1 = (torch.cat(lst)[:n_pairs] for lst in parts)
+    if word0 == 0:
+        _capi.clear_error()
     info = {"training_pairs": int(P.numel()), "samples_drawn": draws * draw, "epochs": epochs,
             "jitter_half_widths": list(jitter)}
     if P.numel() < 1000:
@@ -228,6 +239,9 @@ def train_seed(thermo, states, n_pairs=10_000_000, jitter=(200.0, 3.0, 5e-4), he
     if Ph.numel():
         guess = mlp.forward(Ph, Sh, Qh)
         _, it_seed = secant_iterations(thermo, Ph, Sh, Qh, seed=guess)
+    if word0 == 0:
+        _capi.clear_error()
+    if Ph.numel():
         info.update({"held_out_pairs": int(Ph.numel()),
                      "seed_mean_abs_error_K": float((guess - Th).abs().mean()),
                      "pointwise_mean_iterations_plain": float(its_h.double().mean()),

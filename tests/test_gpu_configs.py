@@ -143,7 +143,7 @@ def _trained_seed(nl, rs, f, steps=(0, 100, 200, 400)):
             g.step()
         done = s
         states.append(tuple(t.clone() for t in learned.cell_inputs(g)))
-    mlp, info = learned.train_seed(g.Th, states, n_pairs=400_000, draw=2_000_000, n_held_out=200_000)
+    mlp, info = learned.train_seed(g.Th, states, n_pairs=2_000_000, draw=4_000_000, n_held_out=200_000)
     assert mlp is not None, info
     return mlp, info
 

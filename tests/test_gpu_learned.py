@@ -91,6 +91,35 @@ def test_mlp_forward_and_gradient_vs_cpu():
     assert np.max(np.abs(y_gpu - y_cpu)) / mlp.out_scale < 3e-2
 
 
+def test_gradient_and_training_are_deterministic():
+    """pb_mlp_grad adds per-block partial sums in a fixed order (no
+    floating-point atomics): the same batch gives the same gradient bit for
+    bit, and the same pairs give the same trained network."""
+    from pycles_b200.learned import SeedMLP
+    rng = np.random.default_rng(2)
+    n = 50_000  # several hundred blocks of partial sums
+    xt = torch.tensor(rng.uniform(-1, 1, size=(n, 3)), dtype=torch.float32, device="cuda")
+    tt = torch.tensor(rng.standard_normal(n) * 0.5, dtype=torch.float32, device="cuda")
+    mlp = SeedMLP(seed=4)
+    grads = []
+    for _ in range(3):
+        mlp.grad_batch(xt, tt)
+        grads.append((mlp.grad.clone(), mlp.loss.clone()))
+    for g, l in grads[1:]:
+        assert torch.equal(g, grads[0][0]) and torch.equal(l, grads[0][1])
+    P = 8.0e4 + 2.0e4 * torch.tensor(rng.uniform(size=n), device="cuda")
+    S = 6900.0 + 100.0 * torch.tensor(rng.uniform(size=n), device="cuda")
+    Q = 0.01 + 0.01 * torch.tensor(rng.uniform(size=n), device="cuda")
+    T1 = 280.0 + torch.tensor(rng.uniform(size=n), device="cuda")
+    T = T1 + 2.0 + torch.tensor(rng.uniform(size=n), device="cuda")
+    nets = []
+    for _ in range(2):
+        m = SeedMLP(seed=0, out_mean=2.5, out_scale=1.0)
+        m.train(P, S, Q, T, T1, epochs=2, batch=8192)
+        nets.append(m.params.clone())
+    assert torch.equal(nets[0], nets[1])
+
+
 def test_trained_seed_cuts_secant_iterations():
     from pycles_b200 import learned
     from pycles_b200.thermodynamics import ThermodynamicsSA

@@ -1,8 +1,9 @@
 """The allocation-free pressure entry point, pb_pressure_solve_noalloc.
 
-Some callers cannot allocate device memory (a graph capture that must not
-allocate, an allocator policy that forbids late device allocations, a host
-binding without a device allocator); this entry point serves them by using
+Some callers cannot allocate device memory (a loop that cannot afford the
+device-wide synchronisation an allocation may bring, an allocator policy that
+forbids late device allocations, a host binding without a device
+allocator); this entry point serves them by using
 a fixed 64 MiB device array inside the library instead of a workspace.  This
 file runs last (pytest collects it last) and checks, through the C ABI, that
 two calls in a row give what pb_pressure_solve gives with a caller
