@@ -681,7 +681,8 @@ def run_ours(args, rank, world, local_rank):
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "form": head, "what": "full prognostic state copied host->device before and device->host "
                                      "after every step (the reference keeps it in host numpy arrays), "
-                                     "through HotPathSimulation.step_host (copies overlap the first "
+                                     "through HotPathSimulation.step_host (copies in quarter-variable chunks, each "
+                                     "uploaded as soon as its download is done; they overlap the first "
                                      "thermodynamics update and the last pressure solve)"}
         del host
 

@@ -194,23 +194,29 @@ class HotPathSimulation:
         for rk in range(self.TS.n_rk_steps):
             self.stage(rk, stream=stream)
 
-    def step_host(self, host_values, stream=None):
+    def step_host(self, host_values, stream=None, chunks_per_variable=4):
         """One time step whose prognostic state lives in pinned host memory,
         as the reference keeps PV.values in host numpy arrays: the state is
-        copied to the device before the step and back after it.  The copies
-        run variable group by variable group on two copy streams (one per
-        direction, so uploads and downloads can use both directions of the
-        link at once): the velocities' upload overlaps the first
-        thermodynamics update (which reads only the scalars), the scalars'
-        download overlaps the last pressure solve (which changes only the
-        velocities; its ghost fill is restricted to them, the scalars' ghosts
-        being already filled), and the next call's scalar upload overlaps
-        this call's velocity download.  Every host region is read only after
-        the download that wrote it.  Asynchronous: host_values holds the new
-        state once `copy_streams()[1]` has finished.
+        copied to the device before the step and back after it.
+
+        The copies run on two copy streams (one per direction, so uploads
+        and downloads use both directions of the link at once), in chunks of
+        1/chunks_per_variable of a variable, each with its own event: the
+        next call uploads a chunk as soon as this call's download of that
+        chunk has finished, so a chunk's round trip is pipelined behind the
+        download of the next one instead of waiting for a whole variable
+        group.  The velocities' upload overlaps the first thermodynamics
+        update (which reads only the scalars); the scalars' download starts
+        before the last pressure solve (which changes only the velocities;
+        its ghost fill is restricted to them, the scalars' ghosts being
+        already filled), and the next call's scalar upload overlaps this
+        call's velocity download.  Every host region is read only after the
+        download that wrote it, and every device region is overwritten only
+        after the download that read it.  Asynchronous: host_values holds
+        the new state once `copy_streams()[1]` has finished.
         host_values: pinned CPU float64 tensor of nv * npg values."""
         import torch
-        Gr, PV, DV, RS = self.Gr, self.PV, self.DV, self.RS
+        Gr, PV = self.Gr, self.PV
         npg = Gr.dims.npg
         st = stream if stream is not None else torch.cuda.current_stream(PV.values.device)
         h2d, d2h = self.copy_streams()
@@ -218,9 +224,16 @@ class HotPathSimulation:
         if vel != list(range(len(vel))):
             raise ValueError("step_host expects the velocities to be the first prognostic variables")
         nvel, nv = len(vel), PV.nv
+        k = max(1, int(chunks_per_variable))
 
-        def copy(dst, src, lo, hi):
-            dst[lo * npg:hi * npg].copy_(src[lo * npg:hi * npg], non_blocking=True)
+        def chunks(v0, v1):
+            step = -(-npg // k)
+            return [(v * npg + lo, v * npg + min(lo + step, npg)) for v in range(v0, v1) for lo in range(0, npg, step)]
+
+        sc_chunks, vel_chunks = chunks(nvel, nv), chunks(0, nvel)
+
+        def copy(dst, src, r):
+            dst[r[0]:r[1]].copy_(src[r[0]:r[1]], non_blocking=True)
 
         def event(stream_):
             e = torch.cuda.Event()
@@ -229,40 +242,45 @@ class HotPathSimulation:
 
         h2d.wait_event(event(st))  # the previous step's work on PV.values is done
         prev = getattr(self, "_host_events", None)
+        if prev is not None and set(prev) != set(sc_chunks + vel_chunks):
+            for e in prev.values():  # another chunking: wait for every download
+                h2d.wait_event(e)
+            prev = None
         with torch.cuda.stream(h2d):
-            if prev is not None:
-                h2d.wait_event(prev[0])  # the previous scalar download has left PV.values / filled host
-            copy(PV.values, host_values, nvel, nv)
+            for r in sc_chunks:
+                if prev is not None:
+                    h2d.wait_event(prev[r])  # the download of this chunk has left PV.values / filled host
+                copy(PV.values, host_values, r)
             e_sc = event(h2d)
-            if prev is not None:
-                h2d.wait_event(prev[1])  # likewise the velocities
-            copy(PV.values, host_values, 0, nvel)
+            for r in vel_chunks:
+                if prev is not None:
+                    h2d.wait_event(prev[r])
+                copy(PV.values, host_values, r)
             e_all = event(h2d)
         st.wait_event(e_sc)
         last = self.TS.n_rk_steps - 1
         out = {}
+
+        def download(rs):
+            d2h.wait_event(event(st))
+            with torch.cuda.stream(d2h):
+                for r in rs:
+                    copy(host_values, PV.values, r)
+                    out[r] = event(d2h)
 
         def hooks(rk):
             def mark(i):
                 if i == 1 and rk == 0:
                     st.wait_event(e_all)  # the velocities' upload, overlapped with the thermodynamics
                 elif i == 4 and rk == last:
-                    # the scalars are final: download them during the pressure solve
-                    d2h.wait_event(event(st))
-                    with torch.cuda.stream(d2h):
-                        copy(host_values, PV.values, nvel, nv)
-                        out["sc"] = event(d2h)
+                    download(sc_chunks)  # the scalars are final: download them during the pressure solve
                 elif i == 5 and rk == last:
-                    d2h.wait_event(event(st))
-                    with torch.cuda.stream(d2h):
-                        copy(host_values, PV.values, 0, nvel)
-                        out["vel"] = event(d2h)
+                    download(vel_chunks)
             return mark
 
         for rk in range(self.TS.n_rk_steps):
             self.stage(rk, st, mark=hooks(rk))
-        e_sc_out, e_vel_out = out["sc"], out["vel"]
-        self._host_events = (e_sc_out, e_vel_out)
+        self._host_events = out
 
     def copy_streams(self):
         """The (host->device, device->host) streams of step_host."""

@@ -236,9 +236,10 @@ def test_device_error_flags():
 
 
 def test_step_host_equals_device_step():
-    """HotPathSimulation.step_host (state in pinned host memory, copies
-    overlapped with the first thermodynamics update and the last pressure
-    solve) gives the device-resident step's state bit for bit."""
+    """HotPathSimulation.step_host (state in pinned host memory, copies in
+    chunks overlapped with the first thermodynamics update and the last
+    pressure solve) gives the device-resident step's state bit for bit, also
+    when the chunking changes between steps."""
     import torch
     nl, rs, f = _setup(MOIST_SMALL, stir=False)
     a, b = gpu_sim(nl, rs, f), gpu_sim(nl, rs, f)
@@ -246,9 +247,9 @@ def test_step_host_equals_device_step():
         g.PV.Update_all_bcs(g.Gr)
     host = torch.empty(b.PV.values.numel(), dtype=torch.float64, pin_memory=True)
     host.copy_(b.PV.values)
-    for _ in range(2):
+    for chunks in (4, 4, 1, 3):
         a.step()
-        b.step_host(host)
+        b.step_host(host, chunks_per_variable=chunks)
     torch.cuda.synchronize()
     ref = a.PV.values.cpu().numpy()
     assert np.all(np.isfinite(ref))
