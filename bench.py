@@ -677,9 +677,10 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         te_ms = max_over_ranks(a.elapsed_time(b), dev, world)
         nbytes = PV.values.numel() * 8
+        link = _link_gbs(host, PV.values, sim.copy_streams())
         e2e = {"value": world * npl * 3 * args.steps / (te_ms / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "form": head, "what": "full prognostic state copied host->device before and device->host "
+               "form": head, "link": link, "what": "full prognostic state copied host->device before and device->host "
                                      "after every step (the reference keeps it in host numpy arrays), "
                                      "through HotPathSimulation.step_host (copies in quarter-variable chunks, each "
                                      "uploaded as soon as its download is done; they overlap the first "
@@ -806,6 +807,39 @@ def run_slabs(args, cfg, rank, world, local_rank):
                        "form": "fp32", "cells": npl, "l2": "inputs larger than L2 (no flush needed)",
                        "parallelism": f"x-slabs x{world}"},
             "e2e": None, "gpu_launches": launches, "device_error_word": _capi.get_error()}
+
+
+def _link_gbs(host, dev_buf, streams, reps=3):
+    """Host<->device copy bandwidth of the state's own pinned buffer, GB/s:
+    each direction alone and both at once (the two copy streams of
+    step_host), best of `reps`; what bounds the end-to-end step."""
+    import torch
+    h2d, d2h = streams
+    nbytes = dev_buf.numel() * 8
+    scratch = torch.empty_like(host, pin_memory=True)
+    out = {}
+    for name, jobs in (("h2d", ((h2d, dev_buf, host),)), ("d2h", ((d2h, scratch, dev_buf),)),
+                       ("both", ((h2d, dev_buf, host), (d2h, scratch, dev_buf)))):
+        best = 0.0
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            start = torch.cuda.Event(enable_timing=True)
+            start.record(torch.cuda.current_stream())
+            ends = []
+            for st, dst, src in jobs:
+                st.wait_event(start)
+                with torch.cuda.stream(st):
+                    dst.copy_(src, non_blocking=True)
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(st)
+                ends.append(e)
+            torch.cuda.synchronize()
+            ms = max(start.elapsed_time(e) for e in ends)
+            best = max(best, len(jobs) * nbytes / (ms / 1e3) / 1e9)
+        out[name + "_gbs"] = round(best, 1)
+    out["bytes_per_copy"] = nbytes
+    del scratch
+    return out
 
 
 def run_accuracy(args, cfg):
