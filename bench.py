@@ -683,8 +683,10 @@ def run_ours(args, rank, world, local_rank):
                "form": head, "link": link, "what": "full prognostic state copied host->device before and device->host "
                                      "after every step (the reference keeps it in host numpy arrays), "
                                      "through HotPathSimulation.step_host (copies in quarter-variable chunks, each "
-                                     "uploaded as soon as its download is done; they overlap the first "
-                                     "thermodynamics update and the last pressure solve)"}
+                                     "uploaded as soon as its download is done; the scalars are downloaded "
+                                     "right after their last pass, the velocities after the last pressure "
+                                     "solve, and the velocities' upload overlaps the first thermodynamics "
+                                     "update)"}
         del host
 
     # ---- roofline per component; the headline is the largest one ----------

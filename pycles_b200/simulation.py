@@ -162,7 +162,12 @@ class HotPathSimulation:
         if not fused:
             m(3)
         TS.update(Gr, PV, stream=stream, mark=m if fused else None)
-        PV.Update_all_bcs(Gr, stream=stream)
+        if self._scalar_ghosts_filled:
+            # a mark hook filled the scalars' ghosts right after their pass
+            self._scalar_ghosts_filled = False
+            self._fill_velocity_ghosts(stream)
+        else:
+            PV.Update_all_bcs(Gr, stream=stream)
         m(4)
         # PressureSolver.update: the solve, then its ghost fill -- of the
         # velocities only, the one thing the correction changed (the
@@ -170,6 +175,8 @@ class HotPathSimulation:
         self.Pr.solve(Gr, RS, DV, PV, stream=stream)
         self._fill_velocity_ghosts(stream)
         m(5)
+
+    _scalar_ghosts_filled = False
 
     def _fused(self) -> bool:
         """The precision form steps with the SSP-RK3 stage fused into the
@@ -206,11 +213,13 @@ class HotPathSimulation:
         chunk has finished, so a chunk's round trip is pipelined behind the
         download of the next one instead of waiting for a whole variable
         group.  The velocities' upload overlaps the first thermodynamics
-        update (which reads only the scalars); the scalars' download starts
-        before the last pressure solve (which changes only the velocities;
-        its ghost fill is restricted to them, the scalars' ghosts being
-        already filled), and the next call's scalar upload overlaps this
-        call's velocity download.  Every host region is read only after the
+        update (which reads only the scalars).  The scalars are final after
+        the last stage's scalar pass: with fused stages their ghosts are
+        filled right there and their download overlaps the momentum pass and
+        the pressure solve (the stage's ghost fill and the solve's are then
+        restricted to the velocities); otherwise it starts before the last
+        pressure solve.  The next call's scalar upload overlaps this call's
+        velocity download.  Every host region is read only after the
         download that wrote it, and every device region is overwritten only
         after the download that read it.  Asynchronous: host_values holds
         the new state once `copy_streams()[1]` has finished.
@@ -261,18 +270,25 @@ class HotPathSimulation:
         last = self.TS.n_rk_steps - 1
         out = {}
 
-        def download(rs):
+        def download(rs, src=None):
             d2h.wait_event(event(st))
             with torch.cuda.stream(d2h):
                 for r in rs:
-                    copy(host_values, PV.values, r)
+                    copy(host_values, PV.values if src is None else src, r)
                     out[r] = event(d2h)
 
         def hooks(rk):
             def mark(i):
                 if i == 1 and rk == 0:
                     st.wait_event(e_all)  # the velocities' upload, overlapped with the thermodynamics
-                elif i == 4 and rk == last:
+                elif i == 2 and rk == last and self.TS.fused_values is not None and sc_chunks:
+                    # the scalars' new values are complete in the fused stage's
+                    # buffer: fill their ghosts and download them from there
+                    buf = self.TS.fused_values
+                    PV.update_bcs_range(Gr, nvel, nv - nvel, stream=st, values=buf)
+                    self._scalar_ghosts_filled = True
+                    download(sc_chunks, src=buf)
+                elif i == 4 and rk == last and sc_chunks and sc_chunks[0] not in out:
                     download(sc_chunks)  # the scalars are final: download them during the pressure solve
                 elif i == 5 and rk == last:
                     download(vel_chunks)

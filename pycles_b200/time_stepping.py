@@ -20,6 +20,7 @@ class TimeStepping:
         self.dt = 1.0
         self.value_copies = None
         self.fused_stages = 0  # stages run through the fused advection + RK3 kernels
+        self.fused_values = None  # during a fused stage: the buffer its passes write the new values to
 
     def initialize(self, namelist, PV, Pa=None):
         ts = namelist["time_stepping"]
@@ -45,7 +46,8 @@ class TimeStepping:
         reference leaves them.  The two value buffers then swap (or, with
         PV.stable_values, the new values are copied back so that PV.values
         keeps its device address).  mark(2) / mark(3), if given, are called
-        after the scalar and the momentum passes."""
+        after the scalar and the momentum passes; during the fused stage
+        `fused_values` names the buffer that receives the new values."""
         pend = PV.take_pending_advection() if PV._pending else {}
         nscal = sum(1 for i in range(PV.nv) if PV.var_type[i] == 1)
         if "momentum" in pend and ("scalar" in pend or nscal == 0):
@@ -72,6 +74,7 @@ class TimeStepping:
             nxt = PV.values_next = torch.zeros_like(PV.values)
         cp = self.value_copies.view(-1)
         tend = PV._tendencies
+        self.fused_values = nxt
         scal = [i for i in range(PV.nv) if PV.var_type[i] == 1]
         if scal:
             SA, _, Rs, _, _ = pend["scalar"]
@@ -104,4 +107,5 @@ class TimeStepping:
                 PV.values.copy_(nxt)
         else:
             PV.values, PV.values_next = nxt, PV.values
+        self.fused_values = None
         self.fused_stages += 1

@@ -155,10 +155,11 @@ class PrognosticVariables:
 
     update_all_bcs = Update_all_bcs
 
-    def update_bcs_range(self, Gr, first, count, stream=None):
-        """Ghost fill of the variables first .. first+count-1 only."""
+    def update_bcs_range(self, Gr, first, count, stream=None, values=None):
+        """Ghost fill of the variables first .. first+count-1 only, of
+        PV.values or of another buffer of the same layout."""
         bc = (ctypes.c_double * count)(*[float(b) for b in self.bc_type[first:first + count]])
-        base = self.values[first * Gr.dims.npg:]
+        base = (self.values if values is None else values)[first * Gr.dims.npg:]
         _capi.check(_capi.load().pb_update_all_bcs(ctypes.byref(Gr.dims), _capi.ptr(base), bc, count,
                                                    _capi.stream_handle(stream)), "pb_update_all_bcs")
 
