@@ -136,6 +136,7 @@ class HotPathSimulation:
         5 after the pressure solve and its ghost fill)."""
         Gr, PV, DV, RS, TS = self.Gr, self.PV, self.DV, self.RS, self.TS
         m = mark if mark is not None else (lambda i: None)
+        self._stages_run += 1
         fused = self._fused()
         PV.fuse_stages = fused
         TS.rk_step = rk_step
@@ -177,6 +178,7 @@ class HotPathSimulation:
         m(5)
 
     _scalar_ghosts_filled = False
+    _stages_run = 0
 
     def _fused(self) -> bool:
         """The precision form steps with the SSP-RK3 stage fused into the
@@ -219,10 +221,17 @@ class HotPathSimulation:
         the pressure solve (the stage's ghost fill and the solve's are then
         restricted to the velocities); otherwise it starts before the last
         pressure solve.  The next call's scalar upload overlaps this call's
-        velocity download.  Every host region is read only after the
-        download that wrote it, and every device region is overwritten only
-        after the download that read it.  Asynchronous: host_values holds
-        the new state once `copy_streams()[1]` has finished.
+        velocity download; the next call's uploads start as soon as their
+        chunks are downloaded, without waiting for the end of this call's
+        pressure solve.  Every host region is read only after the download
+        that wrote it, and every device region is overwritten only after the
+        download that read it and after the last kernel that writes it.
+        Asynchronous: host_values holds the new state once
+        `copy_streams()[1]` has finished.  Between two calls the device copy
+        belongs to step_host: the next call may upload into PV.values before
+        work queued on the stream between the calls has run, so read the
+        state from host_values (a step or stage run between the calls makes
+        the next call wait for the stream, as the first call does).
         host_values: pinned CPU float64 tensor of nv * npg values."""
         import torch
         Gr, PV = self.Gr, self.PV
@@ -249,12 +258,21 @@ class HotPathSimulation:
             e.record(stream_)
             return e
 
-        h2d.wait_event(event(st))  # the previous step's work on PV.values is done
         prev = getattr(self, "_host_events", None)
-        if prev is not None and set(prev) != set(sc_chunks + vel_chunks):
-            for e in prev.values():  # another chunking: wait for every download
-                h2d.wait_event(e)
-            prev = None
+        free = getattr(self, "_host_free", None)
+        if getattr(self, "_host_stages", None) != self._stages_run:
+            prev = free = None  # stages ran since the last call: not a continuation
+        if prev is None or free is None:
+            h2d.wait_event(event(st))  # the work queued on PV.values so far
+        else:
+            # the previous call's last stage no longer writes the scalars
+            # (recorded after its ghost fill); each chunk also waits for its
+            # own download below, the velocities' after the pressure solve
+            h2d.wait_event(free)
+            if set(prev) != set(sc_chunks + vel_chunks):
+                for e in prev.values():  # another chunking: wait for every download
+                    h2d.wait_event(e)
+                prev = None
         with torch.cuda.stream(h2d):
             for r in sc_chunks:
                 if prev is not None:
@@ -288,8 +306,10 @@ class HotPathSimulation:
                     PV.update_bcs_range(Gr, nvel, nv - nvel, stream=st, values=buf)
                     self._scalar_ghosts_filled = True
                     download(sc_chunks, src=buf)
-                elif i == 4 and rk == last and sc_chunks and sc_chunks[0] not in out:
-                    download(sc_chunks)  # the scalars are final: download them during the pressure solve
+                elif i == 4 and rk == last:
+                    if sc_chunks and sc_chunks[0] not in out:
+                        download(sc_chunks)  # the scalars are final: download them during the pressure solve
+                    self._host_free = event(st)
                 elif i == 5 and rk == last:
                     download(vel_chunks)
             return mark
@@ -297,6 +317,7 @@ class HotPathSimulation:
         for rk in range(self.TS.n_rk_steps):
             self.stage(rk, st, mark=hooks(rk))
         self._host_events = out
+        self._host_stages = self._stages_run
 
     def copy_streams(self):
         """The (host->device, device->host) streams of step_host."""
