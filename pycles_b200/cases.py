@@ -2,8 +2,8 @@
 
 Each case follows the structure of a reference initialiser (profiles in z,
 perturbations from ``np.random.seed(rank)`` + ``random_sample(npg)`` drawn in
-[i][j][k] order, Galilean shift) with the amplitudes of the configurations
-this build is measured on.  The functions fill host numpy arrays; the
+[i][j][k] order, Galilean shift) with the amplitudes of the benchmark
+configurations.  The functions fill host numpy arrays; the
 caller uploads them.  Vectorised: levels without perturbation are computed
 once per level and broadcast.
 

@@ -141,7 +141,7 @@ def test_fp32_form_five_steps():
 
 
 def test_fp32_form_1000_steps_against_fp64_form():
-    """The north star's accuracy budget for the precision form: relative L2
+    """The accuracy budget of the precision form: relative L2
     error <= 1e-5 on s, qt and the velocities after 1000 steps.  The
     reference here is the FP64 plain form on the GPU (the oracle is too
     slow for 1000 steps; the plain form equals it to ~1e-13 after a step)."""
