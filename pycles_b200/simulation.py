@@ -230,8 +230,10 @@ class HotPathSimulation:
         `copy_streams()[1]` has finished.  Between two calls the device copy
         belongs to step_host: the next call may upload into PV.values before
         work queued on the stream between the calls has run, so read the
-        state from host_values (a step or stage run between the calls makes
-        the next call wait for the stream, as the first call does).
+        state from host_values.  Work on the device copy between two calls
+        must first wait for `copy_streams()` (the downloads still read it); a
+        step or stage run between the calls makes the next call wait for the
+        stream, as the first call does.
         host_values: pinned CPU float64 tensor of nv * npg values."""
         import torch
         Gr, PV = self.Gr, self.PV

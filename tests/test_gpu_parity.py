@@ -239,7 +239,8 @@ def test_step_host_equals_device_step():
     """HotPathSimulation.step_host (state in pinned host memory, copies in
     chunks overlapped with the first thermodynamics update and the last
     pressure solve) gives the device-resident step's state bit for bit, also
-    when the chunking changes between steps."""
+    when the chunking changes between steps and when a device step runs
+    between two host steps."""
     import torch
     nl, rs, f = _setup(MOIST_SMALL, stir=False)
     a, b = gpu_sim(nl, rs, f), gpu_sim(nl, rs, f)
@@ -250,6 +251,14 @@ def test_step_host_equals_device_step():
     for chunks in (4, 4, 1, 3):
         a.step()
         b.step_host(host, chunks_per_variable=chunks)
+    # a device step between two host steps (ordered after the download, as
+    # any work on the device copy must be): its result is replaced by the
+    # host state's upload, which must wait for it, not race with it
+    for cs in b.copy_streams():
+        torch.cuda.current_stream().wait_stream(cs)
+    b.step()
+    a.step()
+    b.step_host(host)
     torch.cuda.synchronize()
     ref = a.PV.values.cpu().numpy()
     assert np.all(np.isfinite(ref))
