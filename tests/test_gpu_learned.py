@@ -233,25 +233,30 @@ def test_seed_with_refresh_is_faster_on_a_cloudy_grid():
     assert times["seeded"] < times["plain"]
 
 
-def test_tensor_core_refresh_matches_cpu_network():
+@pytest.mark.parametrize("shape,gw,flagged", [((64, 64, 48), 4, 0.5), ((30, 22, 17), 3, 0.5),
+                                               ((30, 22, 17), 3, 0.0), ((30, 22, 17), 3, 1.0)])
+def test_tensor_core_refresh_matches_cpu_network(shape, gw, flagged):
     """pb_mlp_refresh_seed (tcgen05 products, FP32 accumulators in tensor
-    memory) against the FP64 CPU evaluation of the same BF16 network on a
-    field with half of its cells flagged, several scan rounds per block;
-    cells not flagged get NaN.  Tolerance as the forward check: 3e-2 of the
-    output's scale."""
+    memory) against the FP64 CPU evaluation of the same BF16 network: half
+    of the cells flagged (several scan rounds per block), none and all, on a
+    grid whose cell count is a multiple of the 128-cell tile and on a ragged
+    one; cells not flagged get NaN.  Tolerance as the forward check: 3e-2 of
+    the output's scale."""
     import ctypes
 
     from pycles_b200 import _capi
     from pycles_b200.learned import SeedMLP
     from pycles_b200.parallel import slab_dims
     mlp = SeedMLP(seed=5)
-    dims = slab_dims((64, 64, 48), 4, (35.0, 35.0, 5.0))
+    dims = slab_dims(shape, gw, (35.0, 35.0, 5.0))
     npg, n2 = int(dims.npg), int(dims.nlg[2])
     g = torch.Generator(device="cuda").manual_seed(7)
     p0 = 9.0e4 + 5.0e3 * torch.rand(n2, device="cuda", dtype=torch.float64, generator=g)
     s = 6850.0 + 200.0 * torch.rand(npg, device="cuda", dtype=torch.float64, generator=g)
     qt = 0.025 * torch.rand(npg, device="cuda", dtype=torch.float64, generator=g)
-    ql = torch.rand(npg, device="cuda", dtype=torch.float64, generator=g) - 0.5  # > 0: flagged
+    ql = torch.rand(npg, device="cuda", dtype=torch.float64, generator=g) - (1.0 - flagged)  # > 0: flagged
+    if flagged == 1.0:
+        ql += 1e-9
     y = torch.zeros(npg, dtype=torch.float32, device="cuda")
     st = mlp.struct()
     st.seed_y = y.data_ptr()
@@ -264,6 +269,11 @@ def test_tensor_core_refresh_matches_cpu_network():
     assert np.isnan(yg[~flag]).all()
     P = p0.repeat(npg // n2)
     x = mlp.normalise(P, s, qt).cpu().numpy().astype(np.float64)
+    if flagged == 0.0:
+        assert not flag.any()
+        return
+    if flagged == 1.0:
+        assert flag.all()
     yc, _ = _cpu_mlp(mlp.params.cpu().numpy(), x[flag], 0, 1, True)
     err = np.max(np.abs(yg[flag] - yc)) / max(1.0, float(np.max(np.abs(yc))))
     print("tensor-core refresh vs FP64 CPU network: max error", err, "flagged cells", int(flag.sum()))
