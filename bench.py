@@ -637,6 +637,9 @@ def run_ours(args, rank, world, local_rank):
             results[form]["stage_calls"] = ("the reference's call order per stage (Th, SA, MA, TS, bcs, Pr); "
                                             "SA and MA deferred into TS.update, which runs the fused passes")
             log(f"form {form} unfused: {results[form]['unfused_ms_per_step']:.2f} ms/step")
+        if not args.no_graph:
+            results[form]["graph"] = _time_graph(sim, args.steps, local_rank, world)
+            log(f"form {form} as CUDA graphs: {results[form]['graph']['ms_per_step']:.2f} ms/step")
         if form == forms[-1][0]:
             headline_sim = sim
         else:
@@ -811,6 +814,29 @@ def run_slabs(args, cfg, rank, world, local_rank):
             "e2e": None, "gpu_launches": launches, "device_error_word": _capi.get_error()}
 
 
+def _time_graph(sim, steps, local_rank, world):
+    """The same steps recorded as CUDA graphs (HotPathSimulation.capture_steps:
+    graph_steps() time steps per graph, one host launch per replay) and
+    replayed: ms per step over the replays that fit in `steps`, at least
+    one; the state advances as with eager steps."""
+    import torch
+    n = sim.graph_steps()
+    g = sim.capture_steps()
+    g.replay()  # warm-up
+    torch.cuda.synchronize()
+    reps = max(1, steps // n)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        g.replay()
+    b.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(a.elapsed_time(b), torch.device("cuda", local_rank), world) / (reps * n)
+    del g
+    return {"ms_per_step": ms, "steps_per_graph": n, "replays": reps,
+            "value": world * sim.Gr.dims.npl * 3 / (ms / 1e3)}
+
+
 def _link_gbs(host, dev_buf, streams, reps=3):
     """Host<->device copy bandwidth of the state's own pinned buffer, GB/s:
     each direction alone and both at once (the two copy streams of
@@ -943,6 +969,8 @@ def main():
                          "slabs: the configuration's domain split in x-slabs across the GPUs, halo "
                          "exchanges and the pressure's transposes over NCCL (strong scaling)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="skip the per-form timing of the steps recorded as CUDA graphs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surface", action="store_true",
                     help="skip the timings of the case's surface scheme and forcing, of the Smagorinsky "

@@ -329,6 +329,52 @@ class HotPathSimulation:
             self._copy_streams = (torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev))
         return self._copy_streams
 
+    def graph_steps(self) -> int:
+        """The smallest number of time steps that one CUDA graph of the step
+        (capture_steps) may hold: even when the fused stages swap the two
+        value buffers (so that PV.values is the same buffer after the
+        recorded steps), and a whole number of learned-seed refresh periods
+        when the seed is on (so that every replay refreshes as the eager
+        steps do)."""
+        import math
+        n = 2 if (self._fused() and not self.PV.stable_values) else 1
+        if getattr(self.Th, "mlp", None) is not None:
+            upd = self.TS.n_rk_steps
+            every = int(self.Th.seed_refresh_interval)
+            per = every // math.gcd(every, upd)
+            n = n * per // math.gcd(n, per)
+        return n
+
+    def capture_steps(self, nsteps: int = 0):
+        """Records nsteps device-resident time steps (`step`) as one CUDA
+        graph and returns it (torch.cuda.CUDAGraph): `graph.replay()` runs
+        them with one launch from the host.  For grids whose steps are bound
+        by kernel launches (at 64x64x75 a step is ~150 kernels of a few
+        microseconds).  nsteps = 0 takes graph_steps(); other counts must be
+        multiples of it.  At least one step must have run eagerly (the lazily
+        made buffers, workspaces and tables exist then); recording runs no
+        kernel and does not advance the state.  The host-side time (TS.t)
+        does not advance on replay, and the simulation must not change form,
+        grid or learned seed while the graph is in use."""
+        import torch
+        unit = self.graph_steps()
+        n = unit if nsteps == 0 else int(nsteps)
+        if n < 1 or n % unit:
+            raise ValueError(f"a graph of this simulation holds a multiple of {unit} steps, not {nsteps}")
+        if self._stages_run < self.TS.n_rk_steps:
+            raise RuntimeError("run one step eagerly before capturing the step in a graph")
+        dev = self.PV.values.device
+        g = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        t0 = self.TS.t
+        with torch.cuda.graph(g, stream=side):
+            for _ in range(n):
+                self.step()
+        self.TS.t = t0
+        torch.cuda.current_stream(dev).wait_stream(side)
+        return g
+
     def run(self, nsteps: int, stream=None):
         """Simulation3d.run: ghost fill and a thermodynamics update before the
         loop (its first output), then nsteps time steps."""
