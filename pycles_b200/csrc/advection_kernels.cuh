@@ -673,25 +673,65 @@ __global__ void __launch_bounds__(MomTile<ORDER>::NT, 1) momentum_tile(Geo g, Mo
   }
 }
 
-constexpr int kChunk = 64;  // cells per marching thread along x / y
+constexpr int kChunk = 64;  // cells per marching thread along x / y, at most (march_chunk)
+
+// Cells per block along the marching direction.  The grid runs in waves of
+// sms x per_sm resident blocks and a block takes ~chunk + lead steps (lead:
+// its window fill), so the chunk in [8, max_chunk] with the fewest
+// wave-steps is taken (ties: the longer chunk).  A fixed 64 left the last
+// wave nearly empty at 512x512x256 (2520 blocks of the momentum pass on 148
+// SMs: 17.03 waves) and most SMs idle on small grids (15 blocks at
+// 64x64x75).  The results do not depend on the chunk: a face on a chunk
+// boundary is evaluated by both blocks with the same arithmetic.
+inline int march_chunk(long long n_march, long long other_blocks, int per_sm, int lead, int max_chunk) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long slots = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  int best = max_chunk;
+  long long best_cost = -1;
+  for (int c = 8; c <= max_chunk; ++c) {
+    const long long blocks = other_blocks * ((n_march + c - 1) / c);
+    const long long cost = (blocks + slots - 1) / slots * (c + lead);
+    if (best_cost < 0 || cost <= best_cost) {
+      best_cost = cost;
+      best = c;
+    }
+  }
+  return best;
+}
+
+template <class K>
+inline int resident_blocks(K kernel, int threads, size_t smem = 0) {
+  int n = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n < 1) n = 1;
+  return n;
+}
 
 template <int ORDER, bool F32, int NS>
 cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* flux_dir[3],
                                 const double* const vel[3], cudaStream_t st) {
+  constexpr int R = St<ORDER>::R;
   const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
   dim3 blk(32, 4);
   {
     ScalarArgs a = base;
     a.vel = vel[0];
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[0] ? flux_dir[0][q] : nullptr;
-    dim3 grd(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, kChunk));
+    const long long other = (long long)ceil_div(nl2, 32) * ceil_div(nl1, 4);
     if constexpr (F32 && NS == 1) {
-      if (a.fused)
-        scalar_march_f32<0, ORDER, true><<<grd, blk, 0, st>>>(g, a, kChunk);
-      else
-        scalar_march_f32<0, ORDER, false><<<grd, blk, 0, st>>>(g, a, kChunk);
+      if (a.fused) {
+        const int c = march_chunk(nl0, other, resident_blocks(scalar_march_f32<0, ORDER, true>, 128), 2 * R, kChunk);
+        scalar_march_f32<0, ORDER, true><<<dim3(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, c)), blk, 0, st>>>(
+            g, a, c);
+      } else {
+        const int c = march_chunk(nl0, other, resident_blocks(scalar_march_f32<0, ORDER, false>, 128), 2 * R, kChunk);
+        scalar_march_f32<0, ORDER, false><<<dim3(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, c)), blk, 0, st>>>(
+            g, a, c);
+      }
     } else {
-      scalar_march<0, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
+      const int c = march_chunk(nl0, other, resident_blocks(scalar_march<0, ORDER, F32, NS>, 128), 2 * R, kChunk);
+      scalar_march<0, ORDER, F32, NS><<<dim3(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, c)), blk, 0, st>>>(
+          g, a, c);
     }
     pb_note_launch();
   }
@@ -699,11 +739,16 @@ cudaError_t launch_scalar_group(const Geo& g, ScalarArgs base, double* const* fl
     ScalarArgs a = base;
     a.vel = vel[1];
     for (int q = 0; q < NS; ++q) a.flux[q] = flux_dir[1] ? flux_dir[1][q] : nullptr;
-    dim3 grd(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, kChunk));
-    if constexpr (F32 && NS == 1)
-      scalar_march_f32<1, ORDER, false><<<grd, blk, 0, st>>>(g, a, kChunk);
-    else
-      scalar_march<1, ORDER, F32, NS><<<grd, blk, 0, st>>>(g, a, kChunk);
+    const long long other = (long long)ceil_div(nl2, 32) * ceil_div(nl0, 4);
+    if constexpr (F32 && NS == 1) {
+      const int c = march_chunk(nl1, other, resident_blocks(scalar_march_f32<1, ORDER, false>, 128), 2 * R, kChunk);
+      scalar_march_f32<1, ORDER, false><<<dim3(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, c)), blk, 0, st>>>(
+          g, a, c);
+    } else {
+      const int c = march_chunk(nl1, other, resident_blocks(scalar_march<1, ORDER, F32, NS>, 128), 2 * R, kChunk);
+      scalar_march<1, ORDER, F32, NS><<<dim3(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, c)), blk, 0, st>>>(
+          g, a, c);
+    }
     pb_note_launch();
   }
   {
@@ -762,18 +807,24 @@ template <int ORDER, bool F32>
 cudaError_t launch_momentum(const Geo& g, const MomArgs& a, cudaStream_t st) {
   const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
   dim3 blk(32, 4);
+  constexpr int R = St<ORDER>::R;
   if constexpr (F32) {  // precision form: one pass for the three advecting directions
     using T = MomTile<ORDER>;
-    momentum_tile<ORDER, false><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, kChunk)), T::NT, 0,
-                                  st>>>(g, a, kChunk);
+    const int c = march_chunk(nl0, (long long)ceil_div(nl2, 31) * ceil_div(nl1, T::TJ), 1, R + 1, 128);
+    momentum_tile<ORDER, false><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, c)), T::NT, 0,
+                                  st>>>(g, a, c);
     pb_note_launch();
     return cudaGetLastError();
   } else {
-  momentum_march<0, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, kChunk)), blk, 0,
-                                  st>>>(g, a, kChunk);
+  const int c0 = march_chunk(nl0, (long long)ceil_div(nl2, 32) * ceil_div(nl1, 4),
+                             resident_blocks(momentum_march<0, ORDER, F32>, 128), 2 * R, kChunk);
+  momentum_march<0, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl1, 4), ceil_div(nl0, c0)), blk, 0,
+                                  st>>>(g, a, c0);
   pb_note_launch();
-  momentum_march<1, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, kChunk)), blk, 0,
-                                  st>>>(g, a, kChunk);
+  const int c1 = march_chunk(nl1, (long long)ceil_div(nl2, 32) * ceil_div(nl0, 4),
+                             resident_blocks(momentum_march<1, ORDER, F32>, 128), 2 * R, kChunk);
+  momentum_march<1, ORDER, F32><<<dim3(ceil_div(nl2, 32), ceil_div(nl0, 4), ceil_div(nl1, c1)), blk, 0,
+                                  st>>>(g, a, c1);
   pb_note_launch();
   momentum_z<ORDER, F32><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, 4), (unsigned)nl0), 128, 0, st>>>(g, a);
   pb_note_launch();
@@ -786,8 +837,9 @@ template <int ORDER>
 cudaError_t launch_momentum_rk3(const Geo& g, const MomArgs& a, cudaStream_t st) {
   const long long nl0 = g.n0 - 2 * g.gw, nl1 = g.n1 - 2 * g.gw, nl2 = g.n2 - 2 * g.gw;
   using T = MomTile<ORDER>;
-  momentum_tile<ORDER, true><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, kChunk)), T::NT, 0, st>>>(
-      g, a, kChunk);
+  const int c = march_chunk(nl0, (long long)ceil_div(nl2, 31) * ceil_div(nl1, T::TJ), 1, T::R + 1, 128);
+  momentum_tile<ORDER, true><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, c)), T::NT, 0, st>>>(
+      g, a, c);
   pb_note_launch();
   return cudaGetLastError();
 }

@@ -236,8 +236,9 @@ cudaError_t launch_momentum_tma(const Geo& g, const MomArgs& a, cudaStream_t st)
   cudaError_t e = cudaFuncSetAttribute(momentum_tma<ORDER, RK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)Q::SMEM);
   if (e != cudaSuccess) return e;
-  momentum_tma<ORDER, RK><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, kChunk)), T::NT, Q::SMEM,
-                            st>>>(g, a, kChunk, m[0], m[1], m[2]);
+  const int c = march_chunk(nl0, (long long)ceil_div(nl2, 31) * ceil_div(nl1, T::TJ), 1, T::R + 1, 128);
+  momentum_tma<ORDER, RK><<<dim3(ceil_div(nl2, 31), ceil_div(nl1, T::TJ), ceil_div(nl0, c)), T::NT, Q::SMEM,
+                            st>>>(g, a, c, m[0], m[1], m[2]);
   pb_note_launch();
   return cudaGetLastError();
 }
