@@ -1061,7 +1061,13 @@ static int fft_forward(const Geo& g, PArgs& a, int src, cudaStream_t st) {
 template <class C>
 static int fft_columns(const Geo& g, PArgs& a, cudaStream_t st) {
   const long long Nh = (g.n0 - 2 * g.gw) / 2 + 1, Ny = g.n1 - 2 * g.gw;
-  tdma_kernel<C><<<ceil_div(Nh * Ny, 256), 256, 0, st>>>(g, a);
+  // one thread per column; on grids with fewer columns than 256 per SM the
+  // blocks shrink (to a multiple of 32 threads) so that every SM gets some
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long per_sm = (Nh * Ny + sms - 1) / sms;
+  const int threads = per_sm >= 256 ? 256 : (int)((per_sm + 31) / 32 * 32);
+  tdma_kernel<C><<<ceil_div(Nh * Ny, threads), threads, 0, st>>>(g, a);
   pb_note_launch();
   PB_LAUNCH_CHECK();
   return PB_OK;
