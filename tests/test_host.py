@@ -157,3 +157,24 @@ def test_precision_form_refinement_algorithm_on_cpu():
     dq = (q - p64).reshape(sh)[I]
     dq -= dq.mean(axis=(0, 1), keepdims=True)
     assert np.linalg.norm(dq) / np.linalg.norm(p64.reshape(sh)[I]) < 1e-12
+
+
+def test_graph_step_counts():
+    """How many time steps one CUDA graph of the step holds (host logic, no
+    GPU): 1 for the plain form, 2 for the fused precision form (its stages
+    swap the two value buffers, three swaps a step), 1 with stable value
+    addresses, and whole learned-seed refresh periods with the seed."""
+    from pycles_b200.learned import SeedMLP
+    from pycles_b200.simulation import CONFIGS, HotPathSimulation, namelist_for
+    small = dict(CONFIGS["c2_bomex"], nx=16, ny=16, nz=12)
+    plain = HotPathSimulation(namelist_for(**small, precision="fp64"), device="cpu")
+    assert plain.graph_steps() == 1
+    prec = HotPathSimulation(namelist_for(**small, precision="fp32"), device="cpu")
+    assert prec.graph_steps() == 2
+    prec.PV.stable_values = True
+    assert prec.graph_steps() == 1
+    prec.PV.stable_values = False
+    prec.Th.mlp = SeedMLP(device="cpu")
+    for every, steps in ((12, 4), (6, 2), (3, 2), (5, 10), (1, 2)):
+        prec.Th.seed_refresh_interval = every
+        assert prec.graph_steps() == steps, every
