@@ -289,6 +289,7 @@ class HotPathSimulation:
         st.wait_event(e_sc)
         last = self.TS.n_rk_steps - 1
         out = {}
+        freed = [None]
 
         def download(rs, src=None):
             d2h.wait_event(event(st))
@@ -308,10 +309,13 @@ class HotPathSimulation:
                     PV.update_bcs_range(Gr, nvel, nv - nvel, stream=st, values=buf)
                     self._scalar_ghosts_filled = True
                     download(sc_chunks, src=buf)
+                    if not PV.stable_values:  # nothing writes the scalars after this point
+                        self._host_free = freed[0] = event(st)
                 elif i == 4 and rk == last:
                     if sc_chunks and sc_chunks[0] not in out:
                         download(sc_chunks)  # the scalars are final: download them during the pressure solve
-                    self._host_free = event(st)
+                    if freed[0] is None:  # (with stable addresses: after the copy back)
+                        self._host_free = event(st)
                 elif i == 5 and rk == last:
                     download(vel_chunks)
             return mark
